@@ -1,0 +1,17 @@
+"""cutc_b200 -- B200-native (sm_100a) sparse tensor completion engine.
+
+A drop-in for the single-GPU driver of cuTC (abovekumo/cuTC): .tns tensor
+load, CISS tiling, ALS / CCD / CCD++ / SGD with per-epoch train/val/test
+RMSE, behind the C ABI in include/ctc.h (libctc.so).  This package holds the
+CUDA/C++ sources (csrc/), the in-tree build (build.py) and the Python
+bindings (api.py).
+"""
+from .api import (ALS, CCD, CCDPP, SGD, PREC_F32, PREC_F64, PREC_MIXED, LR_BOLD_DRIVER,
+                  LR_CONSTANT, LR_EXP_DECAY, SGD_HOGWILD, SGD_SEQUENTIAL, Context, CtcError,
+                  Dataset, Model, Params, Tensor, ciss_alloc, grad, lib, params, rmse, run, tc_als,
+                  tc_ccd, tc_main_ciss, tc_sgd, tt_read)
+
+__all__ = ["ALS", "CCD", "CCDPP", "SGD", "PREC_F32", "PREC_F64", "PREC_MIXED", "LR_BOLD_DRIVER",
+           "LR_CONSTANT", "LR_EXP_DECAY", "SGD_HOGWILD", "SGD_SEQUENTIAL", "Context", "CtcError",
+           "Dataset", "Model", "Params", "Tensor", "ciss_alloc", "grad", "lib", "params", "rmse",
+           "run", "tc_als", "tc_ccd", "tc_main_ciss", "tc_sgd", "tt_read"]

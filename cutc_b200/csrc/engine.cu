@@ -1,0 +1,1183 @@
+// engine.cu -- device-side orchestration of libctc: staging of the mode
+// copies, the device-resident session (factors, residuals, scratch), the
+// ALS / CCD / CCD++ / SGD epochs (optionally replayed as a CUDA graph),
+// evaluation, early stop, and the C ABI entry points that need the GPU.
+#include "ctc_internal.h"
+#include "kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <thread>
+#include <type_traits>
+
+double ctc_value_through_idx(double v);
+
+namespace ctc {
+
+static void check_cuda(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) fail(e == cudaErrorMemoryAllocation ? CTC_E_NOMEM : CTC_E_CUDA,
+                               "%s: %s", what, cudaGetErrorString(e));
+}
+#define CK(x) check_cuda((x), #x)
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count)
+    {
+        release();
+        if (count == 0) count = 1;
+        CK(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void ensure(size_t count)
+    {
+        if (n < count) alloc(count);
+    }
+    void upload(const T *h, size_t count, cudaStream_t s)
+    {
+        ensure(count);
+        if (count) CK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+};
+
+template <typename F>
+static void par_for(uint64_t n, F &&fn)
+{
+    int P = host_threads();
+    if (n < 65536 || P == 1) {
+        fn((uint64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int p = 0; p < P; ++p) {
+        uint64_t b = n * p / P, e = n * (p + 1) / P;
+        th.emplace_back([&, b, e] { fn(b, e); });
+    }
+    for (auto &t : th) t.join();
+}
+
+template <typename F>
+static void with_rank(int R, F &&f)
+{
+    switch (R) {
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    case 32: f(std::integral_constant<int, 32>{}); break;
+    case 64: f(std::integral_constant<int, 64>{}); break;
+    default: fail(CTC_E_UNSUP, "rank %d not supported (8, 16, 32, 64)", R);
+    }
+}
+
+constexpr int kSMs = 148;
+constexpr int kMaxPartials = kSMs * 8;
+constexpr int kScalars = 16;
+
+static unsigned grid_for(uint64_t work, unsigned per_block, unsigned cap)
+{
+    uint64_t g = (work + per_block - 1) / per_block;
+    if (g < 1) g = 1;
+    return (unsigned)std::min<uint64_t>(g, cap);
+}
+
+// per-kernel device time, from an event pair around every launch
+struct KernelTimes {
+    bool on = false;
+    std::vector<std::pair<const char *, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+    std::map<std::string, std::pair<uint64_t, double>> acc;  // name -> (count, ms)
+    size_t used = 0;
+};
+
+}  // namespace ctc
+
+using namespace ctc;
+
+struct ctc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevBuf<double> partial;   // per-block reduction partials
+    DevBuf<double> scalars;   // reduction results
+    double *h_scalars = nullptr;  // pinned mirror
+    bool capturing = false;
+    KernelTimes kt;
+};
+
+namespace ctc {
+
+static void kt_flush(ctc_ctx *ctx)
+{
+    KernelTimes &k = ctx->kt;
+    if (k.pending.empty()) return;
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (auto &pe : k.pending) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, pe.second.first, pe.second.second));
+        auto &a = k.acc[pe.first];
+        a.first += 1;
+        a.second += ms;
+    }
+    k.pending.clear();
+    k.used = 0;
+}
+
+template <typename Kern, typename... Args>
+static void launch_named(ctc_ctx *ctx, const char *name, Kern kern, unsigned grid, unsigned block,
+                         size_t smem, Args... args)
+{
+    KernelTimes &k = ctx->kt;
+    const bool timed = k.on && !ctx->capturing;
+    std::pair<cudaEvent_t, cudaEvent_t> ev{};
+    if (timed) {
+        if (k.used >= 4096) kt_flush(ctx);
+        if (k.used == k.pool.size()) {
+            cudaEvent_t a, b;
+            CK(cudaEventCreate(&a));
+            CK(cudaEventCreate(&b));
+            k.pool.push_back({a, b});
+        }
+        ev = k.pool[k.used++];
+        CK(cudaEventRecord(ev.first, ctx->stream));
+    }
+    kern<<<grid, block, smem, ctx->stream>>>(args...);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    if (timed) {
+        CK(cudaEventRecord(ev.second, ctx->stream));
+        k.pending.push_back({name, ev});
+    }
+}
+#define LAUNCH(ctx, kern, ...) launch_named(ctx, #kern, kern, __VA_ARGS__)
+
+// One tensor staged on the device as 16-byte records (+ FP64 values in
+// FP64 runs), optionally with its row-aligned work tiles for one mode and
+// the reference lane multiplicities.
+template <typename T>
+struct DevTensor {
+    DevBuf<uint4> rec;
+    DevBuf<double> v64;
+    uint32_t n = 0;
+    int mode = -1;
+    DevBuf<int4> tiles;
+    uint32_t ntiles = 0;
+    DevBuf<uint4> heavy;
+    uint32_t nheavy = 0;
+    DevBuf<T> w;
+    bool has_w = false;
+};
+
+static void validate_tensor(const ctc_tensor *t, const uint64_t *dims, const char *what)
+{
+    if (!t) fail(CTC_E_ARG, "%s: null tensor", what);
+    if (t->nmodes != 3) fail(CTC_E_UNSUP, "%s: only order-3 tensors are supported (got %d)", what, t->nmodes);
+    if (t->nnz == 0) fail(CTC_E_ARG, "%s: empty tensor", what);
+    if (t->nnz >= 0xfffffff0ull) fail(CTC_E_UNSUP, "%s: more than 2^32 nonzeros", what);
+    for (int m = 0; m < 3; ++m)
+        if (dims[m] == 0 || dims[m] >= 0xfffffff0ull)
+            fail(CTC_E_UNSUP, "%s: bad dimension %llu", what, (unsigned long long)dims[m]);
+    std::atomic<int> bad{0};
+    par_for(t->nnz, [&](uint64_t b, uint64_t e) {
+        for (int m = 0; m < 3; ++m) {
+            const uint64_t *ind = t->ind[m].data();
+            for (uint64_t i = b; i < e; ++i)
+                if (ind[i] == 0 || ind[i] > dims[m]) {
+                    bad = 1;
+                    return;
+                }
+        }
+    });
+    if (bad) fail(CTC_E_ARG, "%s: indices must be 1-based and within the model dimensions", what);
+}
+
+template <typename T>
+static void stage_tensor(ctc_ctx *ctx, const ctc_tensor *t, bool trunc, DevTensor<T> &d)
+{
+    const uint64_t n = t->nnz;
+    std::vector<uint4> rec(n);
+    std::vector<double> v64(std::is_same<T, double>::value ? n : 0);
+    par_for(n, [&](uint64_t b, uint64_t e) {
+        for (uint64_t i = b; i < e; ++i) {
+            double v = t->vals[i];
+            if (trunc) v = ctc_value_through_idx(v);
+            float vf = (float)v;
+            uint32_t bits;
+            memcpy(&bits, &vf, 4);
+            rec[i] = make_uint4((uint32_t)(t->ind[0][i] - 1), (uint32_t)(t->ind[1][i] - 1),
+                                (uint32_t)(t->ind[2][i] - 1), bits);
+            if (!v64.empty()) v64[i] = v;
+        }
+    });
+    d.n = (uint32_t)n;
+    d.rec.upload(rec.data(), n, ctx->stream);
+    if (!v64.empty()) d.v64.upload(v64.data(), n, ctx->stream);
+    CK(cudaStreamSynchronize(ctx->stream));
+}
+
+template <typename T>
+static void stage_plan(ctc_ctx *ctx, const ctc_tensor *t, int mode, uint32_t tile_len, DevTensor<T> &d)
+{
+    const uint64_t n = t->nnz;
+    std::vector<uint32_t> rows(n);
+    par_for(n, [&](uint64_t b, uint64_t e) {
+        for (uint64_t i = b; i < e; ++i) rows[i] = (uint32_t)(t->ind[mode][i] - 1);
+    });
+    for (uint64_t i = 1; i < n; ++i)
+        if (rows[i] < rows[i - 1])
+            fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", mode + 1, mode + 1);
+    TilePlan p = plan_tiles(rows.data(), n, tile_len);
+    d.mode = mode;
+    d.ntiles = p.ntiles();
+    d.nheavy = p.nheavy();
+    d.tiles.upload(reinterpret_cast<const int4 *>(p.tiles.data()), p.ntiles(), ctx->stream);
+    d.heavy.upload(reinterpret_cast<const uint4 *>(p.heavy_rows.data()), p.nheavy(), ctx->stream);
+    CK(cudaStreamSynchronize(ctx->stream));
+}
+
+template <typename T>
+static void stage_weights(ctc_ctx *ctx, const ctc_tensor *t, int mode, int kernel, DevTensor<T> &d)
+{
+    ctc_ciss *cp = nullptr;
+    if (ctc_ciss_build(t, mode + 1, 32, &cp) != CTC_OK) fail(CTC_E_ARG, "%s", ctc_last_error());
+    std::unique_ptr<ctc_ciss, int (*)(ctc_ciss *)> guard(cp, ctc_ciss_free);
+    std::vector<double> w;
+    compat_weights(*cp, kernel, w);
+    std::vector<T> wt(w.begin(), w.end());
+    d.w.upload(wt.data(), wt.size(), ctx->stream);
+    d.has_w = true;
+    CK(cudaStreamSynchronize(ctx->stream));
+}
+
+// Device-resident state of one run: factors (row-major, or column-major
+// for CCD++), best-epoch copy, CCD++ residuals in the staged records,
+// scratch, the SGD step on the device, and the captured epoch graph.
+struct SessionBase {
+    virtual ~SessionBase() = default;
+    virtual void set_model(const ctc_model *m) = 0;
+    virtual void get_model(ctc_model *m, bool best) = 0;
+    virtual void epochs(int n) = 0;
+    virtual void evaluate(ctc_epoch_stats *st) = 0;
+    virtual void set_lr(double lr) = 0;
+    virtual void save_best() = 0;
+    virtual uint64_t nonspd() = 0;
+    virtual void set_params(const ctc_params &p) = 0;
+};
+
+}  // namespace ctc
+
+// ---------------------------------------------------------------------
+// dataset: staged tensors for one algorithm / precision + its session
+// ---------------------------------------------------------------------
+struct ctc_dataset {
+    ctc_ctx *ctx = nullptr;
+    ctc_params p{};
+    uint64_t dims[3] = {0, 0, 0};
+    uint64_t nnz_train = 0;
+    bool has_val = false, has_test = false;
+    struct Base {
+        virtual ~Base() = default;
+    };
+    std::unique_ptr<Base> impl;
+    std::unique_ptr<ctc::SessionBase> session;
+    int session_rank = 0;
+};
+
+namespace ctc {
+
+template <typename T>
+struct DatasetImpl : ctc_dataset::Base {
+    DevTensor<T> copy[3];
+    DevTensor<T> val, test;
+    // CCD++ overwrites the staged values with residuals: the values are kept
+    // (FP32 bits / FP64) to restart from another model
+    DevBuf<uint32_t> orig32[3];
+    DevBuf<double> orig64[3];
+    bool resid_dirty = false;
+};
+
+static int default_tile(int alg)
+{
+    switch (alg) {
+    case CTC_ALG_ALS: return 512;
+    case CTC_ALG_SGD: return 256;
+    default: return 256;
+    }
+}
+
+template <typename T>
+static void build_dataset(ctc_dataset *ds, const ctc_tensor *const train[3], const ctc_tensor *val,
+                          const ctc_tensor *test)
+{
+    auto impl = std::make_unique<DatasetImpl<T>>();
+    ctc_ctx *ctx = ds->ctx;
+    const ctc_params &p = ds->p;
+    const bool trunc = p.compat != 0;
+    const uint32_t tl = (uint32_t)(p.tile_len > 0 ? p.tile_len : default_tile(p.alg));
+    std::unique_ptr<ctc_tensor> own[3];
+    const ctc_tensor *srt[3] = {train[0], train[1], train[2]};
+    const int ncopies = (p.alg == CTC_ALG_SGD) ? 1 : 3;
+    for (int m = 0; m < ncopies; ++m) {
+        if (!srt[m]) {
+            own[m].reset(new ctc_tensor(*train[0]));
+            if (ctc_tensor_sort(own[m].get(), m) != CTC_OK) fail(CTC_E_ARG, "%s", ctc_last_error());
+            srt[m] = own[m].get();
+        }
+        if (srt[m]->nnz != train[0]->nnz) fail(CTC_E_ARG, "training copies differ in size");
+        validate_tensor(srt[m], ds->dims, "training tensor");
+        stage_tensor<T>(ctx, srt[m], trunc, impl->copy[m]);
+        if (p.alg != CTC_ALG_SGD) stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
+        if (trunc && (p.alg == CTC_ALG_ALS || p.alg == CTC_ALG_CCD))
+            stage_weights<T>(ctx, srt[m], m, p.alg == CTC_ALG_CCD ? 1 : 0, impl->copy[m]);
+        if (p.alg == CTC_ALG_CCDPP) {
+            DevTensor<T> &c = impl->copy[m];
+            if (std::is_same<T, double>::value) {
+                impl->orig64[m].alloc(c.n);
+                CK(cudaMemcpyAsync(impl->orig64[m].p, c.v64.p, (size_t)c.n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+            } else {
+                impl->orig32[m].alloc(c.n);
+                CK(cudaMemcpy2DAsync(impl->orig32[m].p, 4, reinterpret_cast<const char *>(c.rec.p) + 12, 16, 4, c.n,
+                                     cudaMemcpyDeviceToDevice, ctx->stream));
+            }
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+    }
+    if (p.alg == CTC_ALG_SGD) {
+        // SGD tiles are plain chunks of the mode-1 order (sgpu/sgd.cu:32-34)
+        impl->copy[0].mode = 0;
+        impl->copy[0].ntiles = (uint32_t)((impl->copy[0].n + tl - 1) / tl);
+    }
+    if (val) {
+        validate_tensor(val, ds->dims, "validation tensor");
+        stage_tensor<T>(ctx, val, false, impl->val);
+    }
+    if (test) {
+        validate_tensor(test, ds->dims, "test tensor");
+        stage_tensor<T>(ctx, test, false, impl->test);
+    }
+    ds->impl = std::move(impl);
+}
+
+template <typename T, int R>
+struct Session : SessionBase {
+    ctc_ctx *ctx;
+    ctc_dataset *ds;
+    DatasetImpl<T> *D;
+    ctc_params p;
+    uint32_t dims[3];
+    bool colmajor;
+    uint32_t tile_len;
+    DevBuf<T> U[3], Ubest[3], Urow[3], old[3], slot, slot2, lr_dev, zrow;
+    DevBuf<unsigned long long> nonspd_dev;
+    cudaGraphExec_t graph = nullptr;
+    bool model_set = false;
+
+    Session(ctc_dataset *d) : ctx(d->ctx), ds(d), p(d->p)
+    {
+        D = static_cast<DatasetImpl<T> *>(d->impl.get());
+        for (int m = 0; m < 3; ++m) dims[m] = (uint32_t)d->dims[m];
+        colmajor = p.alg == CTC_ALG_CCDPP;
+        tile_len = (uint32_t)(p.tile_len > 0 ? p.tile_len : default_tile(p.alg));
+        nonspd_dev.alloc(1);
+        lr_dev.alloc(1);
+        for (int m = 0; m < 3; ++m) {
+            const size_t sz = (size_t)dims[m] * R;
+            U[m].alloc(sz);
+            Ubest[m].alloc(sz);
+            if (colmajor) {
+                Urow[m].alloc(sz);
+                old[m].alloc(dims[m]);
+            }
+        }
+        // scratch sized once so an epoch can be captured as a graph
+        size_t need = 1;
+        for (int m = 0; m < 3; ++m) {
+            const DevTensor<T> &c = D->copy[m];
+            if (!c.nheavy && p.alg != CTC_ALG_CCDPP) continue;
+            if (p.alg == CTC_ALG_ALS) need = std::max<size_t>(need, (size_t)c.ntiles * (R * R + R));
+            else if (p.alg == CTC_ALG_CCD) need = std::max<size_t>(need, (size_t)c.ntiles * 2 * R);
+            else if (p.alg == CTC_ALG_CCDPP) need = std::max<size_t>(need, (size_t)c.ntiles);
+        }
+        slot.alloc(need);
+        if (p.alg == CTC_ALG_CCDPP) slot2.alloc(need);
+        uint32_t mx = std::max(dims[0], std::max(dims[1], dims[2]));
+        zrow.alloc((size_t)mx * R);
+        CK(cudaMemsetAsync(zrow.p, 0, (size_t)mx * R * sizeof(T), ctx->stream));
+        if (p.alg == CTC_ALG_ALS) {
+            using Sh = k::AlsShape<R>;
+            const int smem = (int)(4 * Sh::smem_doubles * sizeof(double));
+            CK(cudaFuncSetAttribute(k::k_als_tile<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            CK(cudaFuncSetAttribute(k::k_als_fix<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        }
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+
+    ~Session() override
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+    }
+
+    // run-time parameters (lambda, inner, lr, schedule, order ...); the
+    // staged layout (alg, precision, compat, tile length) stays
+    void set_params(const ctc_params &np) override
+    {
+        p = np;
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+    }
+
+    void set_model(const ctc_model *mdl) override
+    {
+        for (int m = 0; m < 3; ++m) {
+            const uint64_t d = dims[m];
+            std::vector<T> h(d * R);
+            const double *src = mdl->U[m].data();
+            par_for(d, [&](uint64_t b, uint64_t e) {
+                for (uint64_t r = b; r < e; ++r)
+                    for (int f = 0; f < R; ++f)
+                        h[colmajor ? (uint64_t)f * d + r : r * R + f] = (T)src[r * R + f];
+            });
+            U[m].upload(h.data(), h.size(), ctx->stream);
+            CK(cudaMemcpyAsync(Ubest[m].p, U[m].p, h.size() * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+        CK(cudaMemsetAsync(nonspd_dev.p, 0, sizeof(unsigned long long), ctx->stream));
+        set_lr(p.lr * (p.lr_scale > 0 ? p.lr_scale : 1.0));
+        if (colmajor) {
+            if (D->resid_dirty) {
+                for (int m = 0; m < 3; ++m) {
+                    DevTensor<T> &c = D->copy[m];
+                    if (std::is_same<T, double>::value)
+                        CK(cudaMemcpyAsync(c.v64.p, D->orig64[m].p, (size_t)c.n * 8, cudaMemcpyDeviceToDevice,
+                                           ctx->stream));
+                    else
+                        CK(cudaMemcpy2DAsync(reinterpret_cast<char *>(c.rec.p) + 12, 16, D->orig32[m].p, 4, 4, c.n,
+                                             cudaMemcpyDeviceToDevice, ctx->stream));
+                }
+            }
+            ccdpp_init();
+            D->resid_dirty = true;
+        }
+        CK(cudaStreamSynchronize(ctx->stream));
+        model_set = true;
+    }
+
+    void get_model(ctc_model *mdl, bool best) override
+    {
+        DevBuf<T> *src = best ? Ubest : U;
+        for (int m = 0; m < 3; ++m) {
+            const uint64_t d = dims[m];
+            std::vector<T> h(d * R);
+            CK(cudaMemcpyAsync(h.data(), src[m].p, h.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            double *dst = mdl->U[m].data();
+            par_for(d, [&](uint64_t b, uint64_t e) {
+                for (uint64_t r = b; r < e; ++r)
+                    for (int f = 0; f < R; ++f)
+                        dst[r * R + f] = (double)h[colmajor ? (uint64_t)f * d + r : r * R + f];
+            });
+        }
+    }
+
+    void set_lr(double lr) override
+    {
+        T v = (T)lr;
+        CK(cudaMemcpyAsync(lr_dev.p, &v, sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+
+    void save_best() override
+    {
+        for (int m = 0; m < 3; ++m)
+            CK(cudaMemcpyAsync(Ubest[m].p, U[m].p, (size_t)dims[m] * R * sizeof(T), cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+    }
+
+    uint64_t nonspd() override
+    {
+        unsigned long long v = 0;
+        CK(cudaMemcpyAsync(&v, nonspd_dev.p, sizeof(v), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return v;
+    }
+
+    // ---- reductions into ctx->scalars[s]
+    void sse_into(const DevTensor<T> &t, const T *const Urm[3], int s)
+    {
+        const unsigned g = grid_for(t.n, 256, kMaxPartials);
+        LAUNCH(ctx, k::k_sse<T, R>, g, 256, 0, (const uint4 *)t.rec.p, (const double *)t.v64.p, t.n,
+               Urm[0], Urm[1], Urm[2], ctx->partial.p);
+        LAUNCH(ctx, k::k_sum_partials, 1, 256, 0, (const double *)ctx->partial.p, (int)g, ctx->scalars.p + s);
+    }
+    void sumsq_into(const T *x, uint64_t n, int s)
+    {
+        const unsigned g = grid_for(n, 256, kMaxPartials);
+        LAUNCH(ctx, k::k_sumsq<T>, g, 256, 0, x, n, ctx->partial.p);
+        LAUNCH(ctx, k::k_sum_partials, 1, 256, 0, (const double *)ctx->partial.p, (int)g, ctx->scalars.p + s);
+    }
+
+    // ---- epochs
+    void als_epoch()
+    {
+        using Sh = k::AlsShape<R>;
+        const size_t smem = 4 * Sh::smem_doubles * sizeof(double);
+        for (int q = 0; q < 3; ++q) {
+            const int m = (p.mode_start + q) % 3;
+            const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+            DevTensor<T> &c = D->copy[m];
+            CK(cudaMemsetAsync(U[m].p, 0, (size_t)dims[m] * R * sizeof(T), ctx->stream));
+            LAUNCH(ctx, k::k_als_tile<T, R>, grid_for(c.ntiles, 4, kSMs * 16), 128, smem, (const int4 *)c.tiles.p,
+                   c.ntiles, (const uint4 *)c.rec.p, (const double *)c.v64.p,
+                   (const T *)(c.has_w ? c.w.p : nullptr), m, U[m].p, (const T *)U[m1].p, (const T *)U[m2].p,
+                   (T)p.lambda, slot.p, nonspd_dev.p);
+            if (c.nheavy)
+                LAUNCH(ctx, k::k_als_fix<T, R>, grid_for(c.nheavy, 4, kSMs * 16), 128, smem,
+                       (const uint4 *)c.heavy.p, c.nheavy, (const T *)slot.p, U[m].p, (T)p.lambda, nonspd_dev.p);
+        }
+    }
+
+    void ccd_epoch()
+    {
+        for (int q = 0; q < 3; ++q) {
+            const int m = (p.mode_start + q) % 3;
+            const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+            DevTensor<T> &c = D->copy[m];
+            LAUNCH(ctx, k::k_ccdc_tile<T, R>, grid_for(c.ntiles, 4, kSMs * 16), 128, 0, (const int4 *)c.tiles.p,
+                   c.ntiles, (const uint4 *)c.rec.p, (const double *)c.v64.p,
+                   (const T *)(c.has_w ? c.w.p : nullptr), m, U[m].p, (const T *)U[m1].p, (const T *)U[m2].p,
+                   (T)p.lambda, slot.p);
+            if (c.nheavy)
+                LAUNCH(ctx, k::k_ccdc_fix<T, R>, grid_for(c.nheavy, 4, kSMs * 16), 128, 0,
+                       (const uint4 *)c.heavy.p, c.nheavy, (const T *)slot.p, U[m].p, (T)p.lambda);
+        }
+    }
+
+    void sgd_epoch()
+    {
+        DevTensor<T> &c = D->copy[0];
+        constexpr int G = R / k::Vec<T>::n;
+        const int gpb = 8 * (32 / G);  // groups per 256-thread block
+        const bool seq = p.sgd_order == CTC_SGD_SEQUENTIAL;
+        const unsigned g = seq ? 1 : grid_for(c.ntiles, gpb, kSMs * 8);
+        LAUNCH(ctx, k::k_sgd<T, R>, g, seq ? 32 : 256, 0, (const uint4 *)c.rec.p, (const double *)c.v64.p, c.n,
+               tile_len, c.ntiles, U[0].p, U[1].p, U[2].p, (const T *)lr_dev.p, (T)p.lambda, p.sgd_atomic,
+               seq ? 1 : 0);
+    }
+
+    k::CcdCols cols_for(int f, int fprev, int m)
+    {
+        k::CcdCols c{};
+        for (int n = 0; n < 3; ++n) {
+            c.cur[n] = U[n].p + (size_t)f * dims[n];
+            c.prev[n] = fprev < 0 ? nullptr
+                                  : (fprev == f ? (const void *)old[n].p
+                                                : (const void *)(U[n].p + (size_t)fprev * dims[n]));
+            c.old[n] = old[n].p;
+        }
+        c.out = m >= 0 ? (void *)(U[m].p + (size_t)f * dims[m]) : nullptr;
+        return c;
+    }
+
+    void ccdpp_init()
+    {
+        for (int m = 0; m < 3; ++m) {
+            DevTensor<T> &c = D->copy[m];
+            LAUNCH(ctx, k::k_ccd_resid_init<T, R>, grid_for(c.n, 256, kSMs * 16), 256, 0, c.rec.p, c.v64.p, c.n,
+                   (const T *)U[0].p, (const T *)U[1].p, (const T *)U[2].p, dims[0], dims[1], dims[2]);
+        }
+    }
+
+    // One CCD++ outer iteration: per column f, `inner` sweeps over the modes
+    // of the column update (the first sweep of each copy also refreshes its
+    // residual), then a finish pass per copy leaves r = x - model in every
+    // copy and the training SSE in scalars[0].
+    void ccdpp_outer()
+    {
+        const int inner = p.inner > 0 ? p.inner : 1;
+        for (int f = 0; f < R; ++f) {
+            for (int n = 0; n < 3; ++n)
+                CK(cudaMemcpyAsync(old[n].p, U[n].p + (size_t)f * dims[n], dims[n] * sizeof(T),
+                                   cudaMemcpyDeviceToDevice, ctx->stream));
+            for (int it = 0; it < inner; ++it) {
+                for (int q = 0; q < 3; ++q) {
+                    const int m = (p.mode_start + q) % 3;
+                    DevTensor<T> &c = D->copy[m];
+                    k::CcdCols cols = cols_for(f, f > 0 ? f - 1 : -1, m);
+                    CK(cudaMemsetAsync(U[m].p + (size_t)f * dims[m], 0, dims[m] * sizeof(T), ctx->stream));
+                    const unsigned g = grid_for(c.ntiles, 8, kSMs * 8);
+                    if (it == 0)
+                        LAUNCH(ctx, k::k_ccd_pass<T, true>, g, 256, 0, (const int4 *)c.tiles.p, c.ntiles, c.rec.p,
+                               c.v64.p, m, cols, (T)p.lambda, slot.p, slot2.p);
+                    else
+                        LAUNCH(ctx, k::k_ccd_pass<T, false>, g, 256, 0, (const int4 *)c.tiles.p, c.ntiles, c.rec.p,
+                               c.v64.p, m, cols, (T)p.lambda, slot.p, slot2.p);
+                    if (c.nheavy)
+                        LAUNCH(ctx, k::k_ccd_fix<T>, grid_for(c.nheavy, 8, kSMs * 8), 256, 0, (const uint4 *)c.heavy.p,
+                               c.nheavy, (const T *)slot.p, (const T *)slot2.p, (T *)cols.out, (T)p.lambda);
+                }
+            }
+        }
+        for (int m = 0; m < 3; ++m) {
+            DevTensor<T> &c = D->copy[m];
+            k::CcdCols cols = cols_for(R - 1, R - 1, -1);
+            // the last column's final values (not the snapshot)
+            for (int n = 0; n < 3; ++n) cols.prev[n] = U[n].p + (size_t)(R - 1) * dims[n];
+            const unsigned g = grid_for(c.n, 256, kMaxPartials);
+            LAUNCH(ctx, k::k_ccd_finish<T>, g, 256, 0, c.rec.p, c.v64.p, c.n, cols,
+                   m == 0 ? ctx->partial.p : (double *)nullptr);
+            if (m == 0)
+                LAUNCH(ctx, k::k_sum_partials, 1, 256, 0, (const double *)ctx->partial.p, (int)g, ctx->scalars.p + 0);
+        }
+    }
+
+    void one_epoch()
+    {
+        switch (p.alg) {
+        case CTC_ALG_ALS: als_epoch(); break;
+        case CTC_ALG_CCD: ccd_epoch(); break;
+        case CTC_ALG_CCDPP: ccdpp_outer(); break;
+        case CTC_ALG_SGD: sgd_epoch(); break;
+        }
+    }
+
+    void epochs(int n) override
+    {
+        if (!model_set) fail(CTC_E_ARG, "no model staged on the dataset");
+        const bool use_graph = p.use_graph && !ctx->kt.on && p.sgd_order != CTC_SGD_SEQUENTIAL;
+        for (int i = 0; i < n; ++i) {
+            if (!use_graph) {
+                one_epoch();
+                continue;
+            }
+            if (!graph) {
+                cudaGraph_t g = nullptr;
+                ctx->capturing = true;
+                CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+                try {
+                    one_epoch();
+                } catch (...) {
+                    cudaStreamEndCapture(ctx->stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                    ctx->capturing = false;
+                    throw;
+                }
+                CK(cudaStreamEndCapture(ctx->stream, &g));
+                ctx->capturing = false;
+                CK(cudaGraphInstantiate(&graph, g, 0));
+                CK(cudaGraphDestroy(g));
+            }
+            CK(cudaGraphLaunch(graph, ctx->stream));
+            ctx->launches += 1;
+        }
+    }
+
+    // scalars: 0 train SSE, 2 val SSE, 3 test SSE, 4..6 sum of squares of U
+    void evaluate(ctc_epoch_stats *st) override
+    {
+        const T *Urm[3];
+        for (int m = 0; m < 3; ++m) {
+            if (colmajor) {
+                LAUNCH(ctx, k::k_col_to_row<T>, grid_for((uint64_t)dims[m] * R, 256, kSMs * 8), 256, 0,
+                       (const T *)U[m].p, Urow[m].p, dims[m], R);
+                Urm[m] = Urow[m].p;
+            } else {
+                Urm[m] = U[m].p;
+            }
+        }
+        if (colmajor) {
+            // copy 0 holds r = x - model: its SSE is the sum of squares
+            const T *z[3] = {zrow.p, zrow.p, zrow.p};
+            sse_into(D->copy[0], z, 0);
+        } else {
+            sse_into(D->copy[0], Urm, 0);
+        }
+        for (int m = 0; m < 3; ++m) sumsq_into(U[m].p, (uint64_t)dims[m] * R, 4 + m);
+        if (ds->has_val) sse_into(D->val, Urm, 2);
+        if (ds->has_test) sse_into(D->test, Urm, 3);
+        CK(cudaMemcpyAsync(ctx->h_scalars, ctx->scalars.p, kScalars * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const double *s = ctx->h_scalars;
+        st->loss = s[0];
+        st->frob = p.lambda * (s[4] + s[5] + s[6]);
+        st->rmse_tr = std::sqrt(s[0] / (double)ds->nnz_train);
+        st->rmse_vl = ds->has_val ? std::sqrt(s[2] / (double)D->val.n) : -1.0;
+        st->rmse_te = ds->has_test ? std::sqrt(s[3] / (double)D->test.n) : -1.0;
+    }
+};
+
+static SessionBase *session_for(ctc_dataset *d, int rank)
+{
+    if (d->session && d->session_rank == rank) return d->session.get();
+    d->session.reset();
+    with_rank(rank, [&](auto RC) {
+        constexpr int R = decltype(RC)::value;
+        if (d->p.precision == CTC_PREC_F64) d->session.reset(new Session<double, R>(d));
+        else d->session.reset(new Session<float, R>(d));
+    });
+    d->session_rank = rank;
+    return d->session.get();
+}
+
+// The epoch loop of tc_als / tc_sgd / tc_ccd with tc_converge's bookkeeping
+// (sgpu/completion.c:296-362) and the SGD learning-rate schedule
+// (sgpu/sgd.cu:315-323).
+static void run_loop(ctc_dataset *ds, SessionBase *S, ctc_model *model, ctc_model *best, const ctc_params &p,
+                     ctc_epoch_cb cb, void *user, ctc_result *res)
+{
+    ctc_ctx *ctx = ds->ctx;
+    S->set_model(model);
+    double lr_base = p.lr;
+    const double scale = p.lr_scale > 0 ? p.lr_scale : 1.0;
+    double best_rmse = 10000000.0;  // BEST_RMSE, sgpu/base.h:35
+    int nbad = 0, best_epoch = 0;
+    double prev_obj = 0, total_ms = 0;
+    ctc_epoch_stats st{};
+    auto report = [&](int epoch, double ms) -> bool {
+        S->evaluate(&st);
+        st.epoch = epoch;
+        st.ms_epoch = ms;
+        st.lr = lr_base * scale;
+        if (!std::isfinite(st.loss)) fail(CTC_E_NUMERIC, "training loss is not finite at epoch %d", epoch);
+        const double conv = ds->has_val ? st.rmse_vl : st.rmse_tr;
+        bool converged = false;
+        if (conv - best_rmse < -p.tolerance) {
+            nbad = 0;
+            best_rmse = conv;
+            best_epoch = epoch;
+            S->save_best();
+        } else if (++nbad == p.max_bad_epochs) {
+            converged = true;
+        }
+        int stop = cb ? cb(user, &st) : 0;
+        return stop != 0 || (p.early_stop && converged);
+    };
+    bool stop = report(0, 0.0);
+    prev_obj = st.loss + st.frob;
+    int e = 1;
+    for (; !stop && e <= p.iters; ++e) {
+        CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        S->epochs(1);
+        CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        CK(cudaEventSynchronize(ctx->ev1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        total_ms += ms;
+        const bool bold = p.alg == CTC_ALG_SGD && p.lr_schedule == CTC_LR_BOLD_DRIVER;
+        const bool need = p.early_stop || bold || e == p.iters || (p.eval_every > 0 && e % p.eval_every == 0);
+        if (need) stop = report(e, ms);
+        if (p.alg == CTC_ALG_SGD) {
+            if (bold) {
+                const double obj = st.loss + st.frob;
+                if (e > 1) lr_base *= (obj < prev_obj) ? 1.05 : 0.50;
+                prev_obj = obj;
+            } else if (p.lr_schedule == CTC_LR_EXP_DECAY) {
+                lr_base *= p.lr_decay;
+            }
+            S->set_lr(lr_base * scale);
+        }
+    }
+    if (res) {
+        res->epochs_run = e - 1;
+        res->best_epoch = best_epoch;
+        res->best_rmse = best_rmse;
+        res->final_rmse_tr = st.rmse_tr;
+        res->final_rmse_vl = st.rmse_vl;
+        res->final_rmse_te = st.rmse_te;
+        res->total_ms = total_ms;
+        res->nonspd_rows = S->nonspd();
+    }
+    S->get_model(model, false);
+    if (best) {
+        if (best->nmodes != 3 || best->rank != model->rank) *best = *model;
+        S->get_model(best, true);
+    }
+}
+
+static void check_params(const ctc_params *p)
+{
+    if (!p) fail(CTC_E_ARG, "null params");
+    if (p->alg < CTC_ALG_ALS || p->alg > CTC_ALG_CCDPP) fail(CTC_E_ARG, "unknown algorithm %d", p->alg);
+    if (p->precision != CTC_PREC_F32 && p->precision != CTC_PREC_F64)
+        fail(CTC_E_UNSUP, "precision %d not available in this build", p->precision);
+    if (p->rank != 8 && p->rank != 16 && p->rank != 32 && p->rank != 64)
+        fail(CTC_E_UNSUP, "rank %d not supported (8, 16, 32, 64)", p->rank);
+    if (p->tile_len < 0 || p->tile_len > (1 << 20)) fail(CTC_E_ARG, "tile_len %d", p->tile_len);
+    if (p->iters < 0) fail(CTC_E_ARG, "iters %d", p->iters);
+    if (p->mode_start < 0 || p->mode_start > 2) fail(CTC_E_ARG, "mode_start %d", p->mode_start);
+}
+
+static void check_model(const ctc_dataset *d, const ctc_model *model, int rank)
+{
+    if (!model) fail(CTC_E_ARG, "null model");
+    if (model->nmodes != 3 || model->rank != rank) fail(CTC_E_ARG, "model shape does not match the rank");
+    for (int m = 0; m < 3; ++m)
+        if (model->dims[m] != d->dims[m])
+            fail(CTC_E_ARG, "model mode %d has %llu rows, the dataset %llu", m, (unsigned long long)model->dims[m],
+                 (unsigned long long)d->dims[m]);
+}
+
+}  // namespace ctc
+
+// ---------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------
+extern "C" int ctc_ctx_create(int device, ctc_ctx **out)
+{
+    return guarded([&] {
+        if (!out) fail(CTC_E_ARG, "null out");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            fail(CTC_E_NOGPU, "no CUDA device available");
+        }
+        if (device < 0 || device >= n) fail(CTC_E_ARG, "device %d out of range (%d devices)", device, n);
+        CK(cudaSetDevice(device));
+        auto c = std::make_unique<ctc_ctx>();
+        c->device = device;
+        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&c->ev0));
+        CK(cudaEventCreate(&c->ev1));
+        c->partial.alloc(kMaxPartials);
+        c->scalars.alloc(kScalars);
+        CK(cudaMemset(c->scalars.p, 0, kScalars * sizeof(double)));
+        CK(cudaMallocHost(&c->h_scalars, kScalars * sizeof(double)));
+        *out = c.release();
+    });
+}
+
+extern "C" int ctc_ctx_destroy(ctc_ctx *ctx)
+{
+    if (!ctx) return CTC_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto &e : ctx->kt.pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    ctx->partial.release();
+    ctx->scalars.release();
+    if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return CTC_OK;
+}
+
+extern "C" int ctc_ctx_kernel_launches(const ctc_ctx *ctx, uint64_t *out)
+{
+    return guarded([&] {
+        if (!ctx || !out) fail(CTC_E_ARG, "null argument");
+        *out = ctx->launches;
+    });
+}
+
+extern "C" void *ctc_ctx_stream(ctc_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+extern "C" int ctc_ctx_set_profiling(ctc_ctx *ctx, int on)
+{
+    return guarded([&] {
+        if (!ctx) fail(CTC_E_ARG, "null context");
+        kt_flush(ctx);
+        ctx->kt.on = on != 0;
+    });
+}
+
+extern "C" int ctc_ctx_kernel_time(ctc_ctx *ctx, const char *name, uint64_t *count, double *total_ms)
+{
+    return guarded([&] {
+        if (!ctx || !name) fail(CTC_E_ARG, "null argument");
+        kt_flush(ctx);
+        uint64_t c = 0;
+        double ms = 0;
+        for (auto &kv : ctx->kt.acc)
+            if (kv.first.find(name) != std::string::npos) {
+                c += kv.second.first;
+                ms += kv.second.second;
+            }
+        if (count) *count = c;
+        if (total_ms) *total_ms = ms;
+    });
+}
+
+extern "C" int ctc_ctx_reset_kernel_times(ctc_ctx *ctx)
+{
+    return guarded([&] {
+        if (!ctx) fail(CTC_E_ARG, "null context");
+        kt_flush(ctx);
+        ctx->kt.acc.clear();
+    });
+}
+
+extern "C" int ctc_params_default(int alg, ctc_params *p)
+{
+    return guarded([&] {
+        if (!p) fail(CTC_E_ARG, "null params");
+        memset(p, 0, sizeof(*p));
+        p->alg = alg;
+        p->rank = 16;                 // DEFAULT_NFACTORS, sgpu/base.h:21
+        p->lambda = alg == CTC_ALG_ALS ? 10.0 : (alg == CTC_ALG_SGD ? 1e-3 : 100.0);  // base.h:39-41
+        p->lr = 1e-3;                 // LEARN_RATE, base.h:58
+        p->lr_scale = 1e-5;           // SGD_MODIFICATION*, base.h:42-44
+        p->lr_schedule = CTC_LR_BOLD_DRIVER;
+        p->lr_decay = 0.95;
+        p->iters = 1000;              // DEFAULT_MAX_ITERATE, base.h:22
+        p->inner = 1;                 // NUM_INNER, base.h:30
+        p->precision = CTC_PREC_F32;
+        p->early_stop = 1;
+        p->tolerance = 1e-4;          // TOLERANCE, base.h:36
+        p->max_bad_epochs = 3;        // MAX_BADEPOCHS, base.h:32
+        p->sgd_order = CTC_SGD_HOGWILD;
+        p->sgd_atomic = 1;
+        p->eval_every = 1;
+    });
+}
+
+extern "C" int ctc_dataset_create(ctc_ctx *ctx, const ctc_tensor *const train[3], const ctc_tensor *val,
+                                  const ctc_tensor *test, const ctc_params *p, ctc_dataset **out)
+{
+    return guarded([&] {
+        if (!ctx || !train || !train[0] || !out) fail(CTC_E_ARG, "null argument");
+        check_params(p);
+        CK(cudaSetDevice(ctx->device));
+        auto ds = std::make_unique<ctc_dataset>();
+        ds->ctx = ctx;
+        ds->p = *p;
+        for (int m = 0; m < 3; ++m) {
+            uint64_t d = 0;
+            for (const ctc_tensor *t : {train[0], val, test})
+                if (t && t->nmodes == 3) d = std::max(d, t->dims[m]);
+            ds->dims[m] = d;
+        }
+        ds->nnz_train = train[0]->nnz;
+        ds->has_val = val != nullptr;
+        ds->has_test = test != nullptr;
+        if (p->precision == CTC_PREC_F64) build_dataset<double>(ds.get(), train, val, test);
+        else build_dataset<float>(ds.get(), train, val, test);
+        *out = ds.release();
+    });
+}
+
+extern "C" int ctc_dataset_dims(const ctc_dataset *d, uint64_t *dims)
+{
+    return guarded([&] {
+        if (!d || !dims) fail(CTC_E_ARG, "null argument");
+        for (int m = 0; m < 3; ++m) dims[m] = d->dims[m];
+    });
+}
+
+extern "C" int ctc_dataset_free(ctc_dataset *d)
+{
+    if (d) {
+        cudaSetDevice(d->ctx->device);
+        cudaStreamSynchronize(d->ctx->stream);
+        delete d;
+    }
+    return CTC_OK;
+}
+
+static void check_run_params(const ctc_dataset *d, const ctc_params *p)
+{
+    check_params(p);
+    if (p->alg != d->p.alg || p->precision != d->p.precision || p->compat != d->p.compat ||
+        p->tile_len != d->p.tile_len)
+        fail(CTC_E_ARG, "parameters differ from the dataset's (alg/precision/compat/tile_len)");
+}
+
+extern "C" int ctc_dataset_run(ctc_dataset *d, ctc_model *model, ctc_model *best, const ctc_params *p,
+                               ctc_epoch_cb cb, void *user, ctc_result *res)
+{
+    return guarded([&] {
+        if (!d) fail(CTC_E_ARG, "null dataset");
+        check_run_params(d, p);
+        check_model(d, model, p->rank);
+        CK(cudaSetDevice(d->ctx->device));
+        d->p = *p;
+        SessionBase *S = session_for(d, p->rank);
+        S->set_params(*p);
+        run_loop(d, S, model, best, *p, cb, user, res);
+    });
+}
+
+extern "C" int ctc_dataset_set_model(ctc_dataset *d, const ctc_model *model)
+{
+    return guarded([&] {
+        if (!d) fail(CTC_E_ARG, "null dataset");
+        check_model(d, model, model ? model->rank : 0);
+        CK(cudaSetDevice(d->ctx->device));
+        d->p.rank = model->rank;
+        session_for(d, model->rank)->set_model(model);
+    });
+}
+
+extern "C" int ctc_dataset_epochs(ctc_dataset *d, int n)
+{
+    return guarded([&] {
+        if (!d || n < 0) fail(CTC_E_ARG, "bad argument");
+        if (!d->session) fail(CTC_E_ARG, "no model staged on the dataset");
+        CK(cudaSetDevice(d->ctx->device));
+        d->session->epochs(n);
+    });
+}
+
+extern "C" int ctc_dataset_set_lr(ctc_dataset *d, double lr)
+{
+    return guarded([&] {
+        if (!d || !d->session) fail(CTC_E_ARG, "no model staged on the dataset");
+        d->session->set_lr(lr);
+    });
+}
+
+extern "C" int ctc_dataset_evaluate(ctc_dataset *d, ctc_epoch_stats *st)
+{
+    return guarded([&] {
+        if (!d || !st) fail(CTC_E_ARG, "null argument");
+        if (!d->session) fail(CTC_E_ARG, "no model staged on the dataset");
+        CK(cudaSetDevice(d->ctx->device));
+        memset(st, 0, sizeof(*st));
+        d->session->evaluate(st);
+    });
+}
+
+extern "C" int ctc_dataset_get_model(ctc_dataset *d, ctc_model *model)
+{
+    return guarded([&] {
+        if (!d || !d->session) fail(CTC_E_ARG, "no model staged on the dataset");
+        check_model(d, model, d->session_rank);
+        d->session->get_model(model, false);
+    });
+}
+
+extern "C" int ctc_run(ctc_ctx *ctx, const ctc_tensor *const train[3], const ctc_tensor *val,
+                       const ctc_tensor *test, ctc_model *model, ctc_model *best, const ctc_params *p,
+                       ctc_epoch_cb cb, void *user, ctc_result *res)
+{
+    ctc_dataset *ds = nullptr;
+    int rc = ctc_dataset_create(ctx, train, val, test, p, &ds);
+    if (rc != CTC_OK) return rc;
+    // the factor rows cover the tensors' index range (reference: traina
+    // dims, sgpu/completion.c:439-446); a model with more rows is fine
+    rc = guarded([&] {
+        if (!model) fail(CTC_E_ARG, "null model");
+        for (int m = 0; m < 3; ++m) {
+            if (model->dims[m] < ds->dims[m])
+                fail(CTC_E_ARG, "model mode %d has %llu rows, the tensors need %llu", m,
+                     (unsigned long long)model->dims[m], (unsigned long long)ds->dims[m]);
+            ds->dims[m] = model->dims[m];
+        }
+    });
+    if (rc == CTC_OK) rc = ctc_dataset_run(ds, model, best, p, cb, user, res);
+    ctc_dataset_free(ds);
+    return rc;
+}
+
+namespace ctc {
+template <typename T, int R>
+static double rmse_impl(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model)
+{
+    DevTensor<T> d;
+    stage_tensor<T>(ctx, t, false, d);
+    DevBuf<T> U[3];
+    for (int m = 0; m < 3; ++m) {
+        std::vector<T> h(model->U[m].begin(), model->U[m].end());
+        U[m].upload(h.data(), h.size(), ctx->stream);
+    }
+    const unsigned g = grid_for(d.n, 256, kMaxPartials);
+    LAUNCH(ctx, k::k_sse<T, R>, g, 256, 0, (const uint4 *)d.rec.p, (const double *)d.v64.p, d.n, (const T *)U[0].p,
+           (const T *)U[1].p, (const T *)U[2].p, ctx->partial.p);
+    LAUNCH(ctx, k::k_sum_partials, 1, 256, 0, (const double *)ctx->partial.p, (int)g, ctx->scalars.p);
+    double s = 0;
+    CK(cudaMemcpyAsync(&s, ctx->scalars.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return std::sqrt(s / (double)d.n);
+}
+
+template <typename T, int R>
+static void grad_impl(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double lambda,
+                      double *const *grads, double *obj)
+{
+    // mode-0-sorted copy so the mode-0 gradient rows stay in registers
+    ctc_tensor s(*t);
+    if (ctc_tensor_sort(&s, 0) != CTC_OK) fail(CTC_E_ARG, "%s", ctc_last_error());
+    DevTensor<T> d;
+    stage_tensor<T>(ctx, &s, false, d);
+    DevBuf<T> U[3], G[3];
+    for (int m = 0; m < 3; ++m) {
+        std::vector<T> h(model->U[m].begin(), model->U[m].end());
+        U[m].upload(h.data(), h.size(), ctx->stream);
+        G[m].alloc(h.size());
+        LAUNCH(ctx, k::k_scale<T>, grid_for(h.size(), 256, kSMs * 8), 256, 0, (const T *)U[m].p, G[m].p,
+               (uint64_t)h.size(), (T)(2.0 * lambda));
+    }
+    const uint32_t tl = 256;
+    const uint32_t ntiles = (d.n + tl - 1) / tl;
+    constexpr int GR = R / k::Vec<T>::n;
+    const unsigned g = grid_for(ntiles, 8 * (32 / GR), kMaxPartials);
+    LAUNCH(ctx, k::k_grad<T, R>, g, 256, 0, (const uint4 *)d.rec.p, (const double *)d.v64.p, d.n, tl, ntiles,
+           (const T *)U[0].p, (const T *)U[1].p, (const T *)U[2].p, G[0].p, G[1].p, G[2].p, ctx->partial.p);
+    LAUNCH(ctx, k::k_sum_partials, 1, 256, 0, (const double *)ctx->partial.p, (int)g, ctx->scalars.p);
+    double half_sse = 0;
+    CK(cudaMemcpyAsync(&half_sse, ctx->scalars.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    for (int m = 0; m < 3; ++m) {
+        std::vector<T> h(G[m].n);
+        CK(cudaMemcpyAsync(h.data(), G[m].p, h.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (size_t i = 0; i < h.size(); ++i) grads[m][i] = (double)h[i];
+    }
+    if (obj) {
+        double reg = 0;
+        for (int m = 0; m < 3; ++m)
+            for (double v : model->U[m]) reg += v * v;
+        *obj = half_sse + lambda * reg;
+    }
+}
+}  // namespace ctc
+
+extern "C" int ctc_rmse(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double *rmse)
+{
+    return guarded([&] {
+        if (!ctx || !t || !model || !rmse) fail(CTC_E_ARG, "null argument");
+        CK(cudaSetDevice(ctx->device));
+        validate_tensor(t, model->dims, "tensor");
+        with_rank(model->rank, [&](auto RC) {
+            constexpr int R = decltype(RC)::value;
+            *rmse = rmse_impl<float, R>(ctx, t, model);
+        });
+    });
+}
+
+extern "C" int ctc_grad(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double lambda,
+                        double *const *grads, double *obj)
+{
+    return guarded([&] {
+        if (!ctx || !t || !model || !grads) fail(CTC_E_ARG, "null argument");
+        CK(cudaSetDevice(ctx->device));
+        validate_tensor(t, model->dims, "tensor");
+        with_rank(model->rank, [&](auto RC) {
+            constexpr int R = decltype(RC)::value;
+            grad_impl<double, R>(ctx, t, model, lambda, grads, obj);
+        });
+    });
+}

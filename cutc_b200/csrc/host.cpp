@@ -1,0 +1,676 @@
+// host.cpp -- host side of libctc: errors, tensor I/O, sorting, the CISS
+// builder, reference lane multiplicities, work-tile planning, factor models.
+#include "ctc_internal.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <numeric>
+#include <parallel/algorithm>
+#include <thread>
+
+namespace ctc {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
+void fail(int code, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    throw Error(code, buf);
+}
+
+int host_threads()
+{
+    static int n = [] {
+        const char *e = getenv("CTC_HOST_THREADS");
+        int v = e ? atoi(e) : (int)std::thread::hardware_concurrency();
+        return v < 1 ? 1 : (v > 64 ? 64 : v);
+    }();
+    return n;
+}
+
+template <typename F>
+static void parallel_for(uint64_t n, F &&fn)
+{
+    int P = host_threads();
+    if (n < 65536 || P == 1) {
+        fn(0, 0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int p = 0; p < P; ++p) {
+        uint64_t b = n * p / P, e = n * (p + 1) / P;
+        th.emplace_back([&, p, b, e] { fn(p, b, e); });
+    }
+    for (auto &t : th) t.join();
+}
+
+// ------------------------------------------------------------------
+// .tns text reader
+// ------------------------------------------------------------------
+
+// Restates sgpu/io.c:234-308 (tt_get_dims) + io.c:58-106 (p_tt_read_file):
+// the mode count comes from the first data line split on " \t" (the value
+// token and the trailing newline token excluded), a data line is one whose
+// getline() length exceeds 1 and that does not start with '#', indices are
+// strtoul base 10 (kept as read), values strtod.  The file is parsed in
+// parallel over line-aligned chunks.
+static void read_tns(const char *path, ctc_tensor &t)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) fail(CTC_E_IO, "cannot open '%s'", path);
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    std::vector<char> buf((size_t)sz + 1);
+    if (sz > 0 && fread(buf.data(), 1, (size_t)sz, f) != (size_t)sz) {
+        fclose(f);
+        fail(CTC_E_IO, "short read on '%s'", path);
+    }
+    fclose(f);
+    buf[(size_t)sz] = '\0';
+    char *data = buf.data();
+    const size_t N = (size_t)sz;
+
+    // mode count from the first data line (reference counts strtok tokens
+    // on " \t", where the last token carries the newline, then subtracts 1)
+    int nmodes = -1;
+    {
+        size_t p = 0;
+        while (p < N) {
+            size_t e = p;
+            while (e < N && data[e] != '\n') ++e;
+            size_t len = e - p + (e < N ? 1 : 0);
+            if (len > 1 && data[p] != '#') {
+                std::string line(data + p, data + e + (e < N ? 1 : 0));
+                int ntok = 0;
+                char *save = nullptr;
+                for (char *tok = strtok_r(&line[0], " \t", &save); tok;
+                     tok = strtok_r(nullptr, " \t", &save))
+                    ++ntok;
+                nmodes = ntok - 1;
+                break;
+            }
+            p = e + 1;
+        }
+    }
+    if (nmodes < 1 || nmodes > 4) fail(CTC_E_IO, "'%s': cannot determine the number of modes", path);
+
+    // line-aligned chunks
+    int P = host_threads();
+    if (N < (1u << 20)) P = 1;
+    std::vector<size_t> cut(P + 1, 0);
+    cut[P] = N;
+    for (int p = 1; p < P; ++p) {
+        size_t c = N * p / P;
+        while (c < N && data[c - 1] != '\n') ++c;
+        cut[p] = std::max(c, cut[p - 1]);
+    }
+    // NUL-terminate lines so a short line cannot run into the next one
+    for (size_t i = 0; i < N; ++i)
+        if (data[i] == '\n') data[i] = '\0';
+
+    auto is_data = [&](size_t p, size_t e) {
+        size_t len = e - p + (e < N ? 1 : 0);
+        return len > 1 && data[p] != '#';
+    };
+    std::vector<uint64_t> count(P, 0);
+    std::vector<std::thread> th;
+    for (int p = 0; p < P; ++p)
+        th.emplace_back([&, p] {
+            uint64_t c = 0;
+            size_t q = cut[p];
+            while (q < cut[p + 1]) {
+                size_t e = q;
+                while (e < N && data[e] != '\0') ++e;
+                if (is_data(q, e)) ++c;
+                q = e + 1;
+            }
+            count[p] = c;
+        });
+    for (auto &x : th) x.join();
+    th.clear();
+    std::vector<uint64_t> off(P + 1, 0);
+    for (int p = 0; p < P; ++p) off[p + 1] = off[p] + count[p];
+    const uint64_t nnz = off[P];
+
+    t.nmodes = nmodes;
+    t.nnz = nnz;
+    for (int m = 0; m < nmodes; ++m) t.ind[m].assign(nnz, 0);
+    t.vals.assign(nnz, 0.0);
+    std::vector<uint64_t> mx((size_t)P * 4, 0), mn((size_t)P * 4, 1);
+    for (int p = 0; p < P; ++p)
+        th.emplace_back([&, p] {
+            uint64_t n = off[p];
+            size_t q = cut[p];
+            while (q < cut[p + 1]) {
+                size_t e = q;
+                while (e < N && data[e] != '\0') ++e;
+                if (is_data(q, e)) {
+                    char *ptr = data + q;
+                    for (int m = 0; m < nmodes; ++m) {
+                        uint64_t v = strtoul(ptr, &ptr, 10);
+                        t.ind[m][n] = v;
+                        if (v > mx[p * 4 + m]) mx[p * 4 + m] = v;
+                        if (v < mn[p * 4 + m]) mn[p * 4 + m] = v;
+                    }
+                    t.vals[n] = strtod(ptr, &ptr);
+                    ++n;
+                }
+                q = e + 1;
+            }
+        });
+    for (auto &x : th) x.join();
+    for (int m = 0; m < nmodes; ++m) {
+        uint64_t d = 0, o = 1;
+        for (int p = 0; p < P; ++p) {
+            d = std::max(d, mx[p * 4 + m]);
+            o = std::min(o, mn[p * 4 + m]);
+        }
+        t.dims[m] = d + (o == 0 ? 1 : 0);
+    }
+}
+
+static const char kMagic[4] = {'C', 'T', 'C', 'B'};
+
+static void read_bin(const char *path, ctc_tensor &t)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) fail(CTC_E_IO, "cannot open '%s'", path);
+    char mg[4];
+    uint32_t ver = 0, nm = 0;
+    uint64_t nnz = 0;
+    bool ok = fread(mg, 1, 4, f) == 4 && memcmp(mg, kMagic, 4) == 0 &&
+              fread(&ver, 4, 1, f) == 1 && ver == 1 && fread(&nm, 4, 1, f) == 1 &&
+              nm >= 1 && nm <= 4 && fread(&nnz, 8, 1, f) == 1;
+    if (ok) {
+        t.nmodes = (int)nm;
+        t.nnz = nnz;
+        ok = fread(t.dims, 8, nm, f) == nm;
+        for (uint32_t m = 0; ok && m < nm; ++m) {
+            t.ind[m].resize(nnz);
+            ok = fread(t.ind[m].data(), 8, nnz, f) == nnz;
+        }
+        if (ok) {
+            t.vals.resize(nnz);
+            ok = fread(t.vals.data(), 8, nnz, f) == nnz;
+        }
+    }
+    fclose(f);
+    if (!ok) fail(CTC_E_IO, "'%s' is not a valid CTCB tensor file", path);
+}
+
+// ------------------------------------------------------------------
+// CISS builder
+// ------------------------------------------------------------------
+
+// The value store of the reference CISS goes through an idx_t
+// (sgpu/ciss.c:163 "tmpv = newtensor->vals[m]"): restated as the x86-64
+// conversion sequence (signed truncation below 2^63, offset + bit flip
+// above, 0x8000000000000000 for NaN and out-of-range).
+static uint64_t value_through_idx(double v)
+{
+    const double two63 = 9223372036854775808.0;
+    if (std::isnan(v)) return 0x8000000000000000ULL;
+    if (v < two63) {
+        if (v < -two63) return 0x8000000000000000ULL;
+        return (uint64_t)(int64_t)v;
+    }
+    double w = v - two63;
+    uint64_t r = (w < two63) ? (uint64_t)(int64_t)w : 0x8000000000000000ULL;
+    return r ^ 0x8000000000000000ULL;
+}
+
+}  // namespace ctc
+
+double ctc_value_through_idx(double v) { return (double)ctc::value_through_idx(v); }
+
+namespace ctc {
+
+// sgpu/ciss.c:68-195 / ga/ciss.c:69-212 with a runtime tile length.
+static void build_ciss(const ctc_tensor &t, int mode, int T, bool ga, ctc_ciss &c)
+{
+    if (t.nmodes != 3) fail(CTC_E_UNSUP, "CISS needs an order-3 tensor (got %d)", t.nmodes);
+    if (t.nnz == 0) fail(CTC_E_ARG, "CISS of an empty tensor");
+    if (T < 1 || T > 64) fail(CTC_E_ARG, "tile length %d outside [1, 64]", T);
+    if (mode < 0 || mode > 2) fail(CTC_E_ARG, "mode %d outside [0, 2]", mode);
+    const uint64_t nnz = t.nnz;
+    const uint64_t *im = t.ind[mode].data();
+    const uint64_t *ij = t.ind[(mode + 1) % 3].data();
+    const uint64_t *ik = t.ind[(mode + 2) % 3].data();
+    // directory: distinct mode indices in order of appearance (ciss.c:89-115)
+    std::vector<uint64_t> dir;
+    dir.reserve(1024);
+    dir.push_back(im[0]);
+    for (uint64_t m = 1; m < nnz; ++m)
+        if (im[m] != dir.back()) dir.push_back(im[m]);
+    // dcounter[0] = 0 and dcounter[k] = start(slice k) - 1, the inclusive end
+    // of slice k-1, which is what the reference's running counter
+    // (ciss.c:97-114) accumulates; the last slot is nnz-1 (ciss.c:110).
+    c.dlength = dir.size();
+    c.directory = dir;
+    c.dcounter.assign(c.dlength + 1, 0);
+    {
+        uint64_t k = 0;
+        for (uint64_t m = 1; m < nnz; ++m)
+            if (im[m] != im[m - 1]) c.dcounter[++k] = ga ? m : m - 1;
+        // ga/ciss.c:101-120 starts its running count at the first nonzero,
+        // so there the counters are one larger: dcounter[k] = start(slice k)
+        c.dcounter[c.dlength] = nnz - 1;
+    }
+    c.nnz = nnz;
+    c.tile_len = T;
+    const uint64_t tilesize = nnz / (uint64_t)T + 1;
+    c.size_rows = tilesize + nnz + 1;
+    const uint64_t cap = c.size_rows * 3;
+    c.entries.assign(cap, 0.0);
+    c.written.assign(cap, 0);
+    double *E = c.entries.data();
+    uint8_t *Wr = c.written.data();
+    uint64_t npos = 0, nl = 0, m = 0;
+    auto put = [&](uint64_t off, double v) {
+        uint64_t o = npos + off;
+        if (o >= cap) fail(CTC_E_ARG, "CISS layout overflow");
+        E[o] = v;
+        Wr[o] = 1;
+    };
+    while (m < nnz + 1) {
+        uint64_t bitmap = 1;
+        uint64_t ns = nl;
+        uint64_t niv = dir[ns];
+        uint64_t lc = 1;
+        put(0, -1.0 * (double)ns);
+        while (lc <= (uint64_t)T) {
+            if (m == nnz) {
+                put(lc * 3, -1.0);
+                put(lc * 3 + 1, -1.0);
+                put(lc * 3 + 2, -1.0);
+                m++;
+                break;
+            }
+            uint64_t ti = im[m];
+            if (ti == niv) {
+                bitmap = (bitmap << 1) + 1;
+            } else {
+                bitmap = bitmap << 1;
+                niv = ti;
+                nl++;
+                put(1, -1.0 * (double)nl);
+            }
+            put(lc * 3, (double)ij[m]);
+            put(lc * 3 + 1, (double)ik[m]);
+            put(lc * 3 + 2, (double)value_through_idx(t.vals[m]));
+            put(2, (double)bitmap);
+            m++;
+            lc++;
+        }
+        npos += ((uint64_t)T + 1) * 3;
+    }
+}
+
+static uint64_t brev64(uint64_t x)
+{
+    x = ((x >> 1) & 0x5555555555555555ULL) | ((x & 0x5555555555555555ULL) << 1);
+    x = ((x >> 2) & 0x3333333333333333ULL) | ((x & 0x3333333333333333ULL) << 2);
+    x = ((x >> 4) & 0x0F0F0F0F0F0F0F0FULL) | ((x & 0x0F0F0F0F0F0F0F0FULL) << 4);
+    x = ((x >> 8) & 0x00FF00FF00FF00FFULL) | ((x & 0x00FF00FF00FF00FFULL) << 8);
+    x = ((x >> 16) & 0x0000FFFF0000FFFFULL) | ((x & 0x0000FFFF0000FFFFULL) << 16);
+    return (x >> 32) | (x << 32);
+}
+
+// Multiplicity with which the reference's warp kernels (sgpu/als.cu:227-312
+// for ALS, kernel 0; sgpu/ccd.cu:120-200 for CCD, kernel 1) add each
+// nonzero of a 32-long CISS tile into its row: the tile's first row segment
+// is never written (lane 0 has mybit forced to 1), a segment ending at lane
+// 31 gets K-(31-h) extra copies of lane 31 (shfl_down there returns the
+// lane's own value; K = continuation bits of the tile, h = segment head),
+// and the CCD kernel's grid reaches only tiles < 8*(tilenum/256+1)
+// (sgpu/ccd.cu:520).  In a partial last tile the reference reads an
+// inactive lane (undefined); here the inactive lanes count as new rows.
+void compat_weights(const ctc_ciss &c, int kernel, std::vector<double> &w)
+{
+    if (c.tile_len != 32) fail(CTC_E_ARG, "compat multiplicities need tile length 32");
+    const uint64_t nnz = c.nnz, tilenum = nnz / 32 + 1;
+    uint64_t covered = tilenum;
+    if (kernel == 1) covered = std::min<uint64_t>(tilenum, 8 * (tilenum / 256 + 1));
+    w.assign(nnz, 0.0);
+    for (uint64_t tile = 0; tile < covered; ++tile) {
+        const uint64_t first = tile * 32;
+        if (first >= nnz) break;
+        const int active = (int)std::min<uint64_t>(32, nnz - first);
+        uint64_t B = (uint64_t)c.entries[tile * 33 * 3 + 2];
+        if (B == 0) continue;
+        uint64_t b = brev64(B);
+        while ((b & 1) == 0) b >>= 1;
+        b >>= 1;
+        const int K = __builtin_popcountll(b) - (int)(b & 1);
+        int h = -1;
+        for (int l = 0; l <= active; ++l) {
+            bool head = (l == active) || (l > 0 && ((b >> l) & 1) == 0);
+            if (!head) continue;
+            if (h >= 1) {
+                int e = l - 1;
+                for (int q = h; q <= e; ++q) w[first + q] = 1.0;
+                if (e == 31 && h < 31) w[first + 31] += (double)(K - (31 - h));
+            }
+            h = l;
+        }
+    }
+}
+
+// ------------------------------------------------------------------
+// work tiles
+// ------------------------------------------------------------------
+TilePlan plan_tiles(const uint32_t *rows, uint64_t n, uint32_t T)
+{
+    TilePlan p;
+    p.tiles.reserve((size_t)(n / std::max<uint32_t>(T / 2, 1) + 16) * 4);
+    uint64_t i = 0;
+    while (i < n) {
+        uint64_t e = i + 1;
+        while (e < n && rows[e] == rows[i]) ++e;
+        uint64_t len = e - i;
+        if (len > T) {
+            uint32_t h = p.nheavy();
+            uint32_t first = p.ntiles();
+            uint32_t np = (uint32_t)((len + T - 1) / T);
+            for (uint32_t q = 0; q < np; ++q) {
+                uint64_t s = i + (uint64_t)q * T;
+                p.tiles.insert(p.tiles.end(),
+                               {(int32_t)s, (int32_t)std::min<uint64_t>(T, e - s), (int32_t)h, (int32_t)q});
+            }
+            p.heavy_rows.insert(p.heavy_rows.end(), {rows[i], first, np, 0u});
+            i = e;
+            continue;
+        }
+        // pack whole light rows
+        uint64_t s = i, size = 0;
+        while (i < n) {
+            uint64_t ee = i + 1;
+            while (ee < n && rows[ee] == rows[i]) ++ee;
+            uint64_t l = ee - i;
+            if (l > T || size + l > T) break;
+            size += l;
+            i = ee;
+        }
+        p.tiles.insert(p.tiles.end(), {(int32_t)s, (int32_t)size, -1, 0});
+    }
+    return p;
+}
+
+// counter-based uniform in [0,1): splitmix64 of (seed, mode, row, col)
+static inline double u01(uint64_t seed, uint64_t mode, uint64_t row, uint64_t col)
+{
+    uint64_t z = seed ^ (mode * 0x9E3779B97F4A7C15ULL) ^ (row * 0xBF58476D1CE4E5B9ULL) ^
+                 (col * 0x94D049BB133111EBULL);
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+}  // namespace ctc
+
+using namespace ctc;
+
+// ------------------------------------------------------------------
+// C ABI: errors, tensors, CISS, models
+// ------------------------------------------------------------------
+extern "C" const char *ctc_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *ctc_version(void) { return "ctc 0.1 (sm_100a)"; }
+
+extern "C" int ctc_tensor_load_tns(const char *path, ctc_tensor **out)
+{
+    return guarded([&] {
+        if (!path || !out) fail(CTC_E_ARG, "null argument");
+        auto t = new ctc_tensor();
+        try {
+            size_t L = strlen(path);
+            if (L > 5 && strcmp(path + L - 5, ".ctcb") == 0) read_bin(path, *t);
+            else read_tns(path, *t);
+        } catch (...) {
+            delete t;
+            throw;
+        }
+        *out = t;
+    });
+}
+
+extern "C" int ctc_tensor_save_bin(const ctc_tensor *t, const char *path)
+{
+    return guarded([&] {
+        if (!t || !path) fail(CTC_E_ARG, "null argument");
+        FILE *f = fopen(path, "wb");
+        if (!f) fail(CTC_E_IO, "cannot create '%s'", path);
+        uint32_t ver = 1, nm = (uint32_t)t->nmodes;
+        bool ok = fwrite(kMagic, 1, 4, f) == 4 && fwrite(&ver, 4, 1, f) == 1 &&
+                  fwrite(&nm, 4, 1, f) == 1 && fwrite(&t->nnz, 8, 1, f) == 1 &&
+                  fwrite(t->dims, 8, nm, f) == nm;
+        for (uint32_t m = 0; ok && m < nm; ++m)
+            ok = fwrite(t->ind[m].data(), 8, t->nnz, f) == t->nnz;
+        if (ok) ok = fwrite(t->vals.data(), 8, t->nnz, f) == t->nnz;
+        if (fclose(f) != 0) ok = false;
+        if (!ok) fail(CTC_E_IO, "write to '%s' failed", path);
+    });
+}
+
+extern "C" int ctc_tensor_from_coo(int nmodes, uint64_t nnz, const uint64_t *dims,
+                                   const uint64_t *const *ind, const double *vals,
+                                   ctc_tensor **out)
+{
+    return guarded([&] {
+        if (nmodes < 1 || nmodes > 4 || !ind || !vals || !out) fail(CTC_E_ARG, "bad arguments");
+        auto t = new ctc_tensor();
+        t->nmodes = nmodes;
+        t->nnz = nnz;
+        for (int m = 0; m < nmodes; ++m) {
+            t->ind[m].assign(ind[m], ind[m] + nnz);
+            uint64_t mx = 0;
+            bool zero = false;
+            for (uint64_t n = 0; n < nnz; ++n) {
+                mx = std::max(mx, ind[m][n]);
+                zero |= ind[m][n] == 0;
+            }
+            t->dims[m] = dims ? dims[m] : mx + (zero ? 1 : 0);
+        }
+        t->vals.assign(vals, vals + nnz);
+        *out = t;
+    });
+}
+
+extern "C" int ctc_tensor_info(const ctc_tensor *t, int *nmodes, uint64_t *nnz, uint64_t *dims)
+{
+    return guarded([&] {
+        if (!t) fail(CTC_E_ARG, "null tensor");
+        if (nmodes) *nmodes = t->nmodes;
+        if (nnz) *nnz = t->nnz;
+        if (dims)
+            for (int m = 0; m < t->nmodes; ++m) dims[m] = t->dims[m];
+    });
+}
+
+extern "C" int ctc_tensor_export(const ctc_tensor *t, uint64_t *const *ind, double *vals)
+{
+    return guarded([&] {
+        if (!t) fail(CTC_E_ARG, "null tensor");
+        if (ind)
+            for (int m = 0; m < t->nmodes; ++m)
+                if (ind[m]) memcpy(ind[m], t->ind[m].data(), t->nnz * 8);
+        if (vals) memcpy(vals, t->vals.data(), t->nnz * 8);
+    });
+}
+
+extern "C" int ctc_tensor_sort(ctc_tensor *t, int mode)
+{
+    return guarded([&] {
+        if (!t || mode < 0 || mode >= t->nmodes) fail(CTC_E_ARG, "bad sort mode");
+        const uint64_t n = t->nnz;
+        const uint64_t *k1 = t->ind[mode].data();
+        const uint64_t *k2 = t->ind[(mode + 1) % t->nmodes].data();
+        std::vector<uint64_t> perm(n);
+        std::iota(perm.begin(), perm.end(), 0);
+        __gnu_parallel::stable_sort(perm.begin(), perm.end(), [&](uint64_t a, uint64_t b) {
+            return k1[a] < k1[b] || (k1[a] == k1[b] && k2[a] < k2[b]);
+        });
+        std::vector<uint64_t> tmp(n);
+        for (int m = 0; m < t->nmodes; ++m) {
+            const uint64_t *src = t->ind[m].data();
+            parallel_for(n, [&](int, uint64_t b, uint64_t e) {
+                for (uint64_t i = b; i < e; ++i) tmp[i] = src[perm[i]];
+            });
+            t->ind[m].swap(tmp);
+            tmp.resize(n);
+        }
+        std::vector<double> tv(n);
+        parallel_for(n, [&](int, uint64_t b, uint64_t e) {
+            for (uint64_t i = b; i < e; ++i) tv[i] = t->vals[perm[i]];
+        });
+        t->vals.swap(tv);
+    });
+}
+
+extern "C" int ctc_tensor_free(ctc_tensor *t)
+{
+    delete t;
+    return CTC_OK;
+}
+
+extern "C" int ctc_ciss_build(const ctc_tensor *t, int mode, int tile_len, ctc_ciss **out)
+{
+    return guarded([&] {
+        if (!t || !out) fail(CTC_E_ARG, "null argument");
+        auto c = new ctc_ciss();
+        try {
+            build_ciss(*t, mode - 1, tile_len, false, *c);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+extern "C" int ctc_ciss_build_ga(const ctc_tensor *t, int mode, int tile_len, ctc_ciss **out)
+{
+    return guarded([&] {
+        if (!t || !out) fail(CTC_E_ARG, "null argument");
+        auto c = new ctc_ciss();
+        try {
+            build_ciss(*t, mode - 1, tile_len, true, *c);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+extern "C" int ctc_ciss_sizes(const ctc_ciss *c, uint64_t *nnz, uint64_t *dlength,
+                              uint64_t *size_rows, int *tile_len)
+{
+    return guarded([&] {
+        if (!c) fail(CTC_E_ARG, "null CISS");
+        if (nnz) *nnz = c->nnz;
+        if (dlength) *dlength = c->dlength;
+        if (size_rows) *size_rows = c->size_rows;
+        if (tile_len) *tile_len = c->tile_len;
+    });
+}
+
+extern "C" int ctc_ciss_export(const ctc_ciss *c, uint64_t *directory, uint64_t *dcounter,
+                               double *entries, uint8_t *written)
+{
+    return guarded([&] {
+        if (!c) fail(CTC_E_ARG, "null CISS");
+        if (directory) memcpy(directory, c->directory.data(), c->dlength * 8);
+        if (dcounter) memcpy(dcounter, c->dcounter.data(), (c->dlength + 1) * 8);
+        if (entries) memcpy(entries, c->entries.data(), c->size_rows * 3 * 8);
+        if (written) memcpy(written, c->written.data(), c->size_rows * 3);
+    });
+}
+
+extern "C" int ctc_ciss_free(ctc_ciss *c)
+{
+    delete c;
+    return CTC_OK;
+}
+
+extern "C" int ctc_model_create(int nmodes, const uint64_t *dims, int rank, ctc_model **out)
+{
+    return guarded([&] {
+        if (nmodes < 1 || nmodes > 4 || !dims || rank < 1 || !out) fail(CTC_E_ARG, "bad model shape");
+        auto m = new ctc_model();
+        m->nmodes = nmodes;
+        m->rank = rank;
+        for (int q = 0; q < nmodes; ++q) {
+            m->dims[q] = dims[q];
+            m->U[q].assign(dims[q] * (uint64_t)rank, 0.0);
+        }
+        *out = m;
+    });
+}
+
+extern "C" int ctc_model_init_uniform(ctc_model *m, uint64_t seed, double scale)
+{
+    return guarded([&] {
+        if (!m) fail(CTC_E_ARG, "null model");
+        for (int q = 0; q < m->nmodes; ++q) {
+            const uint64_t R = (uint64_t)m->rank;
+            double *U = m->U[q].data();
+            parallel_for(m->dims[q], [&](int, uint64_t b, uint64_t e) {
+                for (uint64_t r = b; r < e; ++r)
+                    for (uint64_t f = 0; f < R; ++f) U[r * R + f] = u01(seed, (uint64_t)q, r, f) * scale;
+            });
+        }
+    });
+}
+
+extern "C" int ctc_model_set(ctc_model *m, int mode, const double *rowmajor)
+{
+    return guarded([&] {
+        if (!m || mode < 0 || mode >= m->nmodes || !rowmajor) fail(CTC_E_ARG, "bad argument");
+        memcpy(m->U[mode].data(), rowmajor, m->U[mode].size() * 8);
+    });
+}
+
+extern "C" int ctc_model_get(const ctc_model *m, int mode, double *rowmajor)
+{
+    return guarded([&] {
+        if (!m || mode < 0 || mode >= m->nmodes || !rowmajor) fail(CTC_E_ARG, "bad argument");
+        memcpy(rowmajor, m->U[mode].data(), m->U[mode].size() * 8);
+    });
+}
+
+extern "C" int ctc_model_copy(const ctc_model *src, ctc_model *dst)
+{
+    return guarded([&] {
+        if (!src || !dst) fail(CTC_E_ARG, "null model");
+        *dst = *src;
+    });
+}
+
+extern "C" int ctc_model_info(const ctc_model *m, int *nmodes, uint64_t *dims, int *rank)
+{
+    return guarded([&] {
+        if (!m) fail(CTC_E_ARG, "null model");
+        if (nmodes) *nmodes = m->nmodes;
+        if (rank) *rank = m->rank;
+        if (dims)
+            for (int q = 0; q < m->nmodes; ++q) dims[q] = m->dims[q];
+    });
+}
+
+extern "C" int ctc_model_free(ctc_model *m)
+{
+    delete m;
+    return CTC_OK;
+}

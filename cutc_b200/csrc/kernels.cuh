@@ -1,0 +1,855 @@
+// kernels.cuh -- sm_100a kernels of the completion engine.
+//
+// Data layout in HBM (one copy of the training nonzeros per mode, sorted
+// for that mode, the order of the reference's traina/b/c files):
+//   rec[n]  : uint4 {i0, i1, i2, value bits}  -- 16 B, one 128-bit load per
+//             nonzero; indices 0-based; the value is FP32 (in FP64 runs it
+//             lives in v64[n] instead, and CCD++ keeps its residual there)
+//   tiles[t]: int4 {start, len, heavy, piece}  -- row-aligned work tiles:
+//             whole rows packed to <= tile_len nonzeros (heavy = -1), or one
+//             tile_len piece of a longer row (heavy = its heavy-row id)
+//   heavy[h]: uint4 {row, first_tile, ntiles, 0}
+// A warp owns a tile: rows inside a light tile are reduced and finalised by
+// that warp alone (no atomics); pieces of heavy rows write per-tile partials
+// that a fixup kernel sums in piece order (deterministic).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ctc {
+namespace k {
+
+constexpr uint32_t kNoKey = 0xffffffffu;
+
+template <typename T>
+struct Vec;
+template <>
+struct Vec<float> {
+    using type = float4;
+    static constexpr int n = 4;
+};
+template <>
+struct Vec<double> {
+    using type = double2;
+    static constexpr int n = 2;
+};
+
+__device__ __forceinline__ float vget(const float4 &v, int i)
+{
+    return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ double vget(const double2 &v, int i) { return i == 0 ? v.x : v.y; }
+__device__ __forceinline__ void vset(float4 &v, int i, float x)
+{
+    if (i == 0) v.x = x;
+    else if (i == 1) v.y = x;
+    else if (i == 2) v.z = x;
+    else v.w = x;
+}
+__device__ __forceinline__ void vset(double2 &v, int i, double x)
+{
+    if (i == 0) v.x = x;
+    else v.y = x;
+}
+
+__device__ __forceinline__ uint32_t key_of(const uint4 &r, int m)
+{
+    return m == 0 ? r.x : (m == 1 ? r.y : r.z);
+}
+
+template <typename T>
+__device__ __forceinline__ T value_of(const uint4 &r, const double *v64, uint64_t n)
+{
+    if constexpr (sizeof(T) == 8) return v64[n];
+    else return __uint_as_float(r.w);
+}
+
+template <typename T>
+__device__ __forceinline__ void store_value(uint4 *rec, double *v64, uint64_t n, T v)
+{
+    if constexpr (sizeof(T) == 8) v64[n] = v;
+    else rec[n].w = __float_as_uint(v);
+}
+
+__device__ __forceinline__ void vatomic_add(float4 *p, const float4 &d) { atomicAdd(p, d); }
+__device__ __forceinline__ void vatomic_add(double2 *p, const double2 &d)
+{
+    atomicAdd(&p->x, d.x);
+    atomicAdd(&p->y, d.y);
+}
+
+// Block-wide double sum; result valid in thread 0.
+__device__ __forceinline__ double block_sum(double v)
+{
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        v = (l < nw) ? red[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+// ---------------------------------------------------------------------
+// Squared error (the residual/RMSE kernel).  Thread per nonzero, rows of
+// the row-major factors read with 16-byte vector loads.  Per-block double
+// partials; k_sum_partials folds them in a fixed order.
+// ---------------------------------------------------------------------
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_sse(const uint4 *__restrict__ rec,
+                                             const double *__restrict__ v64, uint32_t n,
+                                             const T *__restrict__ U0, const T *__restrict__ U1,
+                                             const T *__restrict__ U2, double *__restrict__ partial)
+{
+    using V = typename Vec<T>::type;
+    constexpr int VN = Vec<T>::n;
+    double acc = 0;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        const uint4 r = rec[idx];
+        const T x = value_of<T>(r, v64, idx);
+        const V *a = reinterpret_cast<const V *>(U0 + (size_t)r.x * R);
+        const V *b = reinterpret_cast<const V *>(U1 + (size_t)r.y * R);
+        const V *c = reinterpret_cast<const V *>(U2 + (size_t)r.z * R);
+        T p = 0;
+#pragma unroll
+        for (int q = 0; q < R / VN; ++q) {
+            const V va = a[q], vb = b[q], vc = c[q];
+#pragma unroll
+            for (int v = 0; v < VN; ++v) p += vget(va, v) * vget(vb, v) * vget(vc, v);
+        }
+        const T e = x - p;
+        acc += (double)e * (double)e;
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+// Sum of squares of a dense array (for lambda * ||U||^2).
+template <typename T>
+__global__ void __launch_bounds__(256) k_sumsq(const T *__restrict__ x, uint64_t n,
+                                               double *__restrict__ partial)
+{
+    double acc = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        acc += (double)x[i] * (double)x[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+// out[slot] = sum of partial[0..n) in a fixed order (one block).
+__global__ void __launch_bounds__(256) k_sum_partials(const double *__restrict__ partial, int n,
+                                                      double *__restrict__ out)
+{
+    double acc = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) *out = acc;
+}
+
+// ---------------------------------------------------------------------
+// SGD (sgpu/sgd.cu:21-143 rule).  A group of G = R/VN lanes handles one
+// tile of consecutive mode-0-sorted nonzeros in order; each lane holds a
+// 16-byte slice of the three rows.  The mode-0 row stays in registers while
+// the row does not change (exact for a sequential order) and is flushed as
+// a delta (atomic) or a store (plain) when it does.
+//   e = x - sum a.b.c ;  a += s*((e*b*c) - lambda*a) ; b, c likewise from
+//   the pre-update rows, s = lr * step scale.
+// sequential != 0: one group walks all tiles in order (deterministic).
+// ---------------------------------------------------------------------
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
+                                             const double *__restrict__ v64, uint32_t n,
+                                             uint32_t tile_len, uint32_t ntiles, T *U0, T *U1,
+                                             T *U2, const T *__restrict__ lr_dev, T lambda,
+                                             int atomic, int sequential)
+{
+    using V = typename Vec<T>::type;
+    constexpr int VN = Vec<T>::n;
+    constexpr int G = R / VN;
+    static_assert(G >= 1 && G <= 32 && (32 % G) == 0, "unsupported rank");
+    constexpr int GPW = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;
+    const int gw = lane / G;
+    const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (gw * G));
+    uint64_t group = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * GPW + gw;
+    uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x >> 5) * GPW;
+    if (sequential) {
+        if (group != 0) return;
+        ngroups = 1;
+    }
+    const T s = *lr_dev;
+    for (uint64_t tile = group; tile < ntiles; tile += ngroups) {
+        const uint64_t start = tile * tile_len;
+        const uint64_t end = min(start + tile_len, (uint64_t)n);
+        uint32_t cur = kNoKey;
+        V a, a0;
+        V *arow = nullptr;
+        for (uint64_t p = start; p < end; ++p) {
+            const uint4 r = rec[p];
+            const T x = value_of<T>(r, v64, p);
+            if (r.x != cur) {
+                if (arow) {
+                    if (atomic) {
+                        V d;
+#pragma unroll
+                        for (int v = 0; v < VN; ++v) vset(d, v, vget(a, v) - vget(a0, v));
+                        vatomic_add(arow, d);
+                    } else {
+                        *arow = a;
+                    }
+                }
+                cur = r.x;
+                arow = reinterpret_cast<V *>(U0 + (size_t)r.x * R) + gl;
+                a = *arow;
+                a0 = a;
+            }
+            V *brow = reinterpret_cast<V *>(U1 + (size_t)r.y * R) + gl;
+            V *crow = reinterpret_cast<V *>(U2 + (size_t)r.z * R) + gl;
+            const V b = *brow, c = *crow;
+            T part = 0;
+#pragma unroll
+            for (int v = 0; v < VN; ++v) part += vget(a, v) * vget(b, v) * vget(c, v);
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) part += __shfl_xor_sync(gmask, part, o);
+            const T e = x - part;
+            V an, db, dc;
+#pragma unroll
+            for (int v = 0; v < VN; ++v) {
+                const T av = vget(a, v), bv = vget(b, v), cv = vget(c, v);
+                vset(an, v, av + s * ((e * bv * cv) - lambda * av));
+                vset(db, v, s * ((e * av * cv) - lambda * bv));
+                vset(dc, v, s * ((e * bv * av) - lambda * cv));
+            }
+            if (atomic) {
+                vatomic_add(brow, db);
+                vatomic_add(crow, dc);
+            } else {
+                V bn, cn;
+#pragma unroll
+                for (int v = 0; v < VN; ++v) {
+                    vset(bn, v, vget(b, v) + vget(db, v));
+                    vset(cn, v, vget(c, v) + vget(dc, v));
+                }
+                *brow = bn;
+                *crow = cn;
+            }
+            a = an;
+        }
+        if (arow) {
+            if (atomic) {
+                V d;
+#pragma unroll
+                for (int v = 0; v < VN; ++v) vset(d, v, vget(a, v) - vget(a0, v));
+                vatomic_add(arow, d);
+            } else {
+                *arow = a;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------
+// CCD++ column pass for mode m, column f (column-major factors).  Lane per
+// nonzero, 32 at a time through the tile; per-row sums of r*h and h*h by a
+// segmented warp scan on the (sorted) row keys, carried across sub-tiles;
+// the row's warp writes u = num / (lambda + den).  FIRST: the pass also
+// refreshes the stored residual of this copy:
+//   r <- r - term(fprev, final) + term(f, snapshot before this column).
+// ---------------------------------------------------------------------
+struct CcdCols {
+    const void *cur[3];   // column f, current values
+    const void *prev[3];  // column fprev (final) or null
+    const void *old[3];   // snapshot of column f before its sweeps
+    void *out;            // column f of mode m
+};
+
+template <typename T>
+__device__ __forceinline__ T term3(const void *const *c, const uint4 &r)
+{
+    return static_cast<const T *>(c[0])[r.x] * static_cast<const T *>(c[1])[r.y] *
+           static_cast<const T *>(c[2])[r.z];
+}
+
+template <typename T, bool FIRST>
+__global__ void __launch_bounds__(256) k_ccd_pass(const int4 *__restrict__ tiles, uint32_t ntiles,
+                                                  uint4 *rec, double *v64, int m, CcdCols cols,
+                                                  T lambda, T *__restrict__ slot_nu,
+                                                  T *__restrict__ slot_de)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+    const T *h1 = static_cast<const T *>(cols.cur[m1]);
+    const T *h2 = static_cast<const T *>(cols.cur[m2]);
+    T *out = static_cast<T *>(cols.out);
+    for (uint64_t tile = warp; tile < ntiles; tile += nwarps) {
+        const int4 td = tiles[tile];
+        const uint32_t start = (uint32_t)td.x, end = (uint32_t)td.x + (uint32_t)td.y;
+        const bool heavy = td.z >= 0;
+        uint32_t ckey = kNoKey;
+        T cnu = 0, cde = 0;
+        for (uint32_t base = start; base < end; base += 32) {
+            const uint32_t idx = base + lane;
+            const bool valid = idx < end;
+            uint32_t key = kNoKey - 1;
+            T nu = 0, de = 0;
+            if (valid) {
+                uint4 r = rec[idx];
+                key = key_of(r, m);
+                T res = value_of<T>(r, v64, idx);
+                if constexpr (FIRST) {
+                    if (cols.prev[0]) res -= term3<T>(cols.prev, r);
+                    res += term3<T>(cols.old, r);
+                    store_value<T>(rec, v64, idx, res);
+                }
+                const uint32_t q1 = key_of(r, m1), q2 = key_of(r, m2);
+                const T h = h1[q1] * h2[q2];
+                nu = res * h;
+                de = h * h;
+            }
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t k2 = __shfl_up_sync(0xffffffffu, key, d);
+                const T n2 = __shfl_up_sync(0xffffffffu, nu, d);
+                const T d2 = __shfl_up_sync(0xffffffffu, de, d);
+                if (lane >= d && k2 == key) {
+                    nu += n2;
+                    de += d2;
+                }
+            }
+            if (key == ckey) {
+                nu += cnu;
+                de += cde;
+            }
+            uint32_t nkey = __shfl_down_sync(0xffffffffu, key, 1);
+            if (lane == 31) nkey = (base + 32 < end) ? key_of(rec[base + 32], m) : kNoKey - 2;
+            const bool tail = valid && nkey != key;
+            if (tail) {
+                if (heavy) {
+                    slot_nu[tile] = nu;
+                    slot_de[tile] = de;
+                } else {
+                    out[key] = nu / (lambda + de);
+                }
+            }
+            const bool cont = valid && lane == 31 && nkey == key;
+            ckey = __shfl_sync(0xffffffffu, cont ? key : kNoKey, 31);
+            cnu = __shfl_sync(0xffffffffu, nu, 31);
+            cde = __shfl_sync(0xffffffffu, de, 31);
+        }
+    }
+}
+
+// Heavy rows: sum the per-piece partials in piece order, finalise.
+template <typename T>
+__global__ void __launch_bounds__(256) k_ccd_fix(const uint4 *__restrict__ heavy, uint32_t nheavy,
+                                                 const T *__restrict__ slot_nu,
+                                                 const T *__restrict__ slot_de, T *out, T lambda)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t h = warp; h < nheavy; h += nwarps) {
+        const uint4 hr = heavy[h];
+        T nu = 0, de = 0;
+        for (uint32_t q = lane; q < hr.z; q += 32) {
+            nu += slot_nu[hr.y + q];
+            de += slot_de[hr.y + q];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            nu += __shfl_xor_sync(0xffffffffu, nu, o);
+            de += __shfl_xor_sync(0xffffffffu, de, o);
+        }
+        if (lane == 0) out[hr.x] = nu / (lambda + de);
+    }
+}
+
+// r = x - sum_f U0(i0,f) U1(i1,f) U2(i2,f)   (column-major factors)
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_ccd_resid_init(uint4 *rec, double *v64, uint32_t n,
+                                                        const T *__restrict__ U0,
+                                                        const T *__restrict__ U1,
+                                                        const T *__restrict__ U2, uint32_t d0,
+                                                        uint32_t d1, uint32_t d2)
+{
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        const uint4 r = rec[idx];
+        T p = 0;
+#pragma unroll 8
+        for (int f = 0; f < R; ++f)
+            p += U0[(size_t)f * d0 + r.x] * U1[(size_t)f * d1 + r.y] * U2[(size_t)f * d2 + r.z];
+        store_value<T>(rec, v64, idx, value_of<T>(r, v64, idx) - p);
+    }
+}
+
+// r -= term(column c) ; optional SSE partials of the new residual.
+template <typename T>
+__global__ void __launch_bounds__(256) k_ccd_finish(uint4 *rec, double *v64, uint32_t n,
+                                                    CcdCols cols, double *partial)
+{
+    double acc = 0;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        const uint4 r = rec[idx];
+        T res = value_of<T>(r, v64, idx) - term3<T>(cols.prev, r);
+        store_value<T>(rec, v64, idx, res);
+        acc += (double)res * (double)res;
+    }
+    if (partial) {
+        acc = block_sum(acc);
+        if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+    }
+}
+
+// column-major (R x d) -> row-major (d x R)
+template <typename T>
+__global__ void k_col_to_row(const T *__restrict__ col, T *__restrict__ row, uint32_t d, int R)
+{
+    const uint64_t total = (uint64_t)d * R;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = i / R, f = i % R;
+        row[i] = col[f * d + r];
+    }
+}
+
+// ---------------------------------------------------------------------
+// Reference "CCD+" (sgpu/ccd.cu:82-206, 318-348): all columns of a row at
+// once, residual with the row's old values, optional per-nonzero
+// multiplicity w.  Lane per column (C columns per lane), nonzeros of a tile
+// in order; rows absent from the tensor keep their values.
+// ---------------------------------------------------------------------
+template <typename T, int R>
+__global__ void __launch_bounds__(128) k_ccdc_tile(const int4 *__restrict__ tiles, uint32_t ntiles,
+                                                   const uint4 *__restrict__ rec,
+                                                   const double *__restrict__ v64,
+                                                   const T *__restrict__ w, int m, T *Um,
+                                                   const T *__restrict__ Ua,
+                                                   const T *__restrict__ Ub, T lambda,
+                                                   T *__restrict__ slot)
+{
+    constexpr int C = (R + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+    for (uint64_t tile = warp; tile < ntiles; tile += nwarps) {
+        const int4 td = tiles[tile];
+        const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
+        const bool heavy = td.z >= 0;
+        uint32_t cur = kNoKey;
+        T num[C], den[C], arow[C];
+        auto flush = [&]() {
+            if (cur == kNoKey) return;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const int col = lane + 32 * c;
+                if (col < R) {
+                    if (heavy) {
+                        slot[tile * (2 * R) + col] = num[c];
+                        slot[tile * (2 * R) + R + col] = den[c];
+                    } else {
+                        Um[(size_t)cur * R + col] = num[c] / (lambda + den[c]);
+                    }
+                }
+            }
+        };
+        for (uint32_t p = start; p < end; ++p) {
+            const uint4 r = rec[p];
+            const uint32_t key = key_of(r, m);
+            if (key != cur) {
+                flush();
+                cur = key;
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const int col = lane + 32 * c;
+                    num[c] = den[c] = 0;
+                    arow[c] = col < R ? Um[(size_t)key * R + col] : T(0);
+                }
+            }
+            const T wn = w ? w[p] : T(1);
+            if (wn == T(0)) continue;
+            const uint32_t qa = key_of(r, m1), qb = key_of(r, m2);
+            T h[C];
+            T dot = 0;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const int col = lane + 32 * c;
+                h[c] = col < R ? Ua[(size_t)qa * R + col] * Ub[(size_t)qb * R + col] : T(0);
+                dot += arow[c] * h[c];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+            const T e = value_of<T>(r, v64, p) - dot;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                den[c] += wn * h[c] * h[c];
+                num[c] += wn * h[c] * e;
+            }
+        }
+        flush();
+    }
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(128) k_ccdc_fix(const uint4 *__restrict__ heavy, uint32_t nheavy,
+                                                  const T *__restrict__ slot, T *Um, T lambda)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t h = warp; h < nheavy; h += nwarps) {
+        const uint4 hr = heavy[h];
+        for (int col = lane; col < R; col += 32) {
+            T nu = 0, de = 0;
+            for (uint32_t q = 0; q < hr.z; ++q) {
+                nu += slot[(size_t)(hr.y + q) * 2 * R + col];
+                de += slot[(size_t)(hr.y + q) * 2 * R + R + col];
+            }
+            Um[(size_t)hr.x * R + col] = nu / (lambda + de);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------
+// ALS (sgpu/als.cu:186-317 + 467-491 + cuSOLVER, restated): per row
+//   (sum w h h^T + lambda I) u = sum w x h,  h = Ua(j) o Ub(k).
+// Lane layout: L = min(R,32) lanes per nonzero group, NG = 32/L groups
+// take consecutive nonzeros of the row, C = R/L Gram columns per lane held
+// in registers.  The row's system is solved by its warp in FP64 in shared
+// memory: Cholesky, forward/back substitution, one refinement step against
+// the register copy of the Gram matrix.  Heavy-row pieces store their
+// partial Gram + right-hand side; k_als_fix sums them in piece order.
+// ---------------------------------------------------------------------
+template <int R>
+struct AlsShape {
+    static constexpr int L = R < 32 ? R : 32;
+    static constexpr int NG = 32 / L;
+    static constexpr int C = R / L;
+    static constexpr int smem_doubles = R * R + 2 * R;  // per warp
+};
+
+// Solve (G + lambda I) u = b for the row held by group 0 of the warp.
+// G[a][c] is Gram column (gl + L*c), b[c] the right-hand side entries.
+// Returns 1 when a pivot was not positive (diagonal shifted).
+template <typename T, int R>
+__device__ __forceinline__ int als_solve_warp(const T (&G)[R][AlsShape<R>::C], const T (&b)[AlsShape<R>::C],
+                              T lambda, double *S, T *urow)
+{
+    using Sh = AlsShape<R>;
+    constexpr int L = Sh::L, C = Sh::C;
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % L;
+    const bool g0 = lane < L;
+    double *y = S + R * R;
+    double *u = y + R;
+    if (g0) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const int col = gl + L * c;
+#pragma unroll
+            for (int a = 0; a < R; ++a) S[a * R + col] = (double)G[a][c] + (a == col ? (double)lambda : 0.0);
+            y[col] = (double)b[c];
+        }
+    }
+    __syncwarp();
+    int bad = 0;
+    // right-looking Cholesky, lower triangle of S (row-major, S[i*R+k], k<=i)
+    for (int j = 0; j < R; ++j) {
+        double d = S[j * R + j];
+        if (!(d > 0.0)) {
+            bad = 1;
+            d = 1e-300 + fabs(d) + 1e-12 * (double)lambda + 1e-30;
+        }
+        const double ljj = sqrt(d);
+        __syncwarp();
+        if (lane == 0) S[j * R + j] = ljj;
+        for (int i = j + 1 + lane; i < R; i += 32) S[i * R + j] /= ljj;
+        __syncwarp();
+        for (int i = j + 1 + lane; i < R; i += 32) {
+            const double lij = S[i * R + j];
+            for (int k2 = j + 1; k2 <= i; ++k2) S[i * R + k2] -= lij * S[k2 * R + j];
+        }
+        __syncwarp();
+    }
+    // two solves: the solution, then one refinement step
+    for (int it = 0; it < 2; ++it) {
+        // forward: L z = y (in place in y)
+        for (int i = 0; i < R; ++i) {
+            const double zi = y[i] / S[i * R + i];
+            __syncwarp();
+            if (lane == 0) y[i] = zi;
+            for (int k2 = i + 1 + lane; k2 < R; k2 += 32) y[k2] -= S[k2 * R + i] * zi;
+            __syncwarp();
+        }
+        // backward: L^T v = z
+        for (int i = R - 1; i >= 0; --i) {
+            const double vi = y[i] / S[i * R + i];
+            __syncwarp();
+            if (lane == 0) y[i] = vi;
+            for (int k2 = lane; k2 < i; k2 += 32) y[k2] -= S[i * R + k2] * vi;
+            __syncwarp();
+        }
+        if (it == 0) {
+            for (int k2 = lane; k2 < R; k2 += 32) u[k2] = y[k2];
+            __syncwarp();
+            // residual b - (G + lambda I) u, from the register Gram (symmetric)
+            if (g0) {
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const int col = gl + L * c;
+                    double acc = (double)b[c] - (double)lambda * u[col];
+#pragma unroll
+                    for (int a = 0; a < R; ++a) acc -= (double)G[a][c] * u[a];
+                    y[col] = acc;
+                }
+            }
+            __syncwarp();
+        } else {
+            for (int k2 = lane; k2 < R; k2 += 32) u[k2] += y[k2];
+            __syncwarp();
+        }
+    }
+    for (int k2 = lane; k2 < R; k2 += 32) urow[k2] = (T)u[k2];
+    __syncwarp();
+    return bad;
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void als_accumulate(const uint4 *__restrict__ rec,
+                                               const double *__restrict__ v64,
+                                               const T *__restrict__ w, int m,
+                                               const T *__restrict__ Ua, const T *__restrict__ Ub,
+                                               uint32_t s, uint32_t e, T (&G)[R][AlsShape<R>::C],
+                                               T (&b)[AlsShape<R>::C])
+{
+    using Sh = AlsShape<R>;
+    constexpr int L = Sh::L, NG = Sh::NG, C = Sh::C;
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % L, g = lane / L;
+    const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        b[c] = 0;
+#pragma unroll
+        for (int a = 0; a < R; ++a) G[a][c] = 0;
+    }
+    for (uint32_t base = s; base < e; base += NG) {
+        const uint32_t p = base + g;
+        const bool valid = p < e;
+        T hc[C];
+        T wx = 0, wn = 0;
+        if (valid) {
+            const uint4 r = rec[p];
+            wn = w ? w[p] : T(1);
+            wx = wn * value_of<T>(r, v64, p);
+            const T *ra = Ua + (size_t)key_of(r, m1) * R;
+            const T *rb = Ub + (size_t)key_of(r, m2) * R;
+#pragma unroll
+            for (int c = 0; c < C; ++c) hc[c] = ra[gl + L * c] * rb[gl + L * c];
+        } else {
+#pragma unroll
+            for (int c = 0; c < C; ++c) hc[c] = 0;
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) b[c] += wx * hc[c];
+#pragma unroll
+        for (int a = 0; a < R; ++a) {
+            const T ha = __shfl_sync(0xffffffffu, hc[a / L], g * L + (a % L));
+            const T wa = wn * ha;
+#pragma unroll
+            for (int c = 0; c < C; ++c) G[a][c] += wa * hc[c];
+        }
+    }
+    if constexpr (NG > 1) {
+#pragma unroll
+        for (int o = L; o < 32; o <<= 1) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                b[c] += __shfl_xor_sync(0xffffffffu, b[c], o);
+#pragma unroll
+                for (int a = 0; a < R; ++a) G[a][c] += __shfl_xor_sync(0xffffffffu, G[a][c], o);
+            }
+        }
+    }
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles, uint32_t ntiles,
+                                                  const uint4 *__restrict__ rec,
+                                                  const double *__restrict__ v64,
+                                                  const T *__restrict__ w, int m, T *Um,
+                                                  const T *__restrict__ Ua,
+                                                  const T *__restrict__ Ub, T lambda,
+                                                  T *__restrict__ slot,
+                                                  unsigned long long *nonspd)
+{
+    using Sh = AlsShape<R>;
+    constexpr int L = Sh::L, C = Sh::C;
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    double *S = smem + (size_t)wib * Sh::smem_doubles;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const int gl = lane % L;
+    int bad = 0;
+    T G[R][C];
+    T b[C];
+    for (uint64_t tile = warp; tile < ntiles; tile += nwarps) {
+        const int4 td = tiles[tile];
+        const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
+        if (td.z >= 0) {
+            als_accumulate<T, R>(rec, v64, w, m, Ua, Ub, start, end, G, b);
+            if (lane < L) {
+                T *dst = slot + tile * (size_t)(R * R + R);
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const int col = gl + L * c;
+#pragma unroll
+                    for (int a = 0; a < R; ++a) dst[a * R + col] = G[a][c];
+                    dst[R * R + col] = b[c];
+                }
+            }
+            continue;
+        }
+        uint32_t s = start;
+        while (s < end) {
+            const uint32_t key = key_of(rec[s], m);
+            uint32_t e = s + 1;
+            while (e < end && key_of(rec[e], m) == key) ++e;
+            als_accumulate<T, R>(rec, v64, w, m, Ua, Ub, s, e, G, b);
+            bad += als_solve_warp<T, R>(G, b, lambda, S, Um + (size_t)key * R);
+            s = e;
+        }
+    }
+    if (lane == 0 && bad) atomicAdd(nonspd, (unsigned long long)bad);
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(128) k_als_fix(const uint4 *__restrict__ heavy, uint32_t nheavy,
+                                                 const T *__restrict__ slot, T *Um, T lambda,
+                                                 unsigned long long *nonspd)
+{
+    using Sh = AlsShape<R>;
+    constexpr int L = Sh::L, C = Sh::C;
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    double *S = smem + (size_t)wib * Sh::smem_doubles;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const int gl = lane % L;
+    int bad = 0;
+    T G[R][C];
+    T b[C];
+    for (uint64_t h = warp; h < nheavy; h += nwarps) {
+        const uint4 hr = heavy[h];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            b[c] = 0;
+#pragma unroll
+            for (int a = 0; a < R; ++a) G[a][c] = 0;
+        }
+        for (uint32_t q = 0; q < hr.z; ++q) {
+            const T *src = slot + (size_t)(hr.y + q) * (R * R + R);
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const int col = gl + L * c;
+#pragma unroll
+                for (int a = 0; a < R; ++a) G[a][c] += src[a * R + col];
+                b[c] += src[R * R + col];
+            }
+        }
+        bad += als_solve_warp<T, R>(G, b, lambda, S, Um + (size_t)hr.x * R);
+    }
+    if (lane == 0 && bad) atomicAdd(nonspd, (unsigned long long)bad);
+}
+
+// ---------------------------------------------------------------------
+// Adjoint of 1/2 sum_Omega (x - xhat)^2 + lambda sum ||U||^2 in one pass:
+// groups of G = R/VN lanes walk tiles of mode-0-sorted nonzeros, recompute
+// the residual, keep the mode-0 gradient row in registers while the row
+// does not change, and add the mode-1/2 rows atomically.  G must hold
+// 2*lambda*U on entry (k_axpby).
+// ---------------------------------------------------------------------
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_grad(const uint4 *__restrict__ rec,
+                                              const double *__restrict__ v64, uint32_t n,
+                                              uint32_t tile_len, uint32_t ntiles,
+                                              const T *__restrict__ U0, const T *__restrict__ U1,
+                                              const T *__restrict__ U2, T *G0, T *G1, T *G2,
+                                              double *__restrict__ partial)
+{
+    using V = typename Vec<T>::type;
+    constexpr int VN = Vec<T>::n;
+    constexpr int G = R / VN;
+    constexpr int GPW = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G, gw = lane / G;
+    const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (gw * G));
+    const uint64_t group = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * GPW + gw;
+    const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x >> 5) * GPW;
+    double obj = 0;
+    for (uint64_t tile = group; tile < ntiles; tile += ngroups) {
+        const uint64_t start = tile * tile_len;
+        const uint64_t end = min(start + tile_len, (uint64_t)n);
+        uint32_t cur = kNoKey;
+        V ga;
+        V *grow = nullptr;
+        for (uint64_t p = start; p < end; ++p) {
+            const uint4 r = rec[p];
+            const T x = value_of<T>(r, v64, p);
+            if (r.x != cur) {
+                if (grow) vatomic_add(grow, ga);
+                cur = r.x;
+                grow = reinterpret_cast<V *>(G0 + (size_t)r.x * R) + gl;
+#pragma unroll
+                for (int v = 0; v < VN; ++v) vset(ga, v, T(0));
+            }
+            const V a = reinterpret_cast<const V *>(U0 + (size_t)r.x * R)[gl];
+            const V b = reinterpret_cast<const V *>(U1 + (size_t)r.y * R)[gl];
+            const V c = reinterpret_cast<const V *>(U2 + (size_t)r.z * R)[gl];
+            T part = 0;
+#pragma unroll
+            for (int v = 0; v < VN; ++v) part += vget(a, v) * vget(b, v) * vget(c, v);
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) part += __shfl_xor_sync(gmask, part, o);
+            const T e = x - part;
+            if (gl == 0) obj += 0.5 * (double)e * (double)e;
+            V gb, gc;
+#pragma unroll
+            for (int v = 0; v < VN; ++v) {
+                const T av = vget(a, v), bv = vget(b, v), cv = vget(c, v);
+                vset(ga, v, vget(ga, v) - e * bv * cv);
+                vset(gb, v, -e * av * cv);
+                vset(gc, v, -e * av * bv);
+            }
+            vatomic_add(reinterpret_cast<V *>(G1 + (size_t)r.y * R) + gl, gb);
+            vatomic_add(reinterpret_cast<V *>(G2 + (size_t)r.z * R) + gl, gc);
+        }
+        if (grow) vatomic_add(grow, ga);
+    }
+    obj = block_sum(obj);
+    if (threadIdx.x == 0) partial[blockIdx.x] = obj;
+}
+
+// y = alpha * x (elementwise)
+template <typename T>
+__global__ void k_scale(const T *__restrict__ x, T *__restrict__ y, uint64_t n, T alpha)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        y[i] = alpha * x[i];
+}
+
+}  // namespace k
+}  // namespace ctc

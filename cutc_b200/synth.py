@@ -1,0 +1,146 @@
+"""Seeded synthetic completion workloads with the shapes and value
+distributions of the benchmark configurations (no public dataset is
+available; these stand in for the reference's nell/DARPA/movielens/yelp
+tensors).
+
+Values: a rank-k CP model with N(0,1) factors, affinely mapped to [1, 5]
+with the min/max over the generated cells, plus N(0, sigma^2) noise
+(optionally clipped to [1, 5]).  Coordinates: uniform distinct cells, or
+per-mode truncated Zipf(s) ranks mapped through a seeded permutation, with
+duplicate cells removed and topped up until exactly nnz distinct cells
+remain.  Train/test split by a seeded Bernoulli(train_frac).
+
+Indices are returned 1-based (the .tns convention the reference needs).
+Generation runs in torch on the given device (CUDA for the 100M-nonzero
+workloads, CPU for small ones); the same seed on the same device type gives
+the same tensor.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class Workload:
+    name: str
+    dims: tuple
+    nnz: int
+    cp_rank: int
+    rank: int
+    sigma: float
+    clip: bool
+    zipf: tuple | None  # per-mode exponent, or None for uniform
+
+
+WORKLOADS = {
+    # 2,000 x 1,500 x 200, 200k uniform distinct cells, CP rank 8, R = 16
+    "small-als": Workload("small-als", (2000, 1500, 200), 200_000, 8, 16, 0.1, False, None),
+    # 500k x 20k x 2k, 100M Zipf(1.1) cells, CP rank 16, R = 32
+    "zipf-100m": Workload("zipf-100m", (500_000, 20_000, 2_000), 100_000_000, 16, 32, 0.25, True,
+                          (1.1, 1.1, 1.1)),
+    # 400M Zipf(1.3) cells over 1M x 600k x 300, CP rank 24, R = 64
+    "zipf-400m": Workload("zipf-400m", (1_000_000, 600_000, 300), 400_000_000, 24, 64, 0.2, False,
+                          (1.3, 1.3, 1.3)),
+}
+
+
+def scaled(w: Workload, nnz: int, dims=None) -> Workload:
+    """The same distribution with fewer nonzeros (and optionally other dims)."""
+    return Workload(w.name + f"@{nnz}", tuple(dims or w.dims), nnz, w.cp_rank, w.rank, w.sigma,
+                    w.clip, w.zipf)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _zipf_ranks(torch, n, dim, s, gen, device):
+    # inverse CDF of the truncated Zipf(s) over ranks 1..dim
+    ranks = torch.arange(1, dim + 1, device=device, dtype=torch.float64)
+    pmf = ranks.pow(-s)
+    cdf = torch.cumsum(pmf, 0)
+    cdf = cdf / cdf[-1]
+    u = torch.rand(n, generator=gen, device=device, dtype=torch.float64)
+    return torch.searchsorted(cdf, u).clamp_(max=dim - 1)
+
+
+def _draw_cells(torch, w: Workload, n, gen, device, perms):
+    cols = []
+    for m, d in enumerate(w.dims):
+        if w.zipf is None:
+            c = torch.randint(0, d, (n,), generator=gen, device=device, dtype=torch.int64)
+        else:
+            c = perms[m][_zipf_ranks(torch, n, d, w.zipf[m], gen, device)]
+        cols.append(c)
+    J, K = w.dims[1], w.dims[2]
+    return cols[0] * (J * K) + cols[1] * K + cols[2]
+
+
+def generate(w: Workload, seed: int = 0, device: str = "cpu", train_frac: float = 0.9):
+    """Returns dict(train=(ind, vals), test=(ind, vals), dims) with numpy
+    arrays (ind: 3 x n uint64 1-based, vals float64)."""
+    torch = _torch()
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    I, J, K = w.dims
+    perms = [torch.randperm(d, generator=gen, device=device) for d in w.dims]
+    keys = torch.unique(_draw_cells(torch, w, w.nnz, gen, device, perms))
+    tries = 0
+    while keys.numel() < w.nnz and tries < 64:
+        need = w.nnz - keys.numel()
+        extra = _draw_cells(torch, w, int(need * 1.2) + 1024, gen, device, perms)
+        keys = torch.unique(torch.cat([keys, extra]))
+        tries += 1
+    if keys.numel() < w.nnz:
+        raise RuntimeError("could not draw enough distinct cells")
+    # a seeded random subset of exactly nnz distinct cells
+    sel = torch.randperm(keys.numel(), generator=gen, device=device)[: w.nnz]
+    keys = keys[sel]
+    i = keys // (J * K)
+    j = (keys // K) % J
+    k = keys % K
+    del keys, sel
+    # values: rank-k CP model with N(0,1) factors
+    F = [torch.randn(d, w.cp_rank, generator=gen, device=device, dtype=torch.float32) for d in w.dims]
+    v = torch.empty(w.nnz, device=device, dtype=torch.float32)
+    step = 1 << 24
+    for s0 in range(0, w.nnz, step):
+        sl = slice(s0, min(s0 + step, w.nnz))
+        v[sl] = (F[0][i[sl]] * F[1][j[sl]] * F[2][k[sl]]).sum(1)
+    lo, hi = v.min(), v.max()
+    v = 1.0 + 4.0 * (v - lo) / (hi - lo)
+    v = v.double() + w.sigma * torch.randn(w.nnz, generator=gen, device=device, dtype=torch.float64)
+    if w.clip:
+        v.clamp_(1.0, 5.0)
+    train_mask = torch.rand(w.nnz, generator=gen, device=device) < train_frac
+    ind = torch.stack([i, j, k]) + 1
+
+    def pack(mask):
+        return (ind[:, mask].cpu().numpy().astype(np.uint64), v[mask].cpu().numpy())
+
+    return dict(train=pack(train_mask), test=pack(~train_mask), dims=tuple(w.dims))
+
+
+def sort_for_mode(ind, vals, mode):
+    """Stable sort by (ind[mode], ind[(mode+1)%3]) -- the reference's file order."""
+    order = np.lexsort((ind[(mode + 1) % 3], ind[mode]))
+    return ind[:, order], vals[order]
+
+
+def random_small(nnz, dims, seed=0, low=1.0, high=5.0, distinct=True):
+    """A small uniform test tensor (numpy only), 1-based indices."""
+    rng = np.random.default_rng(seed)
+    I, J, K = dims
+    if distinct:
+        total = I * J * K
+        if nnz > total:
+            raise ValueError("more nonzeros than cells")
+        cells = rng.choice(total, size=nnz, replace=False)
+        ind = np.stack([cells // (J * K), (cells // K) % J, cells % K]).astype(np.uint64) + 1
+    else:
+        ind = np.stack([rng.integers(0, d, nnz) for d in dims]).astype(np.uint64) + 1
+    vals = rng.uniform(low, high, nnz)
+    return ind, vals

@@ -1,0 +1,271 @@
+/*
+ * ctc.h -- C ABI of the B200-native sparse tensor-completion engine
+ * (libctc.so, built from cutc_b200/csrc/).
+ *
+ * Drop-in for the single-GPU driver of cuTC (abovekumo/cuTC).  Each entry
+ * point names the reference interface it replaces, as file:line relative to
+ * the reference project ("sgpu/" = "software/single GPU/sgpu/", "ga/" =
+ * "software/autotuning/performance_GA/").
+ *
+ * Conventions
+ *   - every function returns CTC_OK (0) or a negative CTC_E_* code and
+ *     leaves a message for ctc_last_error() (thread-local); nothing exits
+ *     the process (the reference calls exit(-1), sgpu/base.h:79-90);
+ *   - handles are caller-owned and freed with the matching *_free/destroy;
+ *   - a ctc_ctx owns one CUDA device and one stream; calls on one context
+ *     are serialised by the caller, different contexts are independent;
+ *   - tensors keep their indices exactly as read (1-based .tns files, as the
+ *     reference kernels require: sgpu/als.cu:256-258) and their values in
+ *     double; factors cross the ABI as row-major double, dims[m] x rank.
+ */
+#ifndef CTC_H
+#define CTC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CTC_OK 0
+#define CTC_E_ARG (-1)      /* invalid argument                        */
+#define CTC_E_IO (-2)       /* file could not be opened / parsed        */
+#define CTC_E_CUDA (-3)     /* CUDA runtime error                        */
+#define CTC_E_NOMEM (-4)    /* host or device allocation failed          */
+#define CTC_E_UNSUP (-5)    /* unsupported rank / order / combination    */
+#define CTC_E_NUMERIC (-6)  /* non-finite result                          */
+#define CTC_E_TIMEOUT (-7)  /* bounded device wait expired                */
+#define CTC_E_NOGPU (-8)    /* no CUDA device                             */
+
+typedef struct ctc_ctx ctc_ctx;
+typedef struct ctc_tensor ctc_tensor;
+typedef struct ctc_ciss ctc_ciss;
+typedef struct ctc_model ctc_model;
+typedef struct ctc_dataset ctc_dataset;
+
+/* ---------------------------------------------------------------- */
+/* errors, version                                                   */
+/* ---------------------------------------------------------------- */
+const char *ctc_last_error(void);
+const char *ctc_version(void);
+
+/* ---------------------------------------------------------------- */
+/* context                                                           */
+/* ---------------------------------------------------------------- */
+/* Select `device` and create the context's stream.  The reference picks
+ * device 0 inside every driver (sgpu/als.cu:535, sgpu/sgd.cu:178). */
+int ctc_ctx_create(int device, ctc_ctx **out);
+int ctc_ctx_destroy(ctc_ctx *ctx);
+/* Number of kernels this library launched on the context so far. */
+int ctc_ctx_kernel_launches(const ctc_ctx *ctx, uint64_t *out);
+/* The context's cudaStream_t, for callers timing with CUDA events. */
+void *ctc_ctx_stream(ctc_ctx *ctx);
+
+/* ---------------------------------------------------------------- */
+/* tensors (host)                                                    */
+/* ---------------------------------------------------------------- */
+/* Replaces tt_read (sgpu/sptensor.c:64 -> sgpu/io.c:195-217, text form
+ * io.c:58-106 + tt_get_dims io.c:234-308): whitespace "i j k v" lines,
+ * '#' and empty lines skipped, mode count from the first data line,
+ * dims[m] = max index (+1 when an index 0 occurs).  Parsed in parallel.
+ * Files ending in ".ctcb" use the binary form of ctc_tensor_save_bin. */
+int ctc_tensor_load_tns(const char *path, ctc_tensor **out);
+/* Binary form (replaces the broken .bin path, sgpu/io.c:125, 444-476):
+ * header "CTCB", u32 version, u32 nmodes, u64 nnz, u64 dims[nmodes], then
+ * nmodes arrays of u64 indices and one array of f64 values. */
+int ctc_tensor_save_bin(const ctc_tensor *t, const char *path);
+/* Build from caller arrays (copied).  dims may be NULL (max index). */
+int ctc_tensor_from_coo(int nmodes, uint64_t nnz, const uint64_t *dims,
+                        const uint64_t *const *ind, const double *vals,
+                        ctc_tensor **out);
+int ctc_tensor_info(const ctc_tensor *t, int *nmodes, uint64_t *nnz, uint64_t *dims);
+/* Copy out: ind[m] must hold nnz u64, vals nnz doubles (either may be NULL). */
+int ctc_tensor_export(const ctc_tensor *t, uint64_t *const *ind, double *vals);
+/* Stable sort by (ind[mode], ind[(mode+1)%n]) in place (mode 0-based), the
+ * ordering the reference's input files carry
+ * (software/scripts/stensor.py:36-43, tvtensor.py:103). */
+int ctc_tensor_sort(ctc_tensor *t, int mode);
+int ctc_tensor_free(ctc_tensor *t);
+
+/* ---------------------------------------------------------------- */
+/* CISS (TB-COO) tiling                                              */
+/* ---------------------------------------------------------------- */
+/* Replaces ciss_alloc (sgpu/ciss.c:68-195, mode 1-based, tile length 32)
+ * and cissbasic_alloc (ga/ciss.c:69-212, runtime tile length).  The
+ * tensor must already be sorted for `mode` (the reference's contract).
+ * Bit-exact with the reference on every slot it writes; slots it leaves
+ * uninitialised (header[1] of a tile without a row change, the bitmap of a
+ * terminator-only tile, the unused tail) are 0.0 here.  tile_len in
+ * [1, 64]; bitmaps above 53 bits round as the reference's do. */
+int ctc_ciss_build(const ctc_tensor *t, int mode, int tile_len, ctc_ciss **out);
+/* The GA builder's form (ga/ciss.c:69-212 with one partition covering all
+ * rows): identical tiles; its directory counters count the first nonzero
+ * too (ga/ciss.c:101-120), so dcounter[k] = start of slice k. */
+int ctc_ciss_build_ga(const ctc_tensor *t, int mode, int tile_len, ctc_ciss **out);
+int ctc_ciss_sizes(const ctc_ciss *c, uint64_t *nnz, uint64_t *dlength,
+                   uint64_t *size_rows, int *tile_len);
+/* directory: dlength u64; dcounter: dlength+1 u64; entries: size_rows*3 f64;
+ * written (may be NULL): size_rows*3 bytes, 1 where the reference writes. */
+int ctc_ciss_export(const ctc_ciss *c, uint64_t *directory, uint64_t *dcounter,
+                    double *entries, uint8_t *written);
+int ctc_ciss_free(ctc_ciss *c);
+
+/* ---------------------------------------------------------------- */
+/* factor model                                                      */
+/* ---------------------------------------------------------------- */
+/* Replaces the factor arrays of tc_main_ciss (sgpu/completion.c:422-450,
+ * matrix_randomize / fill_rand sgpu/matrixprocess.c:156-165, 568-577). */
+int ctc_model_create(int nmodes, const uint64_t *dims, int rank, ctc_model **out);
+/* Seeded U(0,1)*scale init (scale 1/sqrt(rank) in the workloads); a
+ * counter-based generator, so the result depends only on (seed, mode,
+ * row, column). */
+int ctc_model_init_uniform(ctc_model *m, uint64_t seed, double scale);
+int ctc_model_set(ctc_model *m, int mode, const double *rowmajor);
+int ctc_model_get(const ctc_model *m, int mode, double *rowmajor);
+int ctc_model_copy(const ctc_model *src, ctc_model *dst);
+int ctc_model_info(const ctc_model *m, int *nmodes, uint64_t *dims, int *rank);
+int ctc_model_free(ctc_model *m);
+
+/* ---------------------------------------------------------------- */
+/* algorithms                                                        */
+/* ---------------------------------------------------------------- */
+enum ctc_alg {
+    CTC_ALG_ALS = 0,        /* tc_als, sgpu/als.cu:512-843                   */
+    CTC_ALG_SGD = 1,        /* tc_sgd, sgpu/sgd.cu:155-342                   */
+    CTC_ALG_CCD = 2,        /* tc_ccd ("CCD+"), sgpu/ccd.cu:359-661           */
+    CTC_ALG_CCDPP = 3       /* rank-one CCD++ (the loop sgpu/ccd.cu:531-556
+                               leaves commented out)                          */
+};
+enum ctc_precision {
+    CTC_PREC_F32 = 0,       /* FP32 factors and accumulation (plain form)     */
+    CTC_PREC_F64 = 1,       /* FP64 throughout (the reference's arithmetic)   */
+    CTC_PREC_MIXED = 2      /* BF16 factor reads, FP32 masters/accumulation   */
+};
+enum ctc_lr_schedule {
+    CTC_LR_BOLD_DRIVER = 0, /* x1.05 / x0.5 from epoch 2 (sgpu/sgd.cu:315-321) */
+    CTC_LR_EXP_DECAY = 1,   /* lr *= lr_decay after every epoch                */
+    CTC_LR_CONSTANT = 2
+};
+enum ctc_sgd_order {
+    CTC_SGD_HOGWILD = 0,    /* tiles in parallel, lock-free updates           */
+    CTC_SGD_SEQUENTIAL = 1  /* one warp, tile-major entry-minor: deterministic */
+};
+
+typedef struct {
+    int alg;               /* enum ctc_alg                                          */
+    int rank;              /* 8, 16, 32 or 64 (reference: DEFAULT_NFACTORS 16)      */
+    double lambda;         /* regularisation (reference: ALS 10, SGD 1e-3, CCD 100) */
+    double lr;             /* SGD learning rate (reference LEARN_RATE 1e-3)         */
+    double lr_scale;       /* SGD step multiplier (reference SGD_MODIFICATION 1e-5) */
+    int lr_schedule;       /* enum ctc_lr_schedule                                  */
+    double lr_decay;       /* factor for CTC_LR_EXP_DECAY                           */
+    int iters;             /* epochs (reference DEFAULT_MAX_ITERATE 1000)           */
+    int inner;             /* CCD++ inner sweeps per column                         */
+    int tile_len;          /* nonzeros per warp work unit (0 = tuned)               */
+    int threads_per_block; /* 0 = tuned                                             */
+    int precision;         /* enum ctc_precision                                    */
+    int compat;            /* 1: reference kernel semantics (values stored through
+                              an integer, sgpu/ciss.c:163; ALS/CCD per-tile lane
+                              multiplicities; CCD grid coverage, sgpu/ccd.cu:520)   */
+    int early_stop;        /* 1: tc_converge rule (sgpu/completion.c:296-362)       */
+    double tolerance;      /* early-stop tolerance (reference TOLERANCE 1e-4)       */
+    int max_bad_epochs;    /* reference MAX_BADEPOCHS 3                             */
+    int mode_start;        /* first mode of the rotation (reference: rand()%3,
+                              sgpu/als.cu:684-685; fixed here)                      */
+    int sgd_order;         /* enum ctc_sgd_order                                    */
+    int sgd_atomic;        /* Hogwild: 1 = atomic adds, 0 = plain stores            */
+    int eval_every;        /* evaluate RMSE every n epochs (0 = only at the end)    */
+    int use_graph;         /* capture the epoch in a CUDA graph when possible       */
+    uint64_t seed;         /* reserved for stochastic modes                          */
+} ctc_params;
+
+/* Reference-default parameters for an algorithm (sgpu/base.h:19-64). */
+int ctc_params_default(int alg, ctc_params *p);
+
+typedef struct {
+    int epoch;
+    double loss;       /* training sum of squared errors (sgpu/completion.c:166) */
+    double frob;       /* lambda * sum ||U||^2                                    */
+    double rmse_tr, rmse_vl, rmse_te;   /* -1 when the tensor was not given     */
+    double ms_epoch;   /* device time of the epoch's update kernels              */
+    double lr;
+} ctc_epoch_stats;
+
+/* Called after every evaluated epoch; a non-zero return stops the run. */
+typedef int (*ctc_epoch_cb)(void *user, const ctc_epoch_stats *s);
+
+typedef struct {
+    int epochs_run;
+    int best_epoch;
+    double best_rmse;       /* best validation RMSE (train RMSE without one)   */
+    double final_rmse_tr, final_rmse_vl, final_rmse_te;
+    double total_ms;        /* device time of all update kernels                */
+    uint64_t nonspd_rows;   /* ALS rows whose system needed a diagonal shift    */
+} ctc_result;
+
+/* Replaces tc_als / tc_sgd / tc_ccd (sgpu/als.cuh:20-33, sgd.cuh:18-32,
+ * ccd.cuh:20-33) and tc_main_ciss (sgpu/completion.c:422-497):
+ * train[m] is the training tensor sorted for mode m (the reference's
+ * traina/b/c); train[1], train[2] may be NULL (sorted copies are then made
+ * internally).  val/test may be NULL.  `model` holds the initial factors
+ * and receives the final ones; `best` (may be NULL) receives the factors of
+ * the best validation epoch (tc_converge's best_mats).  Everything is
+ * staged to the device inside the call and released before it returns. */
+int ctc_run(ctc_ctx *ctx, const ctc_tensor *const train[3], const ctc_tensor *val,
+            const ctc_tensor *test, ctc_model *model, ctc_model *best,
+            const ctc_params *p, ctc_epoch_cb cb, void *user, ctc_result *res);
+
+/* Device-resident form of the same run: the tensors are staged once
+ * (records, tiles, sorted copies) and epochs run on HBM-resident data.
+ * The factor rows are the maximum index over train/val/test per mode
+ * (ctc_dataset_dims); models given to the dataset must have those rows. */
+int ctc_dataset_create(ctc_ctx *ctx, const ctc_tensor *const train[3],
+                       const ctc_tensor *val, const ctc_tensor *test,
+                       const ctc_params *p, ctc_dataset **out);
+int ctc_dataset_dims(const ctc_dataset *d, uint64_t *dims);
+int ctc_dataset_free(ctc_dataset *d);
+/* The whole epoch loop of ctc_run on the staged tensors; `p` may change
+ * the run-time parameters but not alg/precision/compat/tile_len. */
+int ctc_dataset_run(ctc_dataset *d, ctc_model *model, ctc_model *best,
+                    const ctc_params *p, ctc_epoch_cb cb, void *user, ctc_result *res);
+/* Step-wise control of the same device session (one iteration of the loop
+ * in sgpu/als.cu:678-810, sgd.cu:277-324, ccd.cu:521-620 without the host
+ * round trip of the factors):
+ *   set_model  stages factors (and, for CCD++, the residuals x - model);
+ *   epochs     enqueues n update epochs on the context stream and returns
+ *              without waiting (no evaluation in between);
+ *   set_lr     the SGD step (lr * step scale) of later epochs;
+ *   evaluate   waits, then fills loss, frob and the three RMSEs;
+ *   get_model  copies the factors out. */
+int ctc_dataset_set_model(ctc_dataset *d, const ctc_model *model);
+int ctc_dataset_epochs(ctc_dataset *d, int n);
+int ctc_dataset_set_lr(ctc_dataset *d, double lr);
+int ctc_dataset_evaluate(ctc_dataset *d, ctc_epoch_stats *st);
+int ctc_dataset_get_model(ctc_dataset *d, ctc_model *model);
+
+/* Per-kernel device time: with profiling on, every launch of this library
+ * on the context is bracketed by a CUDA event pair; kernel_time sums the
+ * launches whose kernel name contains `name` (count, milliseconds).  No
+ * reference counterpart (the reference times with gettimeofday around
+ * kernels and copies, sgpu/als.cu:682-799). */
+int ctc_ctx_set_profiling(ctc_ctx *ctx, int on);
+int ctc_ctx_kernel_time(ctc_ctx *ctx, const char *name, uint64_t *count, double *total_ms);
+int ctc_ctx_reset_kernel_times(ctc_ctx *ctx);
+
+/* RMSE of `model` on tensor `t` on the GPU (sgpu/completion.c:123-130 with
+ * rows read at index-1).  The reduction is deterministic (fixed order). */
+int ctc_rmse(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double *rmse);
+
+/* Adjoint of the masked CP loss 1/2 ||P_Omega(X - [[A,B,C]])||^2 +
+ * lambda sum ||U_m||^2: every factor gradient from one pass over the
+ * tensor, residuals recomputed, not stored.  grads[m]: dims[m] x rank
+ * row-major doubles.  obj (may be NULL) receives the loss value.
+ * No reference counterpart (the reference has no gradient path). */
+int ctc_grad(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double lambda,
+             double *const *grads, double *obj);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,280 @@
+"""Parity of the CUDA engine (called through the C ABI) with the FP64 CPU
+oracle on the same seeded tensors and initial factors.
+
+Tolerances (relative to the largest magnitude of the compared quantity):
+  FP64 runs          factors and RMSE within 1e-9
+  FP32 runs          per-iteration RMSE within 1e-5, factors within 1e-4 (ALS,
+                     CCD++); SGD trajectory within 1e-3
+  Hogwild SGD        final test RMSE within 0.5 % of the sequential oracle
+"""
+import numpy as np
+import pytest
+
+import cutc_b200 as ctc
+from oracle import pyoracle as po
+from tests.helpers import Problem, max_factor_rel, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def engine_run(ctx, P, alg, iters, **kw):
+    kw.setdefault("early_stop", 0)
+    kw.setdefault("eval_every", 1)
+    kw.setdefault("rank", P.R)
+    p = ctc.params(alg, iters=iters, **kw)
+    model = P.c_model()
+    out = ctc.run(ctx, P.c_sorted(), None, P.c_test(), model, p)
+    return model.factors(), out
+
+
+def oracle_rmse(P, U):
+    return po.rmse(P.o_train(), U), po.rmse(P.o_test(), U)
+
+
+# ------------------------------------------------------------------ RMSE
+def test_rmse_kernel(ctx):
+    P = Problem(20000, (300, 200, 100), 16, seed=1)
+    m = P.c_model()
+    got = ctc.rmse(ctx, P.c_test(), m)
+    want = po.rmse(P.o_test(), P.factors())
+    assert abs(got - want) / want < 1e-5
+
+
+@pytest.mark.parametrize("R", [8, 16, 32, 64])
+def test_rmse_ranks(ctx, R):
+    P = Problem(5000, (80, 70, 60), R, seed=R)
+    assert abs(ctc.rmse(ctx, P.c_test(), P.c_model()) - po.rmse(P.o_test(), P.factors())) < 1e-5 * 5
+
+
+# ------------------------------------------------------------------ ALS
+def oracle_als(P, iters, lam, w=None, trunc=False):
+    U = P.factors()
+    hist = [oracle_rmse(P, U)]
+    for _ in range(iters):
+        for m in range(3):
+            po.als_mode(P.o_sorted(m), m, U, lam, None if w is None else w[m], trunc)
+        hist.append(oracle_rmse(P, U))
+    return U, hist
+
+
+@pytest.mark.parametrize("R", [8, 16, 32])
+def test_als_f64(ctx, R):
+    P = Problem(12000, (150, 120, 40), R, seed=3)
+    U, hist = oracle_als(P, 3, 0.05)
+    G, out = engine_run(ctx, P, ctc.ALS, 3, precision=ctc.PREC_F64, **{"lambda": 0.05})
+    assert max_factor_rel(G, U) < 1e-9
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-9
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-9
+
+
+def test_als_f32_config(ctx):
+    """Plain FP32 ALS at R=16, lambda=0.05 (the small uniform workload's
+    settings), 10 iterations."""
+    P = Problem(40000, (400, 300, 40), 16, seed=4)
+    U, hist = oracle_als(P, 10, 0.05)
+    G, out = engine_run(ctx, P, ctc.ALS, 10, precision=ctc.PREC_F32, **{"lambda": 0.05})
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-5, e
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-5, e
+    assert max_factor_rel(G, U) < 1e-4
+
+
+def test_als_heavy_rows(ctx):
+    """Rows longer than a tile go through the piece + fixup path."""
+    P = Problem(6000, (60, 50, 40), 16, seed=5, heavy_row=1800)
+    U, hist = oracle_als(P, 2, 0.1)
+    G, out = engine_run(ctx, P, ctc.ALS, 2, precision=ctc.PREC_F64, tile_len=64, **{"lambda": 0.1})
+    assert max_factor_rel(G, U) < 1e-9
+
+
+def test_als_compat_matches_reference_semantics(ctx):
+    """compat=1: values stored through an integer and the reference warp
+    kernel's per-lane multiplicities (nnz % 32 == 0 for every copy)."""
+    P = Problem(4096 + 455, (70, 60, 50), 16, seed=6, test_frac=0.0)
+    n = P.train[0].shape[1] // 32 * 32
+    P.train = (P.train[0][:, :n], P.train[1][:n])
+    from cutc_b200 import synth
+    P.sorted = [synth.sort_for_mode(*P.train, m) for m in range(3)]
+    P.test = (P.train[0][:, :64], P.train[1][:64])
+    w = [po.compat_weights(P.o_sorted(m), m, 0) for m in range(3)]
+    U, hist = oracle_als(P, 2, 10.0, w=w, trunc=True)
+    G, out = engine_run(ctx, P, ctc.ALS, 2, precision=ctc.PREC_F64, compat=1, **{"lambda": 10.0})
+    assert max_factor_rel(G, U) < 1e-9
+
+
+# ------------------------------------------------------------------ CCD
+def test_ccd_compat(ctx):
+    P = Problem(8192 + 500, (90, 80, 30), 16, seed=7, test_frac=0.0)
+    n = P.train[0].shape[1] // 32 * 32
+    P.train = (P.train[0][:, :n], P.train[1][:n])
+    from cutc_b200 import synth
+    P.sorted = [synth.sort_for_mode(*P.train, m) for m in range(3)]
+    P.test = (P.train[0][:, :64], P.train[1][:64])
+    w = [po.compat_weights(P.o_sorted(m), m, 1) for m in range(3)]
+    U = P.factors()
+    for _ in range(2):
+        for m in range(3):
+            po.ccd_compat_mode(P.o_sorted(m), m, U, 100.0, w[m], True)
+    G, out = engine_run(ctx, P, ctc.CCD, 2, precision=ctc.PREC_F64, compat=1, **{"lambda": 100.0})
+    assert max_factor_rel(G, U) < 1e-9
+
+
+def test_ccd_plain_f64(ctx):
+    P = Problem(9000, (90, 80, 30), 16, seed=8, heavy_row=700)
+    U = P.factors()
+    for _ in range(2):
+        for m in range(3):
+            po.ccd_compat_mode(P.o_sorted(m), m, U, 1.0, None, False)
+    G, out = engine_run(ctx, P, ctc.CCD, 2, precision=ctc.PREC_F64, tile_len=64, **{"lambda": 1.0})
+    assert max_factor_rel(G, U) < 1e-9
+
+
+# ------------------------------------------------------------------ CCD++
+def oracle_ccdpp(P, iters, lam, inner):
+    U = P.factors()
+    T = P.o_sorted(0)
+    r = po.residual(T, U)
+    hist = [oracle_rmse(P, U)]
+    for _ in range(iters):
+        po.ccdpp_outer(T, U, lam, inner, r)
+        hist.append(oracle_rmse(P, U))
+    return U, hist, r
+
+
+@pytest.mark.parametrize("R", [8, 32])
+def test_ccdpp_f64(ctx, R):
+    P = Problem(15000, (200, 150, 60), R, seed=9, heavy_row=900)
+    U, hist, _ = oracle_ccdpp(P, 2, 0.1, 3)
+    G, out = engine_run(ctx, P, ctc.CCDPP, 2, precision=ctc.PREC_F64, inner=3, tile_len=128,
+                        **{"lambda": 0.1})
+    assert max_factor_rel(G, U) < 1e-9
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-9
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-9
+
+
+def test_ccdpp_f32(ctx):
+    P = Problem(50000, (500, 300, 60), 32, seed=10)
+    U, hist, _ = oracle_ccdpp(P, 3, 0.1, 3)
+    G, out = engine_run(ctx, P, ctc.CCDPP, 3, precision=ctc.PREC_F32, inner=3, **{"lambda": 0.1})
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-5, e
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-5, e
+    assert max_factor_rel(G, U) < 1e-4
+
+
+# ------------------------------------------------------------------ SGD
+def oracle_sgd(P, iters, lr, lam, scale=1.0, decay=1.0, trunc=False):
+    U = P.factors()
+    T = P.o_sorted(0)
+    hist = [oracle_rmse(P, U)]
+    for _ in range(iters):
+        po.sgd_epoch(T, U, lr, lam, scale, trunc)
+        lr *= decay
+        hist.append(oracle_rmse(P, U))
+    return U, hist
+
+
+@pytest.mark.parametrize("R", [16, 32])
+def test_sgd_sequential_f64(ctx, R):
+    P = Problem(6000, (100, 80, 50), R, seed=11)
+    U, hist = oracle_sgd(P, 3, 0.01, 0.01, decay=0.95)
+    G, out = engine_run(ctx, P, ctc.SGD, 3, precision=ctc.PREC_F64, sgd_order=ctc.SGD_SEQUENTIAL,
+                        lr=0.01, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY, lr_decay=0.95,
+                        **{"lambda": 0.01})
+    assert max_factor_rel(G, U) < 1e-9
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-9
+
+
+def test_sgd_sequential_f32_trajectory(ctx):
+    P = Problem(20000, (200, 150, 60), 32, seed=12)
+    U, hist = oracle_sgd(P, 8, 0.01, 0.01, decay=0.95)
+    G, out = engine_run(ctx, P, ctc.SGD, 8, precision=ctc.PREC_F32, sgd_order=ctc.SGD_SEQUENTIAL,
+                        lr=0.01, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY, lr_decay=0.95,
+                        **{"lambda": 0.01})
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-3, e
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-3, e
+
+
+@pytest.mark.parametrize("atomic", [1, 0])
+def test_sgd_hogwild_final_rmse(ctx, atomic):
+    P = Problem(200000, (2000, 1500, 200), 32, seed=13)
+    U, hist = oracle_sgd(P, 10, 0.01, 0.01, decay=0.95)
+    G, out = engine_run(ctx, P, ctc.SGD, 10, precision=ctc.PREC_F32, sgd_order=ctc.SGD_HOGWILD,
+                        sgd_atomic=atomic, lr=0.01, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY,
+                        lr_decay=0.95, **{"lambda": 0.01})
+    assert abs(out.epochs[-1]["rmse_te"] - hist[-1][1]) / hist[-1][1] < 0.005
+
+
+def test_sgd_reference_defaults_bold_driver(ctx):
+    """Reference constants: lr 1e-3, step scale 1e-5, lambda 1e-3, bold driver."""
+    P = Problem(8000, (100, 90, 40), 16, seed=14)
+    U = P.factors()
+    T = P.o_sorted(0)
+    lr, prev = 1e-3, None
+    hist = []
+    for e in range(4):
+        if e > 0:
+            po.sgd_epoch(T, U, lr, 1e-3, 1e-5, False)
+        loss = po.sq_loss(T, U)
+        obj = loss + po.frob(P.dims, U, 1e-3)
+        hist.append(np.sqrt(loss / T.nnz))
+        if e > 1:
+            lr *= 1.05 if obj < prev else 0.5
+        if e > 0:
+            prev = obj
+        else:
+            prev = obj
+    G, out = engine_run(ctx, P, ctc.SGD, 3, precision=ctc.PREC_F64, sgd_order=ctc.SGD_SEQUENTIAL)
+    assert max_factor_rel(G, U) < 1e-9
+    for e in range(4):
+        assert abs(out.epochs[e]["rmse_tr"] - hist[e]) / hist[e] < 1e-9
+
+
+# ------------------------------------------------------------------ adjoint
+def test_grad_matches_oracle_and_finite_differences(ctx):
+    P = Problem(3000, (40, 30, 20), 8, seed=15)
+    lam = 0.05
+    m = P.c_model()
+    G, obj = ctc.grad(ctx, P.c_test() if False else ctc.Tensor.from_coo(*P.train, dims=P.dims), m, lam)
+    U = P.factors()
+    T = P.o_train()
+    Go = po.grad(T, U, lam)
+    assert max_factor_rel(G, Go) < 1e-9
+    assert abs(obj - po.objective(T, U, lam)) / po.objective(T, U, lam) < 1e-10
+    # central finite differences of the FP64 objective on a few coordinates
+    rng = np.random.default_rng(0)
+    h = 1e-5
+    for _ in range(12):
+        mode = int(rng.integers(3))
+        r = int(rng.integers(P.dims[mode]))
+        f = int(rng.integers(P.R))
+        Up = [u.copy() for u in U]
+        Um = [u.copy() for u in U]
+        Up[mode][r, f] += h
+        Um[mode][r, f] -= h
+        fd = (po.objective(T, Up, lam) - po.objective(T, Um, lam)) / (2 * h)
+        assert abs(fd - G[mode][r, f]) <= 1e-6 * max(1.0, abs(fd))
+
+
+# ------------------------------------------------------------------ edge cases
+def test_single_row_and_tiny(ctx):
+    P = Problem(25, (1, 9, 8), 8, seed=16, test_frac=0.0)
+    P.test = (P.train[0][:, :5], P.train[1][:5])
+    U, hist = oracle_als(P, 2, 0.5)
+    G, out = engine_run(ctx, P, ctc.ALS, 2, precision=ctc.PREC_F64, **{"lambda": 0.5})
+    assert max_factor_rel(G, U) < 1e-9
+
+
+def test_rejects_bad_input(ctx):
+    ind = np.array([[0, 1], [1, 1], [1, 2]], dtype=np.uint64)
+    t = ctc.Tensor.from_coo(ind, [1.0, 2.0], dims=[2, 2, 2])
+    m = ctc.Model([2, 2, 2], 8)
+    with pytest.raises(ctc.CtcError) as e:
+        ctc.run(ctx, [t], None, None, m, ctc.params("als", rank=8, iters=1))
+    assert e.value.code == -1
+    with pytest.raises(ctc.CtcError):
+        ctc.run(ctx, [t], None, None, m, ctc.params("als", rank=12, iters=1))

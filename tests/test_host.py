@@ -1,0 +1,210 @@
+"""Host-side behaviour of libctc and of the oracle, CPU only: exports, error
+codes, tensor I/O round trips, sorting, seeded model init, and the oracle's
+own consistency (gradient vs finite differences, monotone ALS / CCD++)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import cutc_b200 as ctc
+from cutc_b200 import api, synth
+from oracle import pyoracle as po
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol():
+    declared = api._declared_names()
+    assert len(declared) >= 30
+    missing = [n for n in declared if not hasattr(api.lib(), n)]
+    assert not missing, missing
+
+
+def test_declared_entry_points_cite_reference_or_say_none():
+    txt = open(os.path.join(ROOT, "include", "ctc.h")).read()
+    assert "sgpu/" in txt and "ga/ciss.c" in txt
+
+
+def test_error_codes_without_crash(tmp_path):
+    with pytest.raises(ctc.CtcError) as e:
+        ctc.tt_read(str(tmp_path / "missing.tns"))
+    assert e.value.code == -2
+    t = ctc.Tensor.from_coo(np.ones((3, 4), dtype=np.uint64), np.ones(4))
+    with pytest.raises(ctc.CtcError) as e:
+        ctc.ciss_alloc(t, 1, 0)
+    assert e.value.code == -1
+    with pytest.raises(ctc.CtcError):
+        ctc.ciss_alloc(t, 4, 32)
+
+
+def test_context_without_gpu_is_an_error_not_a_crash():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(ctc.CtcError) as e:
+        ctc.Context(0)
+    assert e.value.code == -8
+
+
+def test_coo_roundtrip_and_dims():
+    ind, vals = synth.random_small(500, (30, 20, 10), seed=1)
+    t = ctc.Tensor.from_coo(ind, vals)
+    nm, nnz, dims = t.info()
+    assert (nm, nnz) == (3, 500)
+    assert dims == [int(ind[m].max()) for m in range(3)]
+    i2, v2 = t.export()
+    assert np.array_equal(i2, ind) and np.array_equal(v2, vals)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_sort_is_stable_lexsort(mode):
+    ind, vals = synth.random_small(3000, (9, 8, 7), seed=2, distinct=False)
+    t = ctc.Tensor.from_coo(ind, vals).sort(mode)
+    i2, v2 = t.export()
+    si, sv = synth.sort_for_mode(ind, vals, mode)
+    assert np.array_equal(i2, si) and np.array_equal(v2, sv)
+
+
+def test_binary_roundtrip(tmp_path):
+    ind, vals = synth.random_small(777, (50, 40, 30), seed=3)
+    t = ctc.Tensor.from_coo(ind, vals, dims=[60, 40, 30])
+    p = str(tmp_path / "x.ctcb")
+    t.save_bin(p)
+    t2 = ctc.tt_read(p)
+    assert t2.dims == [60, 40, 30]
+    i2, v2 = t2.export()
+    assert np.array_equal(i2, ind) and np.array_equal(v2, vals)
+    (tmp_path / "bad.ctcb").write_bytes(b"CTCX0000")
+    with pytest.raises(ctc.CtcError):
+        ctc.tt_read(str(tmp_path / "bad.ctcb"))
+
+
+def test_tns_reader_large_parallel_matches_oracle(tmp_path):
+    """A file big enough for the parallel chunked parse (> 1 MiB)."""
+    ind, vals = synth.random_small(60000, (500, 400, 300), seed=4)
+    p = str(tmp_path / "big.tns")
+    po.write_tns(p, po.Tensor(ind, vals))
+    a = ctc.tt_read(p)
+    b = po.tns_read(p)
+    ia, va = a.export()
+    assert np.array_equal(ia, b.ind) and np.array_equal(va.view(np.uint64), b.vals.view(np.uint64))
+    assert a.dims == b.dims
+
+
+def test_tns_first_line_token_rule(tmp_path):
+    """The mode count comes from strtok on the first data line, so trailing
+    whitespace there adds a mode (sgpu/io.c:249-257) -- in both readers."""
+    p = tmp_path / "ws.tns"
+    p.write_text("1 2 3 4.5 \n2 1 1 1.0\n")
+    a, b = ctc.tt_read(str(p)), po.tns_read(str(p))
+    assert a.info()[0] == b.nmodes == 4
+
+
+def test_model_init_is_seeded_and_bounded():
+    m1 = ctc.Model([100, 80, 60], 16).init_uniform(42, 0.25)
+    m2 = ctc.Model([100, 80, 60], 16).init_uniform(42, 0.25)
+    m3 = ctc.Model([100, 80, 60], 16).init_uniform(43, 0.25)
+    for a, b, c in zip(m1.factors(), m2.factors(), m3.factors()):
+        assert np.array_equal(a, b)
+        assert not np.array_equal(a, c)
+        assert a.min() >= 0 and a.max() < 0.25
+    assert abs(np.mean(m1.get(0)) - 0.125) < 0.01
+
+
+def test_params_reference_defaults():
+    p = ctc.params("als")
+    assert (p.rank, p.lambda_, p.iters, p.max_bad_epochs) == (16, 10.0, 1000, 3)
+    assert abs(p.tolerance - 1e-4) < 1e-12
+    assert ctc.params("sgd").lambda_ == 1e-3 and ctc.params("sgd").lr_scale == 1e-5
+    assert ctc.params("ccd").lambda_ == 100.0
+
+
+def test_value_through_integer():
+    vals = np.array([3.7, 2.0, 0.999, -2.5, 1e20, 5.0])
+    got = po.value_trunc(vals)
+    assert got[0] == 3.0 and got[1] == 2.0 and got[2] == 0.0 and got[5] == 5.0
+    assert got[3] == float(2**64 - 2)
+
+
+# ------------------------------------------------------------------ oracle
+def test_oracle_grad_finite_differences():
+    ind, vals = synth.random_small(400, (12, 10, 8), seed=5)
+    T = po.Tensor(ind, vals, [12, 10, 8])
+    rng = np.random.default_rng(0)
+    U = [rng.uniform(0, 1, (d, 4)) for d in (12, 10, 8)]
+    G = po.grad(T, U, 0.1)
+    h = 1e-6
+    for mode in range(3):
+        for r, f in [(0, 0), (3, 2), (7, 3)]:
+            Up = [u.copy() for u in U]
+            Um = [u.copy() for u in U]
+            Up[mode][r, f] += h
+            Um[mode][r, f] -= h
+            fd = (po.objective(T, Up, 0.1) - po.objective(T, Um, 0.1)) / (2 * h)
+            assert abs(fd - G[mode][r, f]) < 1e-5 * max(1, abs(fd))
+
+
+def test_oracle_als_and_ccdpp_decrease_objective():
+    ind, vals = synth.random_small(3000, (40, 30, 20), seed=6)
+    T = po.Tensor(ind, vals, [40, 30, 20])
+    rng = np.random.default_rng(1)
+    U = [rng.uniform(0, 1, (d, 8)) / np.sqrt(8) for d in (40, 30, 20)]
+    lam = 0.1
+
+    def obj(U):  # the ALS objective: sum of squares + lambda ||U||^2
+        return po.sq_loss(T, U) + po.frob([40, 30, 20], U, lam)
+
+    prev = obj(U)
+    for _ in range(3):
+        for m in range(3):
+            po.als_mode(T.sorted_for_mode(m), m, U, lam)
+            cur = obj(U)
+            assert cur <= prev * (1 + 1e-12)
+            prev = cur
+    U2 = [rng.uniform(0, 1, (d, 8)) / np.sqrt(8) for d in (40, 30, 20)]
+    r = po.residual(T, U2)
+    prev = obj(U2)
+    for _ in range(2):
+        po.ccdpp_outer(T, U2, lam, 2, r)
+        cur = obj(U2)
+        assert cur <= prev * (1 + 1e-12)
+        prev = cur
+    assert np.allclose(r, po.residual(T, U2), atol=1e-9)
+
+
+def test_oracle_omp_variants_agree():
+    ind, vals = synth.random_small(20000, (300, 200, 100), seed=7)
+    T = po.Tensor(ind, vals, [300, 200, 100])
+    rng = np.random.default_rng(2)
+    U = [rng.uniform(0, 1, (d, 16)) / 4 for d in (300, 200, 100)]
+    assert abs(po.sq_loss(T, U) - po.sq_loss(T, U, nthreads=4)) < 1e-8 * po.sq_loss(T, U)
+    Ua = [u.copy() for u in U]
+    Ub = [u.copy() for u in U]
+    Ts = T.sorted_for_mode(1)
+    po.als_mode(Ts, 1, Ua, 0.1)
+    po.als_mode(Ts, 1, Ub, 0.1, nthreads=4)
+    assert max(np.max(np.abs(a - b)) for a, b in zip(Ua, Ub)) < 1e-10
+    ra, rb = po.residual(T, U), po.residual(T, U)
+    Ua = [u.copy() for u in U]
+    Ub = [u.copy() for u in U]
+    po.ccdpp_outer(T, Ua, 0.1, 1, ra)
+    po.ccdpp_outer(T, Ub, 0.1, 1, rb, nthreads=4)
+    assert max(np.max(np.abs(a - b)) for a, b in zip(Ua, Ub)) < 1e-9
+
+
+def test_compat_weights_rules():
+    """Reference lane multiplicities on a hand-made 64-nonzero tensor."""
+    # rows: tile 0 = 32 nonzeros of row 1 (one segment -> all dropped);
+    # tile 1 = rows 2 (10), 3 (22): row 2 is the tile's first segment -> 0,
+    # row 3 ends at lane 31 with head 10 -> lanes 10..31 weight 1, lane 31
+    # gets K - (31 - 10) extra where K = continuation bits among lanes 1..31
+    rows = np.array([1] * 32 + [2] * 10 + [3] * 22, dtype=np.uint64)
+    ind = np.stack([rows, np.arange(64, dtype=np.uint64) % 5 + 1, np.arange(64, dtype=np.uint64) % 7 + 1])
+    T = po.Tensor(ind, np.ones(64), [3, 5, 7])
+    w = po.compat_weights(T, 0, 0)
+    assert np.all(w[:32] == 0)
+    assert np.all(w[32:42] == 0)
+    K = 9 + 21  # continuation lanes: 1..9 (row 2) and 11..31 (row 3)
+    assert np.all(w[42:63] == 1)
+    assert w[63] == 1 + (K - (31 - 10))
