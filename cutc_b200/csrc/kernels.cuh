@@ -155,12 +155,14 @@ __global__ void __launch_bounds__(256) k_sum_partials(const double *__restrict__
 // ---------------------------------------------------------------------
 // SGD (sgpu/sgd.cu:21-143 rule).  A group of G = R/VN lanes handles one
 // tile of consecutive mode-0-sorted nonzeros in order; each lane holds a
-// 16-byte slice of the three rows.  The mode-0 row stays in registers while
-// the row does not change (exact for a sequential order) and is flushed as
-// a delta (atomic) or a store (plain) when it does.
+// 16-byte slice of the three rows.
 //   e = x - sum a.b.c ;  a += s*((e*b*c) - lambda*a) ; b, c likewise from
 //   the pre-update rows, s = lr * step scale.
-// sequential != 0: one group walks all tiles in order (deterministic).
+// sequential != 0: one group walks all tiles in order (deterministic); the
+//   mode-0 row stays in registers while it does not change (exact there).
+// Hogwild: groups run tiles concurrently; each nonzero reads its three rows
+//   fresh and adds its deltas atomically (vector red.add), or stores the new
+//   rows (atomic == 0, lossy under contention).
 // ---------------------------------------------------------------------
 template <typename T, int R>
 __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
@@ -194,21 +196,17 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
         for (uint64_t p = start; p < end; ++p) {
             const uint4 r = rec[p];
             const T x = value_of<T>(r, v64, p);
-            if (r.x != cur) {
-                if (arow) {
-                    if (atomic) {
-                        V d;
-#pragma unroll
-                        for (int v = 0; v < VN; ++v) vset(d, v, vget(a, v) - vget(a0, v));
-                        vatomic_add(arow, d);
-                    } else {
-                        *arow = a;
-                    }
-                }
-                cur = r.x;
+            if (!sequential) {
+                // Hogwild: every row is read fresh and updated per nonzero, so
+                // the staleness of a hot row is bounded by the updates in flight
                 arow = reinterpret_cast<V *>(U0 + (size_t)r.x * R) + gl;
                 a = *arow;
                 a0 = a;
+            } else if (r.x != cur) {
+                if (arow) *arow = a;
+                cur = r.x;
+                arow = reinterpret_cast<V *>(U0 + (size_t)r.x * R) + gl;
+                a = *arow;
             }
             V *brow = reinterpret_cast<V *>(U1 + (size_t)r.y * R) + gl;
             V *crow = reinterpret_cast<V *>(U2 + (size_t)r.z * R) + gl;
@@ -227,7 +225,11 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
                 vset(db, v, s * ((e * av * cv) - lambda * bv));
                 vset(dc, v, s * ((e * bv * av) - lambda * cv));
             }
-            if (atomic) {
+            if (!sequential && atomic) {
+                V da;
+#pragma unroll
+                for (int v = 0; v < VN; ++v) vset(da, v, vget(an, v) - vget(a0, v));
+                vatomic_add(arow, da);
                 vatomic_add(brow, db);
                 vatomic_add(crow, dc);
             } else {
@@ -237,21 +239,13 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
                     vset(bn, v, vget(b, v) + vget(db, v));
                     vset(cn, v, vget(c, v) + vget(dc, v));
                 }
+                if (!sequential) *arow = an;
                 *brow = bn;
                 *crow = cn;
             }
             a = an;
         }
-        if (arow) {
-            if (atomic) {
-                V d;
-#pragma unroll
-                for (int v = 0; v < VN; ++v) vset(d, v, vget(a, v) - vget(a0, v));
-                vatomic_add(arow, d);
-            } else {
-                *arow = a;
-            }
-        }
+        if (sequential && arow) *arow = a;
     }
 }
 
