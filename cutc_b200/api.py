@@ -119,6 +119,7 @@ def lib():
             "ctc_dataset_run": (C.c_int, [P, P, P, C.POINTER(Params), EPOCH_CB, P, C.POINTER(Result)]),
             "ctc_rmse": (C.c_int, [P, P, P, _f64p]),
             "ctc_grad": (C.c_int, [P, P, P, C.c_double, C.POINTER(_f64p), _f64p]),
+            "ctc_sse_noalloc": (C.c_int, [P, C.c_uint64, P, P, P, C.c_int, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -257,6 +257,22 @@ int ctc_ctx_reset_kernel_times(ctc_ctx *ctx);
  * rows read at index-1).  The reduction is deterministic (fixed order). */
 int ctc_rmse(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double *rmse);
 
+/* Squared-error sum over nonzeros already on the device, allocating no
+ * device memory.  No counterpart in the reference.  For callers that cannot
+ * call cudaMalloc (a process whose GPU memory another allocator has fully
+ * reserved, or a loop that cannot take an allocation's device-wide
+ * synchronisation).  rec: n device records {i0, i1, i2, value bits} (uint4,
+ * 0-based indices, FP32 value); U0..U2: device row-major FP32 factors
+ * (dims x rank); out_sse: one device double receiving sum (x - xhat)^2;
+ * stream: a cudaStream_t (NULL = legacy default stream).  Asynchronous.
+ * Scratch is a fixed 512 KiB file-scope device array (65536 partial sums
+ * of 16384 nonzeros), held until exit by every GPU that loads the library:
+ * n above 2^30 is rejected (CTC_E_ARG).  All calls share that array, so
+ * calls that overlap on the GPU race.  The first call on a device looks up
+ * the array's address (make it before any stream capture there). */
+int ctc_sse_noalloc(const void *rec, uint64_t n, const float *U0, const float *U1,
+                    const float *U2, int rank, double *out_sse, void *stream);
+
 /* Adjoint of the masked CP loss 1/2 ||P_Omega(X - [[A,B,C]])||^2 +
  * lambda sum ||U_m||^2: every factor gradient from one pass over the
  * tensor, residuals recomputed, not stored.  grads[m]: dims[m] x rank
