@@ -185,7 +185,56 @@ struct DevTensor {
     uint32_t nheavy = 0;
     DevBuf<T> w;
     bool has_w = false;
+    // CCD++ copies: packed keys, residual, values (no rec)
+    DevBuf<uint64_t> keys;
+    DevBuf<T> res, x;
+    k::KeyShape ks{};
 };
+
+static int bits_for(uint64_t d)
+{
+    int b = 1;
+    while (b < 64 && (1ull << b) < d) ++b;
+    return b;
+}
+
+// CCD++ copy of mode m: 64-bit keys row | q1 | q2 (row = index in mode m,
+// q1/q2 = indices in modes m+1, m+2, each in just enough bits) and the
+// values; the residual is formed on the device.
+template <typename T>
+static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t *dims, bool trunc,
+                       DevTensor<T> &d)
+{
+    const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+    const int b0 = bits_for(dims[m]), b1 = bits_for(dims[m1]), b2 = bits_for(dims[m2]);
+    if (b0 + b1 + b2 > 64) fail(CTC_E_UNSUP, "CCD++ keys need %d bits (> 64) for these dimensions", b0 + b1 + b2);
+    d.ks.s_row = (uint32_t)(b1 + b2);
+    d.ks.s_q1 = (uint32_t)b2;
+    d.ks.m_q1 = (b1 == 64) ? ~0ull : ((1ull << b1) - 1);
+    d.ks.m_q2 = (b2 == 64) ? ~0ull : ((1ull << b2) - 1);
+    const uint64_t n = t->nnz;
+    std::vector<uint64_t> keys(n);
+    std::vector<T> x(n);
+    const uint32_t s_row = d.ks.s_row, s_q1 = d.ks.s_q1;
+    par_for(n, [&](uint64_t b, uint64_t e) {
+        for (uint64_t i = b; i < e; ++i) {
+            keys[i] = ((t->ind[m][i] - 1) << s_row) | ((t->ind[m1][i] - 1) << s_q1) | (t->ind[m2][i] - 1);
+            const double v = trunc ? ctc_value_through_idx(t->vals[i]) : t->vals[i];
+            x[i] = (T)v;
+        }
+    });
+    d.n = (uint32_t)n;
+    d.keys.upload(keys.data(), n, ctx->stream);
+    d.x.upload(x.data(), n, ctx->stream);
+    d.res.alloc(n);
+    CK(cudaStreamSynchronize(ctx->stream));
+}
+
+// nonzeros per lane of the CCD++ pass for a tile length
+static int ccdpp_lanes(int tile_len)
+{
+    return tile_len <= 128 ? 4 : (tile_len <= 256 ? 8 : 16);
+}
 
 static void validate_tensor(const ctc_tensor *t, const uint64_t *dims, const char *what)
 {
@@ -308,11 +357,7 @@ template <typename T>
 struct DatasetImpl : ctc_dataset::Base {
     DevTensor<T> copy[3];
     DevTensor<T> val, test;
-    // CCD++ overwrites the staged values with residuals: the values are kept
-    // (FP32 bits / FP64) to restart from another model
-    DevBuf<uint32_t> orig32[3];
-    DevBuf<double> orig64[3];
-    bool resid_dirty = false;
+    std::vector<uint32_t> rowcnt[3];  // SGD: nonzeros per row of each mode
 };
 
 static int default_tile(int alg)
@@ -332,7 +377,8 @@ static void build_dataset(ctc_dataset *ds, const ctc_tensor *const train[3], con
     ctc_ctx *ctx = ds->ctx;
     const ctc_params &p = ds->p;
     const bool trunc = p.compat != 0;
-    const uint32_t tl = (uint32_t)(p.tile_len > 0 ? p.tile_len : default_tile(p.alg));
+    uint32_t tl = (uint32_t)(p.tile_len > 0 ? p.tile_len : default_tile(p.alg));
+    if (p.alg == CTC_ALG_CCDPP) tl = 32u * (uint32_t)ccdpp_lanes((int)tl);
     std::unique_ptr<ctc_tensor> own[3];
     const ctc_tensor *srt[3] = {train[0], train[1], train[2]};
     const int ncopies = (p.alg == CTC_ALG_SGD) ? 1 : 3;
@@ -344,27 +390,21 @@ static void build_dataset(ctc_dataset *ds, const ctc_tensor *const train[3], con
         }
         if (srt[m]->nnz != train[0]->nnz) fail(CTC_E_ARG, "training copies differ in size");
         validate_tensor(srt[m], ds->dims, "training tensor");
-        stage_tensor<T>(ctx, srt[m], trunc, impl->copy[m]);
+        if (p.alg == CTC_ALG_CCDPP) stage_keys<T>(ctx, srt[m], m, ds->dims, trunc, impl->copy[m]);
+        else stage_tensor<T>(ctx, srt[m], trunc, impl->copy[m]);
         if (p.alg != CTC_ALG_SGD) stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
         if (trunc && (p.alg == CTC_ALG_ALS || p.alg == CTC_ALG_CCD))
             stage_weights<T>(ctx, srt[m], m, p.alg == CTC_ALG_CCD ? 1 : 0, impl->copy[m]);
-        if (p.alg == CTC_ALG_CCDPP) {
-            DevTensor<T> &c = impl->copy[m];
-            if (std::is_same<T, double>::value) {
-                impl->orig64[m].alloc(c.n);
-                CK(cudaMemcpyAsync(impl->orig64[m].p, c.v64.p, (size_t)c.n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
-            } else {
-                impl->orig32[m].alloc(c.n);
-                CK(cudaMemcpy2DAsync(impl->orig32[m].p, 4, reinterpret_cast<const char *>(c.rec.p) + 12, 16, 4, c.n,
-                                     cudaMemcpyDeviceToDevice, ctx->stream));
-            }
-            CK(cudaStreamSynchronize(ctx->stream));
-        }
     }
     if (p.alg == CTC_ALG_SGD) {
         // SGD tiles are plain chunks of the mode-1 order (sgpu/sgd.cu:32-34)
         impl->copy[0].mode = 0;
         impl->copy[0].ntiles = (uint32_t)((impl->copy[0].n + tl - 1) / tl);
+        for (int m = 0; m < 3; ++m) {
+            impl->rowcnt[m].assign(ds->dims[m], 0);
+            const uint64_t *ind = srt[0]->ind[m].data();
+            for (uint64_t i = 0; i < srt[0]->nnz; ++i) impl->rowcnt[m][ind[i] - 1]++;
+        }
     }
     if (val) {
         validate_tensor(val, ds->dims, "validation tensor");
@@ -386,7 +426,9 @@ struct Session : SessionBase {
     uint32_t dims[3];
     bool colmajor;
     uint32_t tile_len;
-    DevBuf<T> U[3], Ubest[3], Urow[3], old[3], slot, slot2, lr_dev, zrow;
+    DevBuf<T> U[3], Ubest[3], Urow[3], slot, slot2, lr_dev;
+    DevBuf<k::Pack3<T>> pk[3];  // CCD++ per-column {cur, prev, old}
+    DevBuf<unsigned int> hcnt[3];  // CCD++ pieces arrived per heavy row (reset by the finaliser)
     DevBuf<unsigned long long> nonspd_dev;
     cudaGraphExec_t graph = nullptr;
     bool model_set = false;
@@ -405,7 +447,9 @@ struct Session : SessionBase {
             Ubest[m].alloc(sz);
             if (colmajor) {
                 Urow[m].alloc(sz);
-                old[m].alloc(dims[m]);
+                pk[m].alloc(dims[m]);
+                hcnt[m].alloc(D->copy[m].nheavy);
+                CK(cudaMemsetAsync(hcnt[m].p, 0, hcnt[m].n * sizeof(unsigned int), ctx->stream));
             }
         }
         // scratch sized once so an epoch can be captured as a graph
@@ -419,9 +463,6 @@ struct Session : SessionBase {
         }
         slot.alloc(need);
         if (p.alg == CTC_ALG_CCDPP) slot2.alloc(need);
-        uint32_t mx = std::max(dims[0], std::max(dims[1], dims[2]));
-        zrow.alloc((size_t)mx * R);
-        CK(cudaMemsetAsync(zrow.p, 0, (size_t)mx * R * sizeof(T), ctx->stream));
         if (p.alg == CTC_ALG_ALS) {
             using Sh = k::AlsShape<R>;
             const int smem = (int)(4 * Sh::smem_doubles * sizeof(double));
@@ -445,6 +486,39 @@ struct Session : SessionBase {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
         }
+        damp_ready = false;
+    }
+
+    // Hogwild step scale per row: min(1, K / (G * nnz(row) / nnz)), G the
+    // groups in flight (see ctc_params.sgd_conflicts)
+    DevBuf<float> damp[3];
+    bool damp_ready = false, damp_on = false;
+    unsigned sgd_grid(int gpb) const
+    {
+        const unsigned cap = p.sgd_groups > 0 ? (unsigned)std::max(1, p.sgd_groups / gpb) : kSMs * 8;
+        return grid_for(D->copy[0].ntiles, gpb, cap);
+    }
+    void prepare_damping(int gpb)
+    {
+        damp_ready = true;
+        damp_on = false;
+        if (p.sgd_order == CTC_SGD_SEQUENTIAL || p.sgd_conflicts < 0) return;
+        const double K = p.sgd_conflicts > 0 ? (double)p.sgd_conflicts : 128.0;
+        const double G = std::min<double>((double)sgd_grid(gpb) * gpb, (double)D->copy[0].ntiles);
+        const double n = (double)D->copy[0].n;
+        for (int m = 0; m < 3; ++m) {
+            std::vector<float> h(dims[m], 1.0f);
+            const auto &cnt = D->rowcnt[m];
+            for (size_t r = 0; r < cnt.size() && r < h.size(); ++r) {
+                const double conc = G * (double)cnt[r] / n;
+                if (conc > K) {
+                    h[r] = (float)(K / conc);
+                    damp_on = true;
+                }
+            }
+            damp[m].upload(h.data(), h.size(), ctx->stream);
+        }
+        CK(cudaStreamSynchronize(ctx->stream));
     }
 
     void set_model(const ctc_model *mdl) override
@@ -464,21 +538,7 @@ struct Session : SessionBase {
         }
         CK(cudaMemsetAsync(nonspd_dev.p, 0, sizeof(unsigned long long), ctx->stream));
         set_lr(p.lr * (p.lr_scale > 0 ? p.lr_scale : 1.0));
-        if (colmajor) {
-            if (D->resid_dirty) {
-                for (int m = 0; m < 3; ++m) {
-                    DevTensor<T> &c = D->copy[m];
-                    if (std::is_same<T, double>::value)
-                        CK(cudaMemcpyAsync(c.v64.p, D->orig64[m].p, (size_t)c.n * 8, cudaMemcpyDeviceToDevice,
-                                           ctx->stream));
-                    else
-                        CK(cudaMemcpy2DAsync(reinterpret_cast<char *>(c.rec.p) + 12, 16, D->orig32[m].p, 4, 4, c.n,
-                                             cudaMemcpyDeviceToDevice, ctx->stream));
-                }
-            }
-            ccdpp_init();
-            D->resid_dirty = true;
-        }
+        if (colmajor) ccdpp_init();
         CK(cudaStreamSynchronize(ctx->stream));
         model_set = true;
     }
@@ -579,73 +639,91 @@ struct Session : SessionBase {
         constexpr int G = R / k::Vec<T>::n;
         const int gpb = 8 * (32 / G);  // groups per 256-thread block
         const bool seq = p.sgd_order == CTC_SGD_SEQUENTIAL;
-        const unsigned g = seq ? 1 : grid_for(c.ntiles, gpb, kSMs * 8);
+        const unsigned g = seq ? 1 : sgd_grid(gpb);
+        const float *d0 = damp_on ? damp[0].p : nullptr;
+        const float *d1 = damp_on ? damp[1].p : nullptr;
+        const float *d2 = damp_on ? damp[2].p : nullptr;
+        // a prime stride that does not divide the tile count
+        uint64_t stride = 1;
+        if (!seq) {
+            for (uint64_t pr : {1000003ull, 999983ull, 999979ull, 104729ull})
+                if (c.ntiles % pr != 0) {
+                    stride = pr % c.ntiles ? pr : 1;
+                    break;
+                }
+        }
         LAUNCH(ctx, k::k_sgd<T, R>, g, seq ? 32 : 256, 0, (const uint4 *)c.rec.p, (const double *)c.v64.p, c.n,
                tile_len, c.ntiles, U[0].p, U[1].p, U[2].p, (const T *)lr_dev.p, (T)p.lambda, p.sgd_atomic,
-               seq ? 1 : 0);
-    }
-
-    k::CcdCols cols_for(int f, int fprev, int m)
-    {
-        k::CcdCols c{};
-        for (int n = 0; n < 3; ++n) {
-            c.cur[n] = U[n].p + (size_t)f * dims[n];
-            c.prev[n] = fprev < 0 ? nullptr
-                                  : (fprev == f ? (const void *)old[n].p
-                                                : (const void *)(U[n].p + (size_t)fprev * dims[n]));
-            c.old[n] = old[n].p;
-        }
-        c.out = m >= 0 ? (void *)(U[m].p + (size_t)f * dims[m]) : nullptr;
-        return c;
+               seq ? 1 : 0, stride, d0, d1, d2);
     }
 
     void ccdpp_init()
     {
+        for (int m = 0; m < 3; ++m)
+            LAUNCH(ctx, k::k_col_to_row<T>, grid_for((uint64_t)dims[m] * R, 256, kSMs * 8), 256, 0,
+                   (const T *)U[m].p, Urow[m].p, dims[m], R);
         for (int m = 0; m < 3; ++m) {
             DevTensor<T> &c = D->copy[m];
-            LAUNCH(ctx, k::k_ccd_resid_init<T, R>, grid_for(c.n, 256, kSMs * 16), 256, 0, c.rec.p, c.v64.p, c.n,
-                   (const T *)U[0].p, (const T *)U[1].p, (const T *)U[2].p, dims[0], dims[1], dims[2]);
+            LAUNCH(ctx, k::k_ccdpp_init<T, R>, grid_for(c.n, 256, kSMs * 16), 256, 0, (const uint64_t *)c.keys.p,
+                   (const T *)c.x.p, c.res.p, c.n, c.ks, m, (const T *)Urow[0].p, (const T *)Urow[1].p,
+                   (const T *)Urow[2].p);
         }
     }
 
-    // One CCD++ outer iteration: per column f, `inner` sweeps over the modes
-    // of the column update (the first sweep of each copy also refreshes its
-    // residual), then a finish pass per copy leaves r = x - model in every
+    template <int E>
+    void ccdpp_pass(int m, int f, bool first)
+    {
+        DevTensor<T> &c = D->copy[m];
+        const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+        T *out = U[m].p + (size_t)f * dims[m];
+        const unsigned g = grid_for(c.ntiles, 8, kSMs * 8);
+        if (first)
+            LAUNCH(ctx, k::k_ccdpp_pass<T, true, E>, g, 256, 0, (const int4 *)c.tiles.p, c.ntiles,
+                   (const uint64_t *)c.keys.p, c.res.p, c.ks, pk[m].p, (const k::Pack3<T> *)pk[m1].p,
+                   (const k::Pack3<T> *)pk[m2].p, out, (T)p.lambda, slot.p, slot2.p, (const uint4 *)c.heavy.p,
+                   hcnt[m].p);
+        else
+            LAUNCH(ctx, k::k_ccdpp_pass<T, false, E>, g, 256, 0, (const int4 *)c.tiles.p, c.ntiles,
+                   (const uint64_t *)c.keys.p, c.res.p, c.ks, pk[m].p, (const k::Pack3<T> *)pk[m1].p,
+                   (const k::Pack3<T> *)pk[m2].p, out, (T)p.lambda, slot.p, slot2.p, (const uint4 *)c.heavy.p,
+                   hcnt[m].p);
+    }
+
+    // One CCD++ outer iteration: per column f, the {cur, prev, old} packs,
+    // then `inner` sweeps over the modes of the column update (the first
+    // sweep of each copy also refreshes its residual); finally one pass per
+    // copy removes the last column's term, leaving r = x - model in every
     // copy and the training SSE in scalars[0].
     void ccdpp_outer()
     {
         const int inner = p.inner > 0 ? p.inner : 1;
+        const int lanes = ccdpp_lanes((int)tile_len);
         for (int f = 0; f < R; ++f) {
-            for (int n = 0; n < 3; ++n)
-                CK(cudaMemcpyAsync(old[n].p, U[n].p + (size_t)f * dims[n], dims[n] * sizeof(T),
-                                   cudaMemcpyDeviceToDevice, ctx->stream));
+            k::PackArgs pa{};
+            for (int n = 0; n < 3; ++n) {
+                pa.pk[n] = pk[n].p;
+                pa.col[n] = U[n].p + (size_t)f * dims[n];
+                pa.pcol[n] = f > 0 ? (const void *)(U[n].p + (size_t)(f - 1) * dims[n]) : nullptr;
+                pa.dims[n] = dims[n];
+            }
+            LAUNCH(ctx, k::k_ccdpp_pack<T>, grid_for((uint64_t)dims[0] + dims[1] + dims[2], 256, kSMs * 8), 256, 0,
+                   pa);
             for (int it = 0; it < inner; ++it) {
                 for (int q = 0; q < 3; ++q) {
                     const int m = (p.mode_start + q) % 3;
-                    DevTensor<T> &c = D->copy[m];
-                    k::CcdCols cols = cols_for(f, f > 0 ? f - 1 : -1, m);
                     CK(cudaMemsetAsync(U[m].p + (size_t)f * dims[m], 0, dims[m] * sizeof(T), ctx->stream));
-                    const unsigned g = grid_for(c.ntiles, 8, kSMs * 8);
-                    if (it == 0)
-                        LAUNCH(ctx, k::k_ccd_pass<T, true>, g, 256, 0, (const int4 *)c.tiles.p, c.ntiles, c.rec.p,
-                               c.v64.p, m, cols, (T)p.lambda, slot.p, slot2.p);
-                    else
-                        LAUNCH(ctx, k::k_ccd_pass<T, false>, g, 256, 0, (const int4 *)c.tiles.p, c.ntiles, c.rec.p,
-                               c.v64.p, m, cols, (T)p.lambda, slot.p, slot2.p);
-                    if (c.nheavy)
-                        LAUNCH(ctx, k::k_ccd_fix<T>, grid_for(c.nheavy, 8, kSMs * 8), 256, 0, (const uint4 *)c.heavy.p,
-                               c.nheavy, (const T *)slot.p, (const T *)slot2.p, (T *)cols.out, (T)p.lambda);
+                    if (lanes == 4) ccdpp_pass<4>(m, f, it == 0);
+                    else if (lanes == 8) ccdpp_pass<8>(m, f, it == 0);
+                    else ccdpp_pass<16>(m, f, it == 0);
                 }
             }
         }
         for (int m = 0; m < 3; ++m) {
             DevTensor<T> &c = D->copy[m];
-            k::CcdCols cols = cols_for(R - 1, R - 1, -1);
-            // the last column's final values (not the snapshot)
-            for (int n = 0; n < 3; ++n) cols.prev[n] = U[n].p + (size_t)(R - 1) * dims[n];
             const unsigned g = grid_for(c.n, 256, kMaxPartials);
-            LAUNCH(ctx, k::k_ccd_finish<T>, g, 256, 0, c.rec.p, c.v64.p, c.n, cols,
-                   m == 0 ? ctx->partial.p : (double *)nullptr);
+            LAUNCH(ctx, k::k_ccdpp_finish<T>, g, 256, 0, (const uint64_t *)c.keys.p, c.res.p, c.n, c.ks, m,
+                   (const T *)(U[0].p + (size_t)(R - 1) * dims[0]), (const T *)(U[1].p + (size_t)(R - 1) * dims[1]),
+                   (const T *)(U[2].p + (size_t)(R - 1) * dims[2]), m == 0 ? ctx->partial.p : (double *)nullptr);
             if (m == 0)
                 LAUNCH(ctx, k::k_sum_partials, 1, 256, 0, (const double *)ctx->partial.p, (int)g, ctx->scalars.p + 0);
         }
@@ -664,6 +742,7 @@ struct Session : SessionBase {
     void epochs(int n) override
     {
         if (!model_set) fail(CTC_E_ARG, "no model staged on the dataset");
+        if (p.alg == CTC_ALG_SGD && !damp_ready) prepare_damping(8 * (32 / (R / k::Vec<T>::n)));
         const bool use_graph = p.use_graph && !ctx->kt.on && p.sgd_order != CTC_SGD_SEQUENTIAL;
         for (int i = 0; i < n; ++i) {
             if (!use_graph) {
@@ -707,8 +786,7 @@ struct Session : SessionBase {
         }
         if (colmajor) {
             // copy 0 holds r = x - model: its SSE is the sum of squares
-            const T *z[3] = {zrow.p, zrow.p, zrow.p};
-            sse_into(D->copy[0], z, 0);
+            sumsq_into(D->copy[0].res.p, D->copy[0].n, 0);
         } else {
             sse_into(D->copy[0], Urm, 0);
         }

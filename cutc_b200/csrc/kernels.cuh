@@ -169,7 +169,10 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
                                              const double *__restrict__ v64, uint32_t n,
                                              uint32_t tile_len, uint32_t ntiles, T *U0, T *U1,
                                              T *U2, const T *__restrict__ lr_dev, T lambda,
-                                             int atomic, int sequential)
+                                             int atomic, int sequential, uint64_t tile_stride,
+                                             const float *__restrict__ damp0,
+                                             const float *__restrict__ damp1,
+                                             const float *__restrict__ damp2)
 {
     using V = typename Vec<T>::type;
     constexpr int VN = Vec<T>::n;
@@ -187,7 +190,11 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
         ngroups = 1;
     }
     const T s = *lr_dev;
-    for (uint64_t tile = group; tile < ntiles; tile += ngroups) {
+    for (uint64_t t = group; t < ntiles; t += ngroups) {
+        // Hogwild: tiles in flight together are spread over the tensor
+        // (tile_stride is coprime to ntiles), so a long row of the sorted
+        // mode is not updated by every group at once; sequential: stride 1
+        const uint64_t tile = (t * tile_stride) % ntiles;
         const uint64_t start = tile * tile_len;
         const uint64_t end = min(start + tile_len, (uint64_t)n);
         uint32_t cur = kNoKey;
@@ -217,13 +224,19 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
 #pragma unroll
             for (int o = G / 2; o > 0; o >>= 1) part += __shfl_xor_sync(gmask, part, o);
             const T e = x - part;
+            T sa = s, sb = s, sc = s;
+            if (damp0) {
+                sa *= (T)damp0[r.x];
+                sb *= (T)damp1[r.y];
+                sc *= (T)damp2[r.z];
+            }
             V an, db, dc;
 #pragma unroll
             for (int v = 0; v < VN; ++v) {
                 const T av = vget(a, v), bv = vget(b, v), cv = vget(c, v);
-                vset(an, v, av + s * ((e * bv * cv) - lambda * av));
-                vset(db, v, s * ((e * av * cv) - lambda * bv));
-                vset(dc, v, s * ((e * bv * av) - lambda * cv));
+                vset(an, v, av + sa * ((e * bv * cv) - lambda * av));
+                vset(db, v, sb * ((e * av * cv) - lambda * bv));
+                vset(dc, v, sc * ((e * bv * av) - lambda * cv));
             }
             if (!sequential && atomic) {
                 V da;
@@ -250,152 +263,277 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
 }
 
 // ---------------------------------------------------------------------
-// CCD++ column pass for mode m, column f (column-major factors).  Lane per
-// nonzero, 32 at a time through the tile; per-row sums of r*h and h*h by a
-// segmented warp scan on the (sorted) row keys, carried across sub-tiles;
-// the row's warp writes u = num / (lambda + den).  FIRST: the pass also
-// refreshes the stored residual of this copy:
-//   r <- r - term(fprev, final) + term(f, snapshot before this column).
+// CCD++ (rank-one column updates).  Each mode copy of the training tensor
+// is kept as packed 64-bit keys (row | q1 | q2, the row index of the copy's
+// mode and the indices of the next two modes) plus a separate residual
+// array, 12 bytes per nonzero.  Per column f, pack[n][row] holds
+// {current value of column f, final value of column f-1, value of column f
+// before its sweeps} for every mode n, so one 16-byte (FP32) gather per
+// nonzero and mode serves a pass.
+//
+// Pass for mode m (k_ccdpp_pass): a warp owns a row-aligned tile; lane l
+// walks E consecutive nonzeros, accumulating r*h and h*h per run of equal
+// rows (h = product of the other two modes' column f); runs inside a lane
+// are finished there, runs crossing lanes are joined by one segmented warp
+// scan over the lanes' last runs.  The row's owner writes
+// u = sum(r h) / (lambda + sum h^2) into the column and into pack[m].cur.
+// FIRST (the first sweep of column f over this copy) also refreshes the
+// stored residual:  r <- r - term(f-1, final) + term(f, before sweeps),
+// which is the rank-one add-back of f fused with the subtraction of f-1.
 // ---------------------------------------------------------------------
-struct CcdCols {
-    const void *cur[3];   // column f, current values
-    const void *prev[3];  // column fprev (final) or null
-    const void *old[3];   // snapshot of column f before its sweeps
-    void *out;            // column f of mode m
+struct KeyShape {
+    uint32_t s_row, s_q1;   // key >> s_row = row ; (key >> s_q1) & m_q1 = q1
+    uint64_t m_q1, m_q2;    // key & m_q2 = q2
+};
+
+__device__ __forceinline__ void unpack_key(uint64_t k, const KeyShape &ks, uint32_t &row, uint32_t &q1,
+                                           uint32_t &q2)
+{
+    row = (uint32_t)(k >> ks.s_row);
+    q1 = (uint32_t)((k >> ks.s_q1) & ks.m_q1);
+    q2 = (uint32_t)(k & ks.m_q2);
+}
+
+template <typename T>
+struct alignas(4 * sizeof(T)) Pack3 {
+    T cur, prev, old, pad;
 };
 
 template <typename T>
-__device__ __forceinline__ T term3(const void *const *c, const uint4 &r)
+__device__ __forceinline__ void ccdpp_finalize(uint32_t row, T nu, T de, T lambda, T *out, Pack3<T> *pkm)
 {
-    return static_cast<const T *>(c[0])[r.x] * static_cast<const T *>(c[1])[r.y] *
-           static_cast<const T *>(c[2])[r.z];
+    const T u = nu / (lambda + de);
+    out[row] = u;
+    pkm[row].cur = u;
 }
 
-template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256) k_ccd_pass(const int4 *__restrict__ tiles, uint32_t ntiles,
-                                                  uint4 *rec, double *v64, int m, CcdCols cols,
-                                                  T lambda, T *__restrict__ slot_nu,
-                                                  T *__restrict__ slot_de)
+template <typename T, bool FIRST, int E>
+__global__ void __launch_bounds__(256) k_ccdpp_pass(const int4 *__restrict__ tiles, uint32_t ntiles,
+                                                    const uint64_t *__restrict__ keys, T *__restrict__ res,
+                                                    KeyShape ks, Pack3<T> *pkm, const Pack3<T> *__restrict__ pa,
+                                                    const Pack3<T> *__restrict__ pb, T *out, T lambda,
+                                                    T *__restrict__ slot_nu, T *__restrict__ slot_de,
+                                                    const uint4 *__restrict__ heavy, unsigned int *hcnt)
 {
+    constexpr uint32_t kNone = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
-    const T *h1 = static_cast<const T *>(cols.cur[m1]);
-    const T *h2 = static_cast<const T *>(cols.cur[m2]);
-    T *out = static_cast<T *>(cols.out);
     for (uint64_t tile = warp; tile < ntiles; tile += nwarps) {
         const int4 td = tiles[tile];
-        const uint32_t start = (uint32_t)td.x, end = (uint32_t)td.x + (uint32_t)td.y;
-        const bool heavy = td.z >= 0;
-        uint32_t ckey = kNoKey;
-        T cnu = 0, cde = 0;
-        for (uint32_t base = start; base < end; base += 32) {
-            const uint32_t idx = base + lane;
-            const bool valid = idx < end;
-            uint32_t key = kNoKey - 1;
+        const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
+        if (td.z >= 0) {
+            // one piece of a long row: warp reduction into the piece's slot;
+            // the piece that arrives last (counter) sums all pieces of the
+            // row in piece order and finalises it -- no waiting anywhere
+            uint32_t row, q1, q2;
+            unpack_key(keys[start], ks, row, q1, q2);
+            Pack3<T> pm{};
+            if constexpr (FIRST) pm = pkm[row];
             T nu = 0, de = 0;
-            if (valid) {
-                uint4 r = rec[idx];
-                key = key_of(r, m);
-                T res = value_of<T>(r, v64, idx);
+            for (uint32_t p = start + lane; p < end; p += 32) {
+                unpack_key(keys[p], ks, row, q1, q2);
+                const Pack3<T> ga = pa[q1], gb = pb[q2];
+                T r = res[p];
                 if constexpr (FIRST) {
-                    if (cols.prev[0]) res -= term3<T>(cols.prev, r);
-                    res += term3<T>(cols.old, r);
-                    store_value<T>(rec, v64, idx, res);
+                    r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
+                    res[p] = r;
                 }
-                const uint32_t q1 = key_of(r, m1), q2 = key_of(r, m2);
-                const T h = h1[q1] * h2[q2];
-                nu = res * h;
-                de = h * h;
+                const T h = ga.cur * gb.cur;
+                nu += r * h;
+                de += h * h;
             }
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t k2 = __shfl_up_sync(0xffffffffu, key, d);
-                const T n2 = __shfl_up_sync(0xffffffffu, nu, d);
-                const T d2 = __shfl_up_sync(0xffffffffu, de, d);
-                if (lane >= d && k2 == key) {
-                    nu += n2;
-                    de += d2;
+            for (int o = 16; o > 0; o >>= 1) {
+                nu += __shfl_xor_sync(0xffffffffu, nu, o);
+                de += __shfl_xor_sync(0xffffffffu, de, o);
+            }
+            const uint4 hr = heavy[td.z];
+            unsigned int last = 0;
+            if (lane == 0) {
+                slot_nu[tile] = nu;
+                slot_de[tile] = de;
+                __threadfence();
+                last = atomicAdd(&hcnt[td.z], 1u) == hr.z - 1 ? 1u : 0u;
+            }
+            last = __shfl_sync(0xffffffffu, last, 0);
+            if (last) {
+                __threadfence();
+                T sn = 0, sd = 0;
+                for (uint32_t q = lane; q < hr.z; q += 32) {
+                    sn += __ldcg(&slot_nu[hr.y + q]);
+                    sd += __ldcg(&slot_de[hr.y + q]);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    sn += __shfl_xor_sync(0xffffffffu, sn, o);
+                    sd += __shfl_xor_sync(0xffffffffu, sd, o);
+                }
+                if (lane == 0) {
+                    ccdpp_finalize<T>(hr.x, sn, sd, lambda, out, pkm);
+                    hcnt[td.z] = 0;
                 }
             }
-            if (key == ckey) {
-                nu += cnu;
-                de += cde;
-            }
-            uint32_t nkey = __shfl_down_sync(0xffffffffu, key, 1);
-            if (lane == 31) nkey = (base + 32 < end) ? key_of(rec[base + 32], m) : kNoKey - 2;
-            const bool tail = valid && nkey != key;
-            if (tail) {
-                if (heavy) {
-                    slot_nu[tile] = nu;
-                    slot_de[tile] = de;
-                } else {
-                    out[key] = nu / (lambda + de);
-                }
-            }
-            const bool cont = valid && lane == 31 && nkey == key;
-            ckey = __shfl_sync(0xffffffffu, cont ? key : kNoKey, 31);
-            cnu = __shfl_sync(0xffffffffu, nu, 31);
-            cde = __shfl_sync(0xffffffffu, de, 31);
+            continue;
         }
+        const uint32_t base = start + (uint32_t)lane * E;
+        const int cnt = base < end ? (int)min((uint32_t)E, end - base) : 0;
+        uint32_t hk = kNone, tk = kNone;
+        T hn = 0, hd = 0, tn = 0, tdd = 0;
+        int nruns = 0;
+        Pack3<T> pm{};
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            if (e < cnt) {
+                uint32_t row, q1, q2;
+                unpack_key(keys[base + e], ks, row, q1, q2);
+                if (row != tk) {
+                    if (nruns == 1) {
+                        hk = tk;
+                        hn = tn;
+                        hd = tdd;
+                    } else if (nruns >= 2) {
+                        ccdpp_finalize<T>(tk, tn, tdd, lambda, out, pkm);
+                    }
+                    tk = row;
+                    tn = tdd = 0;
+                    ++nruns;
+                    if constexpr (FIRST) pm = pkm[row];
+                }
+                const Pack3<T> ga = pa[q1], gb = pb[q2];
+                T r = res[base + e];
+                if constexpr (FIRST) {
+                    r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
+                    res[base + e] = r;
+                }
+                const T h = ga.cur * gb.cur;
+                tn += r * h;
+                tdd += h * h;
+            }
+        }
+        // join runs across lanes: segmented inclusive scan of the last runs
+        const uint32_t in_key = nruns >= 2 ? hk : tk;
+        const uint32_t out_key = tk;
+        uint32_t prev_out = __shfl_up_sync(0xffffffffu, out_key, 1);
+        uint32_t next_in = __shfl_down_sync(0xffffffffu, in_key, 1);
+        if (lane == 0) prev_out = kNone;
+        if (lane == 31) next_in = kNone;
+        int flag = !(nruns == 1 && in_key == prev_out);
+        T sn = tn, sd = tdd;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const T n2 = __shfl_up_sync(0xffffffffu, sn, d);
+            const T d2 = __shfl_up_sync(0xffffffffu, sd, d);
+            const int f2 = __shfl_up_sync(0xffffffffu, flag, d);
+            if (lane >= d) {
+                if (!flag) {
+                    sn += n2;
+                    sd += d2;
+                }
+                flag |= f2;
+            }
+        }
+        const T psn = __shfl_up_sync(0xffffffffu, sn, 1);
+        const T psd = __shfl_up_sync(0xffffffffu, sd, 1);
+        if (nruns >= 2) {
+            T n = hn, d = hd;
+            if (lane > 0 && hk == prev_out) {
+                n += psn;
+                d += psd;
+            }
+            ccdpp_finalize<T>(hk, n, d, lambda, out, pkm);
+        }
+        if (nruns >= 1 && next_in != out_key) ccdpp_finalize<T>(out_key, sn, sd, lambda, out, pkm);
     }
 }
 
-// Heavy rows: sum the per-piece partials in piece order, finalise.
+// pack[n][row] = {U_n(row, f), U_n(row, f-1) or 0, U_n(row, f), 0} for the
+// three modes (column-major factors), before the sweeps of column f.
+struct PackArgs {
+    void *pk[3];
+    const void *col[3];   // column f
+    const void *pcol[3];  // column f-1 or null
+    uint32_t dims[3];
+};
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_ccd_fix(const uint4 *__restrict__ heavy, uint32_t nheavy,
-                                                 const T *__restrict__ slot_nu,
-                                                 const T *__restrict__ slot_de, T *out, T lambda)
+__global__ void k_ccdpp_pack(PackArgs a)
 {
-    const int lane = threadIdx.x & 31;
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t h = warp; h < nheavy; h += nwarps) {
-        const uint4 hr = heavy[h];
-        T nu = 0, de = 0;
-        for (uint32_t q = lane; q < hr.z; q += 32) {
-            nu += slot_nu[hr.y + q];
-            de += slot_de[hr.y + q];
+    const uint64_t total = (uint64_t)a.dims[0] + a.dims[1] + a.dims[2];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        int n = 0;
+        uint64_t r = i;
+        if (r >= a.dims[0]) {
+            r -= a.dims[0];
+            n = 1;
+            if (r >= a.dims[1]) {
+                r -= a.dims[1];
+                n = 2;
+            }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            nu += __shfl_xor_sync(0xffffffffu, nu, o);
-            de += __shfl_xor_sync(0xffffffffu, de, o);
-        }
-        if (lane == 0) out[hr.x] = nu / (lambda + de);
+        const T c = static_cast<const T *>(a.col[n])[r];
+        const T p = a.pcol[n] ? static_cast<const T *>(a.pcol[n])[r] : T(0);
+        Pack3<T> v;
+        v.cur = c;
+        v.prev = p;
+        v.old = c;
+        v.pad = 0;
+        static_cast<Pack3<T> *>(a.pk[n])[r] = v;
     }
 }
 
-// r = x - sum_f U0(i0,f) U1(i1,f) U2(i2,f)   (column-major factors)
+// indices of the three modes from a key of the mode-m copy
+__device__ __forceinline__ void key_modes(uint64_t k, const KeyShape &ks, int m, uint32_t idx[3])
+{
+    uint32_t row, q1, q2;
+    unpack_key(k, ks, row, q1, q2);
+    idx[m] = row;
+    idx[(m + 1) % 3] = q1;
+    idx[(m + 2) % 3] = q2;
+}
+
+// res = x - sum_f U0(i0,f) U1(i1,f) U2(i2,f), row-major factors
 template <typename T, int R>
-__global__ void __launch_bounds__(256) k_ccd_resid_init(uint4 *rec, double *v64, uint32_t n,
-                                                        const T *__restrict__ U0,
-                                                        const T *__restrict__ U1,
-                                                        const T *__restrict__ U2, uint32_t d0,
-                                                        uint32_t d1, uint32_t d2)
+__global__ void __launch_bounds__(256) k_ccdpp_init(const uint64_t *__restrict__ keys, const T *__restrict__ x,
+                                                    T *__restrict__ res, uint32_t n, KeyShape ks, int m,
+                                                    const T *__restrict__ U0, const T *__restrict__ U1,
+                                                    const T *__restrict__ U2)
 {
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
-        const uint4 r = rec[idx];
-        T p = 0;
-#pragma unroll 8
-        for (int f = 0; f < R; ++f)
-            p += U0[(size_t)f * d0 + r.x] * U1[(size_t)f * d1 + r.y] * U2[(size_t)f * d2 + r.z];
-        store_value<T>(rec, v64, idx, value_of<T>(r, v64, idx) - p);
+    using V = typename Vec<T>::type;
+    constexpr int VN = Vec<T>::n;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        uint32_t idx[3];
+        key_modes(keys[p], ks, m, idx);
+        const V *a = reinterpret_cast<const V *>(U0 + (size_t)idx[0] * R);
+        const V *b = reinterpret_cast<const V *>(U1 + (size_t)idx[1] * R);
+        const V *c = reinterpret_cast<const V *>(U2 + (size_t)idx[2] * R);
+        T s = 0;
+#pragma unroll
+        for (int q = 0; q < R / VN; ++q) {
+            const V va = a[q], vb = b[q], vc = c[q];
+#pragma unroll
+            for (int v = 0; v < VN; ++v) s += vget(va, v) * vget(vb, v) * vget(vc, v);
+        }
+        res[p] = x[p] - s;
     }
 }
 
-// r -= term(column c) ; optional SSE partials of the new residual.
+// res -= U0(i0,c) U1(i1,c) U2(i2,c) for one column c (column-major
+// pointers); optional SSE partials of the new residual.
 template <typename T>
-__global__ void __launch_bounds__(256) k_ccd_finish(uint4 *rec, double *v64, uint32_t n,
-                                                    CcdCols cols, double *partial)
+__global__ void __launch_bounds__(256) k_ccdpp_finish(const uint64_t *__restrict__ keys, T *__restrict__ res,
+                                                      uint32_t n, KeyShape ks, int m, const T *__restrict__ c0,
+                                                      const T *__restrict__ c1, const T *__restrict__ c2,
+                                                      double *__restrict__ partial)
 {
     double acc = 0;
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
-        const uint4 r = rec[idx];
-        T res = value_of<T>(r, v64, idx) - term3<T>(cols.prev, r);
-        store_value<T>(rec, v64, idx, res);
-        acc += (double)res * (double)res;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        uint32_t idx[3];
+        key_modes(keys[p], ks, m, idx);
+        const T r = res[p] - c0[idx[0]] * c1[idx[1]] * c2[idx[2]];
+        res[p] = r;
+        acc += (double)r * (double)r;
     }
     if (partial) {
         acc = block_sum(acc);

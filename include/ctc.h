@@ -178,6 +178,13 @@ typedef struct {
     int eval_every;        /* evaluate RMSE every n epochs (0 = only at the end)    */
     int use_graph;         /* capture the epoch in a CUDA graph when possible       */
     uint64_t seed;         /* reserved for stochastic modes                          */
+    int sgd_groups;        /* Hogwild: nonzero groups in flight (0 = default)       */
+    int sgd_conflicts;     /* Hogwild: bound K on the expected number of in-flight
+                              updates of one row, G * nnz(row) / nnz; rows above it
+                              take steps scaled by K / that number, so a hot row
+                              moves by at most ~K single steps per wave of stale
+                              updates (0 = 128, < 0 = no scaling).  With one group
+                              in flight (sequential order) no row is scaled.       */
 } ctc_params;
 
 /* Reference-default parameters for an algorithm (sgpu/base.h:19-64). */
