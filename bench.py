@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--sample", type=int, default=2_000_000, help="CPU baseline sample size")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e / time-to-RMSE / CPU legs")
+    ap.add_argument("--ccdpp-tile", type=int, default=0, help="CCD++ tile length (0 = library default)")
     return ap.parse_args()
 
 
@@ -225,7 +226,8 @@ def run_ours(args):
     base0 = sorted3[0] if (rank == 0 and not args.no_extras) else None
     del sorted3
 
-    p_ccd = ctc.params("ccdpp", rank=R, inner=3, early_stop=0, iters=10, **{"lambda": 0.1})
+    p_ccd = ctc.params("ccdpp", rank=R, inner=3, early_stop=0, iters=10, tile_len=args.ccdpp_tile,
+                       **{"lambda": 0.1})
     p_sgd = ctc.params("sgd", rank=R, lr=1e-3, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY, lr_decay=0.95,
                        early_stop=0, iters=20, **{"lambda": 0.01})
     ds_ccd = ctc.Dataset(ctx, tr, None, te, p_ccd)

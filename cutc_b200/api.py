@@ -48,7 +48,8 @@ class Params(C.Structure):
                 ("early_stop", C.c_int), ("tolerance", C.c_double), ("max_bad_epochs", C.c_int),
                 ("mode_start", C.c_int), ("sgd_order", C.c_int), ("sgd_atomic", C.c_int),
                 ("eval_every", C.c_int), ("use_graph", C.c_int), ("seed", C.c_uint64),
-                ("sgd_groups", C.c_int), ("sgd_conflicts", C.c_int)]
+                ("sgd_groups", C.c_int), ("sgd_conflicts", C.c_int), ("threads_per_row", C.c_int),
+                ("smem_budget", C.c_int)]
 
 
 class EpochStats(C.Structure):

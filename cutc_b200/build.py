@@ -35,7 +35,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "--ex
 
 HOST_SOURCES = ["host.cpp"]
 CUDA_SOURCES = ["engine.cu", "noalloc.cu"]
-HEADERS = ["ctc_internal.h", "kernels.cuh"]
+HEADERS = ["ctc_internal.h", "kernels.cuh", "als_tc.cuh", "ptx.cuh"]
 
 
 def _newer(src_list, out):

@@ -1,0 +1,244 @@
+// als_tc.cuh -- ALS Gram blocks on the 5th-generation tensor cores
+// (tcgen05.mma, accumulator in tensor memory), rank 64, mixed precision.
+//
+// For one piece of a long row (tile_len nonzeros of one row of the mode's
+// sorted copy) the CTA forms
+//     G = sum_k h_k h_k^T      (64 x 64, FP32 in TMEM)
+//     b = sum_k x_k h_k        (64, FP32 on the CUDA cores)
+// with h_k = U_a(q1) o U_b(q2) read from BF16 copies of the factors, and
+// writes them to the piece's slot ({G row-major, b}, the layout the FP64
+// fixup solve k_als_fix reads).
+//
+// The h rows of 128 nonzeros are staged in shared memory as BF16, one
+// 128-byte row per nonzero with the 128-byte swizzle (16-byte chunk c of
+// row k stored at chunk c ^ (k & 7), 1 KiB aligned).  Read as an MN-major
+// operand that tile is both A = H^T (M = 64 x K) and B = H (K x N = 64), so
+// each tcgen05.mma (M=64, N=64, K=16, kind::f16, BF16 in, FP32 out)
+// accumulates 16 nonzeros of h h^T.  One thread issues the MMAs and commits
+// them to an mbarrier; the CTA waits with a bounded spin, then each warp
+// reads its quarter of the accumulator (for M = 64, rows 16w..16w+15 live in
+// TMEM lanes 32w..32w+15) with tcgen05.ld.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ptx.cuh"
+
+namespace ctc {
+namespace tc {
+
+constexpr int kR = 64;        // rank handled here
+constexpr int kChunk = 128;   // nonzeros staged per round (one per thread)
+constexpr int kThreads = 128;
+constexpr int kSmemBytes = kChunk * 128 + 1024;  // operand tile + alignment slack
+
+using px::smem_u32;
+using px::mbar_try_wait;
+using px::mbar_wait_bounded;
+
+// UMMA shared-memory descriptor: MN-major, 128-byte swizzle, SM100 version 1
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr)
+{
+    const uint64_t start = (addr >> 4) & 0x3FFFull;
+    const uint64_t lbo = 1ull;                 // one 64-element block along MN: unused
+    const uint64_t sbo = (1024u >> 4) & 0x3FFFull;  // 8 rows x 128 B between row groups
+    return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// instruction descriptor: D F32, A/B BF16, both MN-major, M = 64, N = 64
+__host__ __device__ constexpr uint32_t idesc_bf16_m64_n64()
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((64u >> 3) << 17) |
+           ((64u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar_addr)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_addr)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld_32x32b_x64(uint32_t taddr, uint32_t (&v)[64])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31]),
+          "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]),
+          "=r"(v[40]), "=r"(v[41]), "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]),
+          "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]), "=r"(v[55]),
+          "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+// Gram + right-hand side of the heavy pieces listed in `pieces` (tile
+// indices of the mode's plan); slot[t] = {G (64 x 64 row-major), b (64)}.
+// err[0] is set when a bounded wait expires.
+__global__ void __launch_bounds__(kThreads, 2)
+    k_als_gram_tc(const int4 *__restrict__ tiles, const uint32_t *__restrict__ pieces, uint32_t npieces,
+                  const uint4 *__restrict__ rec, int m, const __nv_bfloat16 *__restrict__ Ua,
+                  const __nv_bfloat16 *__restrict__ Ub, float *__restrict__ slot, int *err)
+{
+    // the swizzled operand tile: kChunk x 128 B, 1 KiB aligned inside the
+    // dynamic shared memory (launched with kSmemBytes)
+    extern __shared__ uint8_t dsm[];
+    uint8_t *hs = dsm + ((1024u - (smem_u32(dsm) & 1023u)) & 1023u);
+    __shared__ float rhs_part[kThreads / 32][kR];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base_sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+    const uint32_t mbar_addr = smem_u32(&mbar);
+    const uint32_t hs_addr = smem_u32(hs);
+    const uint32_t idesc = idesc_bf16_m64_n64();
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base_sh)),
+                     "r"(64u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_addr));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem_d = tmem_base_sh;
+    uint32_t phase = 0;
+    bool ok = true;
+
+    for (uint32_t pi = blockIdx.x; pi < npieces && ok; pi += gridDim.x) {
+        const uint32_t tile = pieces[pi];
+        const int4 td = tiles[tile];
+        const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
+        float rhs[kR];
+#pragma unroll
+        for (int f = 0; f < kR; ++f) rhs[f] = 0.f;
+        for (uint32_t c0 = start; c0 < end && ok; c0 += kChunk) {
+            const uint32_t p = c0 + tid;
+            uint8_t *row = hs + tid * 128;
+            if (p < end) {
+                const uint4 r = rec[p];
+                const float x = __uint_as_float(r.w);
+                const uint32_t q1 = m1 == 0 ? r.x : (m1 == 1 ? r.y : r.z);
+                const uint32_t q2 = m2 == 0 ? r.x : (m2 == 1 ? r.y : r.z);
+                const uint4 *ba = reinterpret_cast<const uint4 *>(Ua + (size_t)q1 * kR);
+                const uint4 *bb = reinterpret_cast<const uint4 *>(Ub + (size_t)q2 * kR);
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const uint4 va = ba[c], vb = bb[c];
+                    const __nv_bfloat162 *pa = reinterpret_cast<const __nv_bfloat162 *>(&va);
+                    const __nv_bfloat162 *pb = reinterpret_cast<const __nv_bfloat162 *>(&vb);
+                    uint32_t outw[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 fa = __bfloat1622float2(pa[q]);
+                        const float2 fb = __bfloat1622float2(pb[q]);
+                        const float h0 = fa.x * fb.x, h1 = fa.y * fb.y;
+                        rhs[8 * c + 2 * q] += x * h0;
+                        rhs[8 * c + 2 * q + 1] += x * h1;
+                        outw[q] = pack_bf16(h0, h1);
+                    }
+                    *reinterpret_cast<uint4 *>(row + ((c ^ (tid & 7)) << 4)) =
+                        make_uint4(outw[0], outw[1], outw[2], outw[3]);
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4 *>(row + (c << 4)) = make_uint4(0, 0, 0, 0);
+            }
+            // make the generic-proxy stores visible to the tensor core
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t nk = min((uint32_t)kChunk, end - c0);
+                const uint32_t nmma = (nk + 15) / 16;
+                for (uint32_t kk = 0; kk < nmma; ++kk) {
+                    const uint64_t d = smem_desc_sw128(hs_addr + kk * 16 * 128);
+                    mma_bf16(tmem_d, d, d, idesc, (c0 != start || kk != 0) ? 1u : 0u);
+                }
+                mma_commit(mbar_addr);
+            }
+            // every thread waits; the outcome is made CTA-uniform so no
+            // thread can leave the loop while others sit at a barrier
+            const int got = mbar_wait_bounded(mbar_addr, phase) ? 1 : 0;
+            ok = __syncthreads_and(got) != 0;
+            if (!ok) break;
+            phase ^= 1;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        }
+        if (!ok) break;
+        // right-hand side: warp butterflies, then a fixed-order sum over warps
+#pragma unroll
+        for (int f = 0; f < kR; ++f) {
+            float v = rhs[f];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) rhs_part[warp][f] = v;
+        }
+        // Gram rows 16w..16w+15 from this warp's TMEM lanes
+        uint32_t g[64];
+        tmem_ld_32x32b_x64(tmem_d + ((uint32_t)(32 * warp) << 16), g);
+        float *dst = slot + (size_t)tile * (kR * kR + kR);
+        if (lane < 16) {
+            const int grow = 16 * warp + lane;
+            float4 *d4 = reinterpret_cast<float4 *>(dst + grow * kR);
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                d4[q] = make_float4(__uint_as_float(g[4 * q]), __uint_as_float(g[4 * q + 1]),
+                                    __uint_as_float(g[4 * q + 2]), __uint_as_float(g[4 * q + 3]));
+        }
+        __syncthreads();
+        if (tid < kR) dst[kR * kR + tid] = ((rhs_part[0][tid] + rhs_part[1][tid]) + rhs_part[2][tid]) + rhs_part[3][tid];
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    if (!ok) {
+        // report, and give the MMAs in flight one more bounded wait before
+        // the tensor memory they write is released
+        if (tid == 0) atomicExch(err, 1);
+        mbar_wait_bounded(mbar_addr, phase);
+    }
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(64u));
+}
+
+// FP32 factor rows -> BF16 copies (row-major, same shape)
+__global__ void k_to_bf16(const float *__restrict__ src, __nv_bfloat16 *__restrict__ dst, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = __float2bfloat16_rn(src[i]);
+}
+
+}  // namespace tc
+}  // namespace ctc

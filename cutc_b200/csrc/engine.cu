@@ -4,6 +4,7 @@
 // evaluation, early stop, and the C ABI entry points that need the GPU.
 #include "ctc_internal.h"
 #include "kernels.cuh"
+#include "als_tc.cuh"
 
 #include <cuda_runtime.h>
 
@@ -23,8 +24,12 @@ namespace ctc {
 
 static void check_cuda(cudaError_t e, const char *what)
 {
-    if (e != cudaSuccess) fail(e == cudaErrorMemoryAllocation ? CTC_E_NOMEM : CTC_E_CUDA,
-                               "%s: %s", what, cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        // clear a non-sticky error so that it is not reported again by the
+        // next launch check of an unrelated call
+        (void)cudaGetLastError();
+        fail(e == cudaErrorMemoryAllocation ? CTC_E_NOMEM : CTC_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    }
 }
 #define CK(x) check_cuda((x), #x)
 
@@ -182,6 +187,8 @@ struct DevTensor {
     DevBuf<int4> tiles;
     uint32_t ntiles = 0;
     DevBuf<uint4> heavy;
+    DevBuf<uint32_t> pieces;  // tile indices of the heavy pieces
+    uint32_t npieces = 0;
     uint32_t nheavy = 0;
     DevBuf<T> w;
     bool has_w = false;
@@ -189,6 +196,9 @@ struct DevTensor {
     DevBuf<uint64_t> keys;
     DevBuf<T> res, x;
     k::KeyShape ks{};
+    uint32_t nslots = 0;  // CCD++: ntiles * slot length (lane-interleaved tiles)
+    DevBuf<int4> tasks;   // CCD++ warp tasks (light tiles, groups of pieces)
+    uint32_t ntasks = 0;
 };
 
 static int bits_for(uint64_t d)
@@ -201,9 +211,14 @@ static int bits_for(uint64_t d)
 // CCD++ copy of mode m: 64-bit keys row | q1 | q2 (row = index in mode m,
 // q1/q2 = indices in modes m+1, m+2, each in just enough bits) and the
 // values; the residual is formed on the device.
+// CCD++ copy of mode m: packed keys (row | q1 | q2) and values in the
+// tile slots of `plan` (slot length S = 32 * E): entry p of tile t sits at
+// t*S + (p % E)*32 + p / E, so that lane p / E of the warp owning the tile
+// holds its E consecutive entries and every warp load is coalesced.
+// Unused slot entries hold kPadKey, value 0 and residual 0.
 template <typename T>
 static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t *dims, bool trunc,
-                       DevTensor<T> &d)
+                       const TilePlan &plan, int E, DevTensor<T> &d)
 {
     const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
     const int b0 = bits_for(dims[m]), b1 = bits_for(dims[m1]), b2 = bits_for(dims[m2]);
@@ -212,21 +227,55 @@ static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t 
     d.ks.s_q1 = (uint32_t)b2;
     d.ks.m_q1 = (b1 == 64) ? ~0ull : ((1ull << b1) - 1);
     d.ks.m_q2 = (b2 == 64) ? ~0ull : ((1ull << b2) - 1);
-    const uint64_t n = t->nnz;
-    std::vector<uint64_t> keys(n);
-    std::vector<T> x(n);
+    const uint64_t S = 32ull * (uint64_t)E;
+    const uint64_t ntiles = plan.ntiles();
+    const uint64_t nslots = ntiles * S;
+    if (nslots >= 0xfffffff0ull) fail(CTC_E_UNSUP, "CCD++: more than 2^32 slot entries");
+    std::vector<uint64_t> keys(nslots, k::kPadKey);
+    std::vector<T> x(nslots, T(0));
     const uint32_t s_row = d.ks.s_row, s_q1 = d.ks.s_q1;
-    par_for(n, [&](uint64_t b, uint64_t e) {
-        for (uint64_t i = b; i < e; ++i) {
-            keys[i] = ((t->ind[m][i] - 1) << s_row) | ((t->ind[m1][i] - 1) << s_q1) | (t->ind[m2][i] - 1);
-            const double v = trunc ? ctc_value_through_idx(t->vals[i]) : t->vals[i];
-            x[i] = (T)v;
+    par_for(ntiles, [&](uint64_t tb, uint64_t te) {
+        for (uint64_t tt = tb; tt < te; ++tt) {
+            const uint64_t start = (uint64_t)plan.tiles[4 * tt], len = (uint64_t)plan.tiles[4 * tt + 1];
+            for (uint64_t q = 0; q < len; ++q) {
+                const uint64_t i = start + q, dst = tt * S + (q % E) * 32 + q / E;
+                keys[dst] = ((t->ind[m][i] - 1) << s_row) | ((t->ind[m1][i] - 1) << s_q1) | (t->ind[m2][i] - 1);
+                const double v = trunc ? ctc_value_through_idx(t->vals[i]) : t->vals[i];
+                x[dst] = (T)v;
+            }
         }
     });
-    d.n = (uint32_t)n;
-    d.keys.upload(keys.data(), n, ctx->stream);
-    d.x.upload(x.data(), n, ctx->stream);
-    d.res.alloc(n);
+    // warp tasks: a light tile, or up to kCcdppGroup consecutive pieces of a
+    // long row; the long-row table becomes {row, first group, groups, 0}
+    std::vector<int32_t> tasks;
+    std::vector<uint32_t> hv;
+    tasks.reserve((size_t)ntiles * 4);
+    uint32_t gslot = 0;
+    for (uint32_t tt = 0; tt < (uint32_t)ntiles;) {
+        const int32_t h = plan.tiles[4 * tt + 2];
+        if (h < 0) {
+            tasks.insert(tasks.end(), {(int32_t)tt, plan.tiles[4 * tt + 1], -1, 0});
+            ++tt;
+            continue;
+        }
+        const uint32_t np = plan.heavy_rows[4 * h + 2];
+        const uint32_t ng = (np + k::kCcdppGroup - 1) / k::kCcdppGroup;
+        hv.insert(hv.end(), {plan.heavy_rows[4 * h], gslot, ng, 0u});
+        for (uint32_t g = 0; g < ng; ++g)
+            tasks.insert(tasks.end(), {(int32_t)(tt + g * k::kCcdppGroup),
+                                       (int32_t)std::min<uint32_t>(k::kCcdppGroup, np - g * k::kCcdppGroup), h,
+                                       (int32_t)gslot++});
+        tt += np;
+    }
+    d.ntasks = (uint32_t)(tasks.size() / 4);
+    d.tasks.upload(reinterpret_cast<const int4 *>(tasks.data()), d.ntasks, ctx->stream);
+    d.heavy.upload(reinterpret_cast<const uint4 *>(hv.data()), hv.size() / 4, ctx->stream);
+    d.n = (uint32_t)t->nnz;
+    d.nslots = (uint32_t)nslots;
+    d.keys.upload(keys.data(), nslots, ctx->stream);
+    d.x.upload(x.data(), nslots, ctx->stream);
+    d.res.alloc(nslots);
+    CK(cudaMemsetAsync(d.res.p, 0, nslots * sizeof(T), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
 }
 
@@ -284,7 +333,7 @@ static void stage_tensor(ctc_ctx *ctx, const ctc_tensor *t, bool trunc, DevTenso
 }
 
 template <typename T>
-static void stage_plan(ctc_ctx *ctx, const ctc_tensor *t, int mode, uint32_t tile_len, DevTensor<T> &d)
+static TilePlan stage_plan(ctc_ctx *ctx, const ctc_tensor *t, int mode, uint32_t tile_len, DevTensor<T> &d)
 {
     const uint64_t n = t->nnz;
     std::vector<uint32_t> rows(n);
@@ -294,13 +343,20 @@ static void stage_plan(ctc_ctx *ctx, const ctc_tensor *t, int mode, uint32_t til
     for (uint64_t i = 1; i < n; ++i)
         if (rows[i] < rows[i - 1])
             fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", mode + 1, mode + 1);
+    if (n >= 0x7fffffffull) fail(CTC_E_UNSUP, "tile plans index at most 2^31 - 1 nonzeros");
     TilePlan p = plan_tiles(rows.data(), n, tile_len);
     d.mode = mode;
     d.ntiles = p.ntiles();
     d.nheavy = p.nheavy();
     d.tiles.upload(reinterpret_cast<const int4 *>(p.tiles.data()), p.ntiles(), ctx->stream);
     d.heavy.upload(reinterpret_cast<const uint4 *>(p.heavy_rows.data()), p.nheavy(), ctx->stream);
+    std::vector<uint32_t> pieces;
+    for (uint32_t t = 0; t < p.ntiles(); ++t)
+        if (p.tiles[4 * t + 2] >= 0) pieces.push_back(t);
+    d.npieces = (uint32_t)pieces.size();
+    d.pieces.upload(pieces.data(), pieces.size(), ctx->stream);
     CK(cudaStreamSynchronize(ctx->stream));
+    return p;
 }
 
 template <typename T>
@@ -378,6 +434,7 @@ static void build_dataset(ctc_dataset *ds, const ctc_tensor *const train[3], con
     const ctc_params &p = ds->p;
     const bool trunc = p.compat != 0;
     uint32_t tl = (uint32_t)(p.tile_len > 0 ? p.tile_len : default_tile(p.alg));
+    // CCD++: tiles fill slots of 32*E entries
     if (p.alg == CTC_ALG_CCDPP) tl = 32u * (uint32_t)ccdpp_lanes((int)tl);
     std::unique_ptr<ctc_tensor> own[3];
     const ctc_tensor *srt[3] = {train[0], train[1], train[2]};
@@ -390,9 +447,13 @@ static void build_dataset(ctc_dataset *ds, const ctc_tensor *const train[3], con
         }
         if (srt[m]->nnz != train[0]->nnz) fail(CTC_E_ARG, "training copies differ in size");
         validate_tensor(srt[m], ds->dims, "training tensor");
-        if (p.alg == CTC_ALG_CCDPP) stage_keys<T>(ctx, srt[m], m, ds->dims, trunc, impl->copy[m]);
-        else stage_tensor<T>(ctx, srt[m], trunc, impl->copy[m]);
-        if (p.alg != CTC_ALG_SGD) stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
+        if (p.alg == CTC_ALG_CCDPP) {
+            const TilePlan plan = stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
+            stage_keys<T>(ctx, srt[m], m, ds->dims, trunc, plan, (int)(tl / 32), impl->copy[m]);
+        } else {
+            stage_tensor<T>(ctx, srt[m], trunc, impl->copy[m]);
+            if (p.alg != CTC_ALG_SGD) stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
+        }
         if (trunc && (p.alg == CTC_ALG_ALS || p.alg == CTC_ALG_CCD))
             stage_weights<T>(ctx, srt[m], m, p.alg == CTC_ALG_CCD ? 1 : 0, impl->copy[m]);
     }
@@ -429,6 +490,11 @@ struct Session : SessionBase {
     DevBuf<T> U[3], Ubest[3], Urow[3], slot, slot2, lr_dev;
     DevBuf<k::Pack3<T>> pk[3];  // CCD++ per-column {cur, prev, old}
     DevBuf<unsigned int> hcnt[3];  // CCD++ pieces arrived per heavy row (reset by the finaliser)
+    // mixed-precision ALS at rank 64: BF16 copies of the factors feed the
+    // tensor-core Gram of long-row pieces; err flags an expired bounded wait
+    bool tc = false;
+    DevBuf<__nv_bfloat16> Ubf[3];
+    DevBuf<int> dev_err;
     DevBuf<unsigned long long> nonspd_dev;
     cudaGraphExec_t graph = nullptr;
     bool model_set = false;
@@ -441,9 +507,14 @@ struct Session : SessionBase {
         tile_len = (uint32_t)(p.tile_len > 0 ? p.tile_len : default_tile(p.alg));
         nonspd_dev.alloc(1);
         lr_dev.alloc(1);
+        dev_err.alloc(1);
+        CK(cudaMemsetAsync(dev_err.p, 0, sizeof(int), ctx->stream));
         for (int m = 0; m < 3; ++m) {
             const size_t sz = (size_t)dims[m] * R;
-            U[m].alloc(sz);
+            // (+4: the CCD++ column staging copies whole 16-byte words and
+            // may read up to 15 bytes past the last column)
+            U[m].alloc(sz + 4);
+            CK(cudaMemsetAsync(U[m].p, 0, (sz + 4) * sizeof(T), ctx->stream));
             Ubest[m].alloc(sz);
             if (colmajor) {
                 Urow[m].alloc(sz);
@@ -463,6 +534,16 @@ struct Session : SessionBase {
         }
         slot.alloc(need);
         if (p.alg == CTC_ALG_CCDPP) slot2.alloc(need);
+        if (p.alg == CTC_ALG_CCDPP) {
+            set_ccdpp_smem<4>();
+            set_ccdpp_smem<8>();
+            set_ccdpp_smem<16>();
+        }
+        tc = p.alg == CTC_ALG_ALS && p.precision == CTC_PREC_MIXED && R == 64 && std::is_same<T, float>::value;
+        if (tc) {
+            for (int m = 0; m < 3; ++m) Ubf[m].alloc((size_t)dims[m] * R);
+            CK(cudaFuncSetAttribute(tc::k_als_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
+        }
         if (p.alg == CTC_ALG_ALS) {
             using Sh = k::AlsShape<R>;
             const int smem = (int)(4 * Sh::smem_doubles * sizeof(double));
@@ -479,6 +560,34 @@ struct Session : SessionBase {
 
     // run-time parameters (lambda, inner, lr, schedule, order ...); the
     // staged layout (alg, precision, compat, tile length) stays
+    template <int E>
+    void set_ccdpp_smem()
+    {
+        // the largest budget ctc_params.smem_budget may ask for
+        const int smem = ccdpp_smem_max();
+        CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, true, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, false, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    }
+
+    // shared memory per block of a CCD++ pass for staged factor columns: two
+    // 512-thread blocks per SM share the 228 KiB
+    size_t ccdpp_budget() const
+    {
+        if (p.smem_budget < 0) return 0;
+        const size_t b = p.smem_budget > 0 ? (size_t)p.smem_budget : (size_t)110 * 1024;
+        return std::min<size_t>(b, (size_t)ccdpp_smem_max());
+    }
+
+    // opt-in dynamic shared memory of a block, less room for the pass's
+    // static mbarrier (and a margin)
+    static int ccdpp_smem_max()
+    {
+        int dev = 0, optin = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        return optin - 1024;
+    }
+
     void set_params(const ctc_params &np) override
     {
         p = np;
@@ -539,6 +648,8 @@ struct Session : SessionBase {
         CK(cudaMemsetAsync(nonspd_dev.p, 0, sizeof(unsigned long long), ctx->stream));
         set_lr(p.lr * (p.lr_scale > 0 ? p.lr_scale : 1.0));
         if (colmajor) ccdpp_init();
+        if (tc)
+            for (int m = 0; m < 3; ++m) refresh_bf16(m);
         CK(cudaStreamSynchronize(ctx->stream));
         model_set = true;
     }
@@ -610,11 +721,43 @@ struct Session : SessionBase {
             LAUNCH(ctx, k::k_als_tile<T, R>, grid_for(c.ntiles, 4, kSMs * 16), 128, smem, (const int4 *)c.tiles.p,
                    c.ntiles, (const uint4 *)c.rec.p, (const double *)c.v64.p,
                    (const T *)(c.has_w ? c.w.p : nullptr), m, U[m].p, (const T *)U[m1].p, (const T *)U[m2].p,
-                   (T)p.lambda, slot.p, nonspd_dev.p);
+                   (T)p.lambda, slot.p, nonspd_dev.p, tc ? 1 : 0);
+            if (tc && c.npieces) als_gram_tc(c, m);
             if (c.nheavy)
                 LAUNCH(ctx, k::k_als_fix<T, R>, grid_for(c.nheavy, 4, kSMs * 16), 128, smem,
                        (const uint4 *)c.heavy.p, c.nheavy, (const T *)slot.p, U[m].p, (T)p.lambda, nonspd_dev.p);
+            if (tc) refresh_bf16(m);
         }
+    }
+
+    void refresh_bf16(int m)
+    {
+        if constexpr (std::is_same<T, float>::value)
+            LAUNCH(ctx, tc::k_to_bf16, grid_for((uint64_t)dims[m] * R, 256, kSMs * 8), 256, 0, (const float *)U[m].p,
+                   Ubf[m].p, (uint64_t)dims[m] * R);
+    }
+
+    void als_gram_tc(DevTensor<T> &c, int m)
+    {
+        if constexpr (std::is_same<T, float>::value) {
+            const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+            const unsigned g = std::min<unsigned>(c.npieces, 2 * kSMs);
+            LAUNCH(ctx, tc::k_als_gram_tc, g, tc::kThreads, tc::kSmemBytes, (const int4 *)c.tiles.p,
+                   (const uint32_t *)c.pieces.p, c.npieces, (const uint4 *)c.rec.p, m,
+                   (const __nv_bfloat16 *)Ubf[m1].p, (const __nv_bfloat16 *)Ubf[m2].p, (float *)slot.p, dev_err.p);
+        }
+    }
+
+    // device-side error flag: 1 = the tensor-core Gram's bounded wait for
+    // its MMAs expired, 2 = a CCD++ pass's bounded wait for its staged
+    // columns expired (the pass left the column unfinished)
+    void check_errors()
+    {
+        int e = 0;
+        CK(cudaMemcpyAsync(&e, dev_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (e == 1) fail(CTC_E_TIMEOUT, "tensor-core Gram: a bounded wait for the MMAs expired");
+        if (e) fail(CTC_E_TIMEOUT, "CCD++ pass: a bounded wait for the staged factor columns expired");
     }
 
     void ccd_epoch()
@@ -633,11 +776,36 @@ struct Session : SessionBase {
         }
     }
 
+    // 16-byte vectors per lane of the SGD kernel (1, 2 or 4): the lanes per
+    // nonzero are R / (vector width * C), ctc_params.threads_per_row.  The
+    // default is one vector per lane (R/4 lanes per FP32 nonzero), the
+    // fastest setting measured at R = 32 on the 100M-nonzero Zipf tensor
+    // (35 ms per epoch against 63 ms with two vectors and 79 ms with four).
+    int sgd_vectors() const
+    {
+        constexpr int base = R / k::Vec<T>::n;
+        if (p.sgd_order == CTC_SGD_SEQUENTIAL) return 1;
+        int c = p.threads_per_row > 0 ? base / p.threads_per_row : 1;
+        if (c >= 4 && base % 4 == 0) return 4;
+        if (c >= 2 && base % 2 == 0) return 2;
+        return 1;
+    }
+    int sgd_groups_per_block() const { return 8 * (32 / (R / k::Vec<T>::n / sgd_vectors())); }
+
     void sgd_epoch()
     {
+        switch (sgd_vectors()) {
+        case 4: sgd_launch<4>(); break;
+        case 2: sgd_launch<2>(); break;
+        default: sgd_launch<1>(); break;
+        }
+    }
+
+    template <int C>
+    void sgd_launch()
+    {
         DevTensor<T> &c = D->copy[0];
-        constexpr int G = R / k::Vec<T>::n;
-        const int gpb = 8 * (32 / G);  // groups per 256-thread block
+        const int gpb = sgd_groups_per_block();
         const bool seq = p.sgd_order == CTC_SGD_SEQUENTIAL;
         const unsigned g = seq ? 1 : sgd_grid(gpb);
         const float *d0 = damp_on ? damp[0].p : nullptr;
@@ -652,9 +820,10 @@ struct Session : SessionBase {
                     break;
                 }
         }
-        LAUNCH(ctx, k::k_sgd<T, R>, g, seq ? 32 : 256, 0, (const uint4 *)c.rec.p, (const double *)c.v64.p, c.n,
-               tile_len, c.ntiles, U[0].p, U[1].p, U[2].p, (const T *)lr_dev.p, (T)p.lambda, p.sgd_atomic,
-               seq ? 1 : 0, stride, d0, d1, d2);
+        if constexpr ((R / k::Vec<T>::n) % C == 0)
+            LAUNCH(ctx, k::k_sgd<T, R, C>, g, seq ? 32 : 256, 0, (const uint4 *)c.rec.p, (const double *)c.v64.p,
+                   c.n, tile_len, c.ntiles, U[0].p, U[1].p, U[2].p, (const T *)lr_dev.p, (T)p.lambda, p.sgd_atomic,
+                   seq ? 1 : 0, stride, d0, d1, d2);
     }
 
     void ccdpp_init()
@@ -664,8 +833,9 @@ struct Session : SessionBase {
                    (const T *)U[m].p, Urow[m].p, dims[m], R);
         for (int m = 0; m < 3; ++m) {
             DevTensor<T> &c = D->copy[m];
-            LAUNCH(ctx, k::k_ccdpp_init<T, R>, grid_for(c.n, 256, kSMs * 16), 256, 0, (const uint64_t *)c.keys.p,
-                   (const T *)c.x.p, c.res.p, c.n, c.ks, m, (const T *)Urow[0].p, (const T *)Urow[1].p,
+            LAUNCH(ctx, k::k_ccdpp_init<T, R>, grid_for(c.nslots, 256, kSMs * 16), 256, 0,
+                   (const uint64_t *)c.keys.p, (const T *)c.x.p, c.res.p, c.nslots, c.ks, m, (const T *)Urow[0].p,
+                   (const T *)Urow[1].p,
                    (const T *)Urow[2].p);
         }
     }
@@ -674,19 +844,36 @@ struct Session : SessionBase {
     void ccdpp_pass(int m, int f, bool first)
     {
         DevTensor<T> &c = D->copy[m];
-        const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
         T *out = U[m].p + (size_t)f * dims[m];
-        const unsigned g = grid_for(c.ntiles, 8, kSMs * 8);
+        k::CcdppCols<T> cols{};
+        size_t need[2];
+        for (int q = 0; q < 2; ++q) {
+            const int n = (m + 1 + q) % 3;
+            cols.col[q] = U[n].p + (size_t)f * dims[n];
+            cols.pk[q] = pk[n].p;
+            cols.dim[q] = dims[n];
+            // bytes one copy takes (the column copy may start up to 15
+            // bytes early to reach a 16-byte boundary)
+            need[q] = first ? (size_t)dims[n] * sizeof(k::Pack3<T>) : (((size_t)dims[n] * sizeof(T) + 15 + 15) & ~15ull);
+        }
+        // stage both when they fit, else the one that fits
+        const size_t budget = ccdpp_budget();
+        if (need[0] + need[1] <= budget) {
+            cols.stage[0] = cols.stage[1] = 1;
+        } else if (need[0] <= budget || need[1] <= budget) {
+            const int q = (need[0] <= budget && (need[1] > budget || need[0] >= need[1])) ? 0 : 1;
+            cols.stage[q] = 1;
+        }
+        const size_t smem = (cols.stage[0] ? need[0] : 0) + (cols.stage[1] ? need[1] : 0);
+        const unsigned g = grid_for((uint64_t)c.ntasks, 16, kSMs * 2);
         if (first)
-            LAUNCH(ctx, k::k_ccdpp_pass<T, true, E>, g, 256, 0, (const int4 *)c.tiles.p, c.ntiles,
-                   (const uint64_t *)c.keys.p, c.res.p, c.ks, pk[m].p, (const k::Pack3<T> *)pk[m1].p,
-                   (const k::Pack3<T> *)pk[m2].p, out, (T)p.lambda, slot.p, slot2.p, (const uint4 *)c.heavy.p,
-                   hcnt[m].p);
+            LAUNCH(ctx, k::k_ccdpp_pass<T, true, E>, g, 512, smem, (const int4 *)c.tasks.p, c.ntasks,
+                   (const uint64_t *)c.keys.p, c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p,
+                   (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p);
         else
-            LAUNCH(ctx, k::k_ccdpp_pass<T, false, E>, g, 256, 0, (const int4 *)c.tiles.p, c.ntiles,
-                   (const uint64_t *)c.keys.p, c.res.p, c.ks, pk[m].p, (const k::Pack3<T> *)pk[m1].p,
-                   (const k::Pack3<T> *)pk[m2].p, out, (T)p.lambda, slot.p, slot2.p, (const uint4 *)c.heavy.p,
-                   hcnt[m].p);
+            LAUNCH(ctx, k::k_ccdpp_pass<T, false, E>, g, 512, smem, (const int4 *)c.tasks.p, c.ntasks,
+                   (const uint64_t *)c.keys.p, c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p,
+                   (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p);
     }
 
     // One CCD++ outer iteration: per column f, the {cur, prev, old} packs,
@@ -720,8 +907,8 @@ struct Session : SessionBase {
         }
         for (int m = 0; m < 3; ++m) {
             DevTensor<T> &c = D->copy[m];
-            const unsigned g = grid_for(c.n, 256, kMaxPartials);
-            LAUNCH(ctx, k::k_ccdpp_finish<T>, g, 256, 0, (const uint64_t *)c.keys.p, c.res.p, c.n, c.ks, m,
+            const unsigned g = grid_for(c.nslots, 256, kMaxPartials);
+            LAUNCH(ctx, k::k_ccdpp_finish<T>, g, 256, 0, (const uint64_t *)c.keys.p, c.res.p, c.nslots, c.ks, m,
                    (const T *)(U[0].p + (size_t)(R - 1) * dims[0]), (const T *)(U[1].p + (size_t)(R - 1) * dims[1]),
                    (const T *)(U[2].p + (size_t)(R - 1) * dims[2]), m == 0 ? ctx->partial.p : (double *)nullptr);
             if (m == 0)
@@ -742,7 +929,7 @@ struct Session : SessionBase {
     void epochs(int n) override
     {
         if (!model_set) fail(CTC_E_ARG, "no model staged on the dataset");
-        if (p.alg == CTC_ALG_SGD && !damp_ready) prepare_damping(8 * (32 / (R / k::Vec<T>::n)));
+        if (p.alg == CTC_ALG_SGD && !damp_ready) prepare_damping(sgd_groups_per_block());
         const bool use_graph = p.use_graph && !ctx->kt.on && p.sgd_order != CTC_SGD_SEQUENTIAL;
         for (int i = 0; i < n; ++i) {
             if (!use_graph) {
@@ -774,6 +961,7 @@ struct Session : SessionBase {
     // scalars: 0 train SSE, 2 val SSE, 3 test SSE, 4..6 sum of squares of U
     void evaluate(ctc_epoch_stats *st) override
     {
+        check_errors();
         const T *Urm[3];
         for (int m = 0; m < 3; ++m) {
             if (colmajor) {
@@ -786,7 +974,7 @@ struct Session : SessionBase {
         }
         if (colmajor) {
             // copy 0 holds r = x - model: its SSE is the sum of squares
-            sumsq_into(D->copy[0].res.p, D->copy[0].n, 0);
+            sumsq_into(D->copy[0].res.p, D->copy[0].nslots, 0);
         } else {
             sse_into(D->copy[0], Urm, 0);
         }
@@ -897,8 +1085,10 @@ static void check_params(const ctc_params *p)
 {
     if (!p) fail(CTC_E_ARG, "null params");
     if (p->alg < CTC_ALG_ALS || p->alg > CTC_ALG_CCDPP) fail(CTC_E_ARG, "unknown algorithm %d", p->alg);
-    if (p->precision != CTC_PREC_F32 && p->precision != CTC_PREC_F64)
-        fail(CTC_E_UNSUP, "precision %d not available in this build", p->precision);
+    if (p->precision != CTC_PREC_F32 && p->precision != CTC_PREC_F64 && p->precision != CTC_PREC_MIXED)
+        fail(CTC_E_ARG, "unknown precision %d", p->precision);
+    if (p->precision == CTC_PREC_MIXED && !(p->alg == CTC_ALG_ALS && p->rank == 64))
+        fail(CTC_E_UNSUP, "mixed precision (BF16 tensor-core Gram) is available for ALS at rank 64");
     if (p->rank != 8 && p->rank != 16 && p->rank != 32 && p->rank != 64)
         fail(CTC_E_UNSUP, "rank %d not supported (8, 16, 32, 64)", p->rank);
     if (p->tile_len < 0 || p->tile_len > (1 << 20)) fail(CTC_E_ARG, "tile_len %d", p->tile_len);

@@ -17,6 +17,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
+#include "ptx.cuh"
+
 namespace ctc {
 namespace k {
 
@@ -153,18 +157,22 @@ __global__ void __launch_bounds__(256) k_sum_partials(const double *__restrict__
 }
 
 // ---------------------------------------------------------------------
-// SGD (sgpu/sgd.cu:21-143 rule).  A group of G = R/VN lanes handles one
-// tile of consecutive mode-0-sorted nonzeros in order; each lane holds a
-// 16-byte slice of the three rows.
+// SGD (sgpu/sgd.cu:21-143 rule).  A group of G = R/(VN*C) lanes handles one
+// tile of consecutive mode-0-sorted nonzeros; each lane holds C 16-byte
+// slices of the three rows (C is the "threads per row" knob: fewer lanes
+// per nonzero put more nonzeros in flight per warp).
 //   e = x - sum a.b.c ;  a += s*((e*b*c) - lambda*a) ; b, c likewise from
-//   the pre-update rows, s = lr * step scale.
+//   the pre-update rows, s = lr * step scale (times a per-row factor when
+//   damping is on, see ctc_params.sgd_conflicts).
 // sequential != 0: one group walks all tiles in order (deterministic); the
 //   mode-0 row stays in registers while it does not change (exact there).
-// Hogwild: groups run tiles concurrently; each nonzero reads its three rows
-//   fresh and adds its deltas atomically (vector red.add), or stores the new
-//   rows (atomic == 0, lossy under contention).
+// Hogwild: groups run tiles concurrently, in a scattered tile order; each
+//   nonzero reads its three rows fresh and adds its deltas atomically
+//   (vector red.add), or stores the new rows (atomic == 0, lossy under
+//   contention).  The next nonzero's record is fetched while the current
+//   one is processed.
 // ---------------------------------------------------------------------
-template <typename T, int R>
+template <typename T, int R, int C>
 __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
                                              const double *__restrict__ v64, uint32_t n,
                                              uint32_t tile_len, uint32_t ntiles, T *U0, T *U1,
@@ -176,8 +184,8 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
 {
     using V = typename Vec<T>::type;
     constexpr int VN = Vec<T>::n;
-    constexpr int G = R / VN;
-    static_assert(G >= 1 && G <= 32 && (32 % G) == 0, "unsupported rank");
+    constexpr int G = R / (VN * C);
+    static_assert(G >= 1 && G <= 32 && (32 % G) == 0 && G * VN * C == R, "unsupported rank / lanes");
     constexpr int GPW = 32 / G;
     const int lane = threadIdx.x & 31;
     const int gl = lane % G;
@@ -198,29 +206,41 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
         const uint64_t start = tile * tile_len;
         const uint64_t end = min(start + tile_len, (uint64_t)n);
         uint32_t cur = kNoKey;
-        V a, a0;
+        V a[C], a0[C];
         V *arow = nullptr;
+        uint4 rn = start < end ? rec[start] : make_uint4(0, 0, 0, 0);
         for (uint64_t p = start; p < end; ++p) {
-            const uint4 r = rec[p];
+            const uint4 r = rn;
+            if (p + 1 < end) rn = rec[p + 1];
             const T x = value_of<T>(r, v64, p);
             if (!sequential) {
-                // Hogwild: every row is read fresh and updated per nonzero, so
-                // the staleness of a hot row is bounded by the updates in flight
-                arow = reinterpret_cast<V *>(U0 + (size_t)r.x * R) + gl;
-                a = *arow;
-                a0 = a;
+                // every row read fresh: the staleness of a hot row is bounded
+                // by the updates in flight
+                arow = reinterpret_cast<V *>(U0 + (size_t)r.x * R) + gl * C;
+#pragma unroll
+                for (int q = 0; q < C; ++q) a0[q] = a[q] = arow[q];
             } else if (r.x != cur) {
-                if (arow) *arow = a;
+                if (arow)
+#pragma unroll
+                    for (int q = 0; q < C; ++q) arow[q] = a[q];
                 cur = r.x;
-                arow = reinterpret_cast<V *>(U0 + (size_t)r.x * R) + gl;
-                a = *arow;
+                arow = reinterpret_cast<V *>(U0 + (size_t)r.x * R) + gl * C;
+#pragma unroll
+                for (int q = 0; q < C; ++q) a[q] = arow[q];
             }
-            V *brow = reinterpret_cast<V *>(U1 + (size_t)r.y * R) + gl;
-            V *crow = reinterpret_cast<V *>(U2 + (size_t)r.z * R) + gl;
-            const V b = *brow, c = *crow;
+            V *brow = reinterpret_cast<V *>(U1 + (size_t)r.y * R) + gl * C;
+            V *crow = reinterpret_cast<V *>(U2 + (size_t)r.z * R) + gl * C;
+            V b[C], c[C];
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                b[q] = brow[q];
+                c[q] = crow[q];
+            }
             T part = 0;
 #pragma unroll
-            for (int v = 0; v < VN; ++v) part += vget(a, v) * vget(b, v) * vget(c, v);
+            for (int q = 0; q < C; ++q)
+#pragma unroll
+                for (int v = 0; v < VN; ++v) part += vget(a[q], v) * vget(b[q], v) * vget(c[q], v);
 #pragma unroll
             for (int o = G / 2; o > 0; o >>= 1) part += __shfl_xor_sync(gmask, part, o);
             const T e = x - part;
@@ -230,35 +250,40 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
                 sb *= (T)damp1[r.y];
                 sc *= (T)damp2[r.z];
             }
-            V an, db, dc;
 #pragma unroll
-            for (int v = 0; v < VN; ++v) {
-                const T av = vget(a, v), bv = vget(b, v), cv = vget(c, v);
-                vset(an, v, av + sa * ((e * bv * cv) - lambda * av));
-                vset(db, v, sb * ((e * av * cv) - lambda * bv));
-                vset(dc, v, sc * ((e * bv * av) - lambda * cv));
-            }
-            if (!sequential && atomic) {
-                V da;
-#pragma unroll
-                for (int v = 0; v < VN; ++v) vset(da, v, vget(an, v) - vget(a0, v));
-                vatomic_add(arow, da);
-                vatomic_add(brow, db);
-                vatomic_add(crow, dc);
-            } else {
-                V bn, cn;
+            for (int q = 0; q < C; ++q) {
+                V an, db, dc;
 #pragma unroll
                 for (int v = 0; v < VN; ++v) {
-                    vset(bn, v, vget(b, v) + vget(db, v));
-                    vset(cn, v, vget(c, v) + vget(dc, v));
+                    const T av = vget(a[q], v), bv = vget(b[q], v), cv = vget(c[q], v);
+                    vset(an, v, av + sa * ((e * bv * cv) - lambda * av));
+                    vset(db, v, sb * ((e * av * cv) - lambda * bv));
+                    vset(dc, v, sc * ((e * bv * av) - lambda * cv));
                 }
-                if (!sequential) *arow = an;
-                *brow = bn;
-                *crow = cn;
+                if (!sequential && atomic) {
+                    V da;
+#pragma unroll
+                    for (int v = 0; v < VN; ++v) vset(da, v, vget(an, v) - vget(a0[q], v));
+                    vatomic_add(arow + q, da);
+                    vatomic_add(brow + q, db);
+                    vatomic_add(crow + q, dc);
+                } else {
+                    V bn, cn;
+#pragma unroll
+                    for (int v = 0; v < VN; ++v) {
+                        vset(bn, v, vget(b[q], v) + vget(db, v));
+                        vset(cn, v, vget(c[q], v) + vget(dc, v));
+                    }
+                    if (!sequential) arow[q] = an;
+                    brow[q] = bn;
+                    crow[q] = cn;
+                }
+                a[q] = an;
             }
-            a = an;
         }
-        if (sequential && arow) *arow = a;
+        if (sequential && arow)
+#pragma unroll
+            for (int q = 0; q < C; ++q) arow[q] = a[q];
     }
 }
 
@@ -266,10 +291,9 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
 // CCD++ (rank-one column updates).  Each mode copy of the training tensor
 // is kept as packed 64-bit keys (row | q1 | q2, the row index of the copy's
 // mode and the indices of the next two modes) plus a separate residual
-// array, 12 bytes per nonzero.  Per column f, pack[n][row] holds
-// {current value of column f, final value of column f-1, value of column f
-// before its sweeps} for every mode n, so one 16-byte (FP32) gather per
-// nonzero and mode serves a pass.
+// array, 12 bytes per nonzero, in lane-interleaved tile slots (below).  Per
+// column f, pack[n][row] holds {current value of column f, final value of
+// column f-1, value of column f before its sweeps} for every mode n.
 //
 // Pass for mode m (k_ccdpp_pass): a warp owns a row-aligned tile; lane l
 // walks E consecutive nonzeros, accumulating r*h and h*h per run of equal
@@ -280,6 +304,9 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
 // FIRST (the first sweep of column f over this copy) also refreshes the
 // stored residual:  r <- r - term(f-1, final) + term(f, before sweeps),
 // which is the rank-one add-back of f fused with the subtraction of f-1.
+// The other two modes' column f (or packs, in FIRST) are gathered from
+// shared memory when they fit the block's budget (copied in once per
+// persistent block by a bulk async copy), else through L1.
 // ---------------------------------------------------------------------
 struct KeyShape {
     uint32_t s_row, s_q1;   // key >> s_row = row ; (key >> s_q1) & m_q1 = q1
@@ -307,52 +334,177 @@ __device__ __forceinline__ void ccdpp_finalize(uint32_t row, T nu, T de, T lambd
     pkm[row].cur = u;
 }
 
-template <typename T, bool FIRST, int E>
-__global__ void __launch_bounds__(256) k_ccdpp_pass(const int4 *__restrict__ tiles, uint32_t ntiles,
-                                                    const uint64_t *__restrict__ keys, T *__restrict__ res,
-                                                    KeyShape ks, Pack3<T> *pkm, const Pack3<T> *__restrict__ pa,
-                                                    const Pack3<T> *__restrict__ pb, T *out, T lambda,
-                                                    T *__restrict__ slot_nu, T *__restrict__ slot_de,
-                                                    const uint4 *__restrict__ heavy, unsigned int *hcnt)
+// Tiles of a CCD++ copy are stored in fixed slots of 32*E entries, lane-
+// interleaved: entry p of the tile (lane p / E, step p % E) sits at
+// slot + (p % E) * 32 + p / E.  Each lane walks its E consecutive entries
+// while every load instruction of the warp reads 32 adjacent elements.
+// Unused entries of a slot carry kPadKey and a zero residual.
+constexpr uint64_t kPadKey = ~0ull;
+// pieces of a long row one warp task covers (one slot partial per group)
+constexpr int kCcdppGroup = 8;
+
+template <typename T, int E>
+__device__ __forceinline__ void ccdpp_load_slot(const uint64_t *__restrict__ keys, const T *__restrict__ res,
+                                                uint64_t base, int lane, uint64_t (&kv)[E], T (&rv)[E])
 {
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        kv[e] = __ldcs(keys + base + 32u * e + lane);
+        rv[e] = __ldcs(res + base + 32u * e + lane);
+    }
+}
+
+// FIRST: the refreshed residuals of the lane's valid entries back
+template <typename T, int E>
+__device__ __forceinline__ void ccdpp_store_slot(T *__restrict__ res, uint64_t base, int lane, int cnt,
+                                                 const T (&rv)[E])
+{
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+        if (e < cnt) res[base + 32u * e + lane] = rv[e];
+}
+
+// The two gathered modes of a pass.  Non-FIRST passes read column f of each
+// (one T per row); FIRST passes read the {cur, prev, old} packs.  A mode
+// whose column (or packs) fits the block's shared-memory budget is copied
+// there once per block with a bulk async copy and gathered from shared
+// memory; the other is gathered through L1 from global memory.
+template <typename T>
+struct CcdppCols {
+    const T *col[2];          // column f of modes m+1, m+2 (global)
+    const Pack3<T> *pk[2];    // packs of modes m+1, m+2 (global)
+    uint32_t dim[2];
+    int stage[2];             // 1: staged in shared memory
+};
+
+template <typename T, bool FIRST>
+__device__ __forceinline__ uint32_t ccdpp_stage_span(const CcdppCols<T> &c, int q, const unsigned char *&src,
+                                                     uint32_t &skew)
+{
+    if constexpr (FIRST) {
+        src = reinterpret_cast<const unsigned char *>(c.pk[q]);
+        skew = 0;
+        return c.dim[q] * (uint32_t)sizeof(Pack3<T>);
+    } else {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(c.col[q]);
+        skew = (uint32_t)(a & 15u);
+        src = reinterpret_cast<const unsigned char *>(a - skew);
+        return (skew + c.dim[q] * (uint32_t)sizeof(T) + 15u) & ~15u;
+    }
+}
+
+template <typename T, bool FIRST, int E>
+__global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ tasks, uint32_t ntasks,
+                                                       const uint64_t *__restrict__ keys, T *__restrict__ res,
+                                                       KeyShape ks, Pack3<T> *pkm, CcdppCols<T> cols, T *out,
+                                                       T lambda, T *__restrict__ slot_nu, T *__restrict__ slot_de,
+                                                       const uint4 *__restrict__ heavy, unsigned int *hcnt, int *err)
+{
+    using ColT = typename std::conditional<FIRST, Pack3<T>, T>::type;
     constexpr uint32_t kNone = 0xffffffffu;
+    extern __shared__ __align__(16) unsigned char ccdpp_smem[];
+    __shared__ __align__(8) uint64_t mbar;
     const int lane = threadIdx.x & 31;
+
+    // ---- stage the gathered columns that fit (one bulk copy each) ----
+    const ColT *sc[2] = {nullptr, nullptr};
+    if (cols.stage[0] | cols.stage[1]) {
+        uint32_t off = 0, total = 0;
+        const unsigned char *src[2];
+        uint32_t bytes[2] = {0, 0}, dst[2] = {0, 0};
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (cols.stage[q]) {
+                uint32_t skew;
+                bytes[q] = ccdpp_stage_span<T, FIRST>(cols, q, src[q], skew);
+                dst[q] = off;
+                sc[q] = reinterpret_cast<const ColT *>(ccdpp_smem + off + skew);
+                off += bytes[q];
+                total += bytes[q];
+            }
+        if (threadIdx.x == 0) {
+            px::mbar_init(&mbar, 1);
+            px::mbar_arrive_expect_tx(&mbar, total);
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+                for (uint32_t o = 0; o < bytes[q]; o += 32768u)
+                    px::bulk_g2s(ccdpp_smem + dst[q] + o, src[q] + o, min(32768u, bytes[q] - o), &mbar);
+        }
+        __syncthreads();
+        const int ok = __syncthreads_and(px::mbar_wait_bounded(px::smem_u32(&mbar), 0) ? 1 : 0);
+        if (!ok) {
+            // the copy did not complete in time: report, let any copy still
+            // in flight land (bounded), and leave the column untouched
+            if (threadIdx.x == 0) {
+                atomicExch(err, 2);
+                px::mbar_wait_bounded(px::smem_u32(&mbar), 0);
+            }
+            __syncthreads();
+            return;
+        }
+    }
+    auto gat = [&](int q, uint32_t i) -> ColT {
+        if constexpr (FIRST) return sc[q] ? sc[q][i] : cols.pk[q][i];
+        else return sc[q] ? sc[q][i] : __ldg(cols.col[q] + i);
+    };
+
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t tile = warp; tile < ntiles; tile += nwarps) {
-        const int4 td = tiles[tile];
-        const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
+    // tasks: {tile, len, -1, 0} for a light tile, {first tile, pieces,
+    // heavy row, group} for up to kCcdppGroup consecutive pieces of one long
+    // row; the next task's descriptor is fetched while this one runs
+    int4 td_next = warp < ntasks ? tasks[warp] : make_int4(0, 0, -1, 0);
+    for (uint64_t task = warp; task < ntasks; task += nwarps) {
+        const int4 td = td_next;
+        if (task + nwarps < ntasks) td_next = tasks[task + nwarps];
+        uint64_t kv[E];
+        T rv[E];
         if (td.z >= 0) {
-            // one piece of a long row: warp reduction into the piece's slot;
-            // the piece that arrives last (counter) sums all pieces of the
-            // row in piece order and finalises it -- no waiting anywhere
-            uint32_t row, q1, q2;
-            unpack_key(keys[start], ks, row, q1, q2);
+            // pieces of a long row: per-lane sums over the group's pieces,
+            // one warp reduction into the group's slot; the group that
+            // arrives last (counter) sums all groups of the row in order and
+            // finalises it -- no waiting anywhere
+            const uint4 hr = heavy[td.z];
             Pack3<T> pm{};
-            if constexpr (FIRST) pm = pkm[row];
+            if constexpr (FIRST) pm = pkm[hr.x];
             T nu = 0, de = 0;
-            for (uint32_t p = start + lane; p < end; p += 32) {
-                unpack_key(keys[p], ks, row, q1, q2);
-                const Pack3<T> ga = pa[q1], gb = pb[q2];
-                T r = res[p];
-                if constexpr (FIRST) {
-                    r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
-                    res[p] = r;
+            for (int j = 0; j < td.y; ++j) {
+                const uint64_t base = (uint64_t)(td.x + j) * (uint64_t)(32 * E);
+                ccdpp_load_slot<T, E>(keys, res, base, lane, kv, rv);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    if (kv[e] != kPadKey) {
+                        uint32_t rr, q1, q2;
+                        unpack_key(kv[e], ks, rr, q1, q2);
+                        T r = rv[e];
+                        T h;
+                        if constexpr (FIRST) {
+                            const Pack3<T> ga = gat(0, q1), gb = gat(1, q2);
+                            r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
+                            rv[e] = r;
+                            h = ga.cur * gb.cur;
+                        } else {
+                            h = gat(0, q1) * gat(1, q2);
+                        }
+                        nu += r * h;
+                        de += h * h;
+                    }
                 }
-                const T h = ga.cur * gb.cur;
-                nu += r * h;
-                de += h * h;
+                if constexpr (FIRST) {
+#pragma unroll
+                    for (int e = 0; e < E; ++e)
+                        if (kv[e] != kPadKey) res[base + 32u * e + lane] = rv[e];
+                }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 nu += __shfl_xor_sync(0xffffffffu, nu, o);
                 de += __shfl_xor_sync(0xffffffffu, de, o);
             }
-            const uint4 hr = heavy[td.z];
             unsigned int last = 0;
             if (lane == 0) {
-                slot_nu[tile] = nu;
-                slot_de[tile] = de;
+                slot_nu[td.w] = nu;
+                slot_de[td.w] = de;
                 __threadfence();
                 last = atomicAdd(&hcnt[td.z], 1u) == hr.z - 1 ? 1u : 0u;
             }
@@ -376,8 +528,12 @@ __global__ void __launch_bounds__(256) k_ccdpp_pass(const int4 *__restrict__ til
             }
             continue;
         }
-        const uint32_t base = start + (uint32_t)lane * E;
-        const int cnt = base < end ? (int)min((uint32_t)E, end - base) : 0;
+        const uint64_t base = (uint64_t)td.x * (uint64_t)(32 * E);
+        // valid entries of this lane: the tile's positions lane*E .. +E-1
+        const int cnt = max(0, min(E, td.y - lane * E));
+        ccdpp_load_slot<T, E>(keys, res, base, lane, kv, rv);
+        // light tile: runs of equal rows inside the lane, then one segmented
+        // warp scan joins the runs that cross lanes
         uint32_t hk = kNone, tk = kNone;
         T hn = 0, hd = 0, tn = 0, tdd = 0;
         int nruns = 0;
@@ -386,7 +542,7 @@ __global__ void __launch_bounds__(256) k_ccdpp_pass(const int4 *__restrict__ til
         for (int e = 0; e < E; ++e) {
             if (e < cnt) {
                 uint32_t row, q1, q2;
-                unpack_key(keys[base + e], ks, row, q1, q2);
+                unpack_key(kv[e], ks, row, q1, q2);
                 if (row != tk) {
                     if (nruns == 1) {
                         hk = tk;
@@ -400,18 +556,21 @@ __global__ void __launch_bounds__(256) k_ccdpp_pass(const int4 *__restrict__ til
                     ++nruns;
                     if constexpr (FIRST) pm = pkm[row];
                 }
-                const Pack3<T> ga = pa[q1], gb = pb[q2];
-                T r = res[base + e];
+                T r = rv[e];
+                T h;
                 if constexpr (FIRST) {
+                    const Pack3<T> ga = gat(0, q1), gb = gat(1, q2);
                     r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
-                    res[base + e] = r;
+                    rv[e] = r;
+                    h = ga.cur * gb.cur;
+                } else {
+                    h = gat(0, q1) * gat(1, q2);
                 }
-                const T h = ga.cur * gb.cur;
                 tn += r * h;
                 tdd += h * h;
             }
         }
-        // join runs across lanes: segmented inclusive scan of the last runs
+        if constexpr (FIRST) ccdpp_store_slot<T, E>(res, base, lane, cnt, rv);
         const uint32_t in_key = nruns >= 2 ? hk : tk;
         const uint32_t out_key = tk;
         uint32_t prev_out = __shfl_up_sync(0xffffffffu, out_key, 1);
@@ -503,8 +662,10 @@ __global__ void __launch_bounds__(256) k_ccdpp_init(const uint64_t *__restrict__
     using V = typename Vec<T>::type;
     constexpr int VN = Vec<T>::n;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[p];
+        if (key == kPadKey) continue;  // unused slot entry: residual stays 0
         uint32_t idx[3];
-        key_modes(keys[p], ks, m, idx);
+        key_modes(key, ks, m, idx);
         const V *a = reinterpret_cast<const V *>(U0 + (size_t)idx[0] * R);
         const V *b = reinterpret_cast<const V *>(U1 + (size_t)idx[1] * R);
         const V *c = reinterpret_cast<const V *>(U2 + (size_t)idx[2] * R);
@@ -529,8 +690,10 @@ __global__ void __launch_bounds__(256) k_ccdpp_finish(const uint64_t *__restrict
 {
     double acc = 0;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[p];
+        if (key == kPadKey) continue;
         uint32_t idx[3];
-        key_modes(keys[p], ks, m, idx);
+        key_modes(key, ks, m, idx);
         const T r = res[p] - c0[idx[0]] * c1[idx[1]] * c2[idx[2]];
         res[p] = r;
         acc += (double)r * (double)r;
@@ -822,7 +985,7 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
                                                   const T *__restrict__ Ua,
                                                   const T *__restrict__ Ub, T lambda,
                                                   T *__restrict__ slot,
-                                                  unsigned long long *nonspd)
+                                                  unsigned long long *nonspd, int skip_heavy)
 {
     using Sh = AlsShape<R>;
     constexpr int L = Sh::L, C = Sh::C;
@@ -840,6 +1003,7 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
         const int4 td = tiles[tile];
         const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
         if (td.z >= 0) {
+            if (skip_heavy) continue;  // pieces of long rows go to the tensor-core Gram
             als_accumulate<T, R>(rec, v64, w, m, Ua, Ub, start, end, G, b);
             if (lane < L) {
                 T *dst = slot + tile * (size_t)(R * R + R);

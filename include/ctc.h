@@ -185,6 +185,13 @@ typedef struct {
                               moves by at most ~K single steps per wave of stale
                               updates (0 = 128, < 0 = no scaling).  With one group
                               in flight (sequential order) no row is scaled.       */
+    int threads_per_row;   /* SGD: lanes per nonzero (each holds rank/lanes values of
+                              the three rows); 0 = rank/4 (FP32) or rank/2 (FP64).
+                              The reference uses one thread per nonzero
+                              (sgpu/sgd.cu:32)                                      */
+    int smem_budget;       /* CCD++: shared memory per block (bytes) for the factor
+                              columns a pass gathers; columns that fit are staged
+                              there once per block.  0 = 110 KiB, < 0 = none       */
 } ctc_params;
 
 /* Reference-default parameters for an algorithm (sgpu/base.h:19-64). */

@@ -88,6 +88,29 @@ def test_als_heavy_rows(ctx):
     assert max_factor_rel(G, U) < 1e-9
 
 
+def test_als_mixed_tensor_core(ctx):
+    """Rank 64, mixed precision: pieces of long rows get their Gram from
+    tcgen05 MMAs on BF16 factor copies (FP32 accumulation in tensor memory),
+    every row its FP64 solve.  Final test RMSE within 0.5 % of plain FP32,
+    first-iteration factors within BF16-level error of the FP64 oracle."""
+    P = Problem(60000, (200, 150, 100), 64, seed=30, heavy_row=20000)
+    lam = {"lambda": 0.05}
+    # tile length 256: every mode has rows longer than a tile, so the
+    # tensor-core Gram runs once per mode and iteration
+    _, o32 = engine_run(ctx, P, ctc.ALS, 5, precision=ctc.PREC_F32, tile_len=256, **lam)
+    ctx.set_profiling(True)
+    ctx.reset_kernel_times()
+    Gm, om = engine_run(ctx, P, ctc.ALS, 5, precision=ctc.PREC_MIXED, tile_len=256, **lam)
+    n_tc, ms_tc = ctx.kernel_time("k_als_gram_tc")
+    ctx.set_profiling(False)
+    assert n_tc == 3 * 5, n_tc
+    te32, tem = o32.epochs[-1]["rmse_te"], om.epochs[-1]["rmse_te"]
+    assert abs(tem - te32) / te32 < 0.005, (tem, te32)
+    U, _ = oracle_als(P, 1, 0.05)
+    G1, _ = engine_run(ctx, P, ctc.ALS, 1, precision=ctc.PREC_MIXED, tile_len=256, **lam)
+    assert max_factor_rel(G1, U) < 3e-2
+
+
 def test_als_compat_matches_reference_semantics(ctx):
     """compat=1: values stored through an integer and the reference warp
     kernel's per-lane multiplicities (nnz % 32 == 0 for every copy)."""
@@ -158,6 +181,30 @@ def test_ccdpp_f32(ctx):
     P = Problem(50000, (500, 300, 60), 32, seed=10)
     U, hist, _ = oracle_ccdpp(P, 3, 0.1, 3)
     G, out = engine_run(ctx, P, ctc.CCDPP, 3, precision=ctc.PREC_F32, inner=3, **{"lambda": 0.1})
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-5, e
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-5, e
+    assert max_factor_rel(G, U) < 1e-4
+
+
+@pytest.mark.parametrize("tile_len", [128, 256, 512])
+def test_ccdpp_column_staging_paths_agree(ctx, tile_len):
+    """The factor columns a pass gathers come from shared memory (staged by a
+    bulk async copy) when they fit the block budget, else from global
+    memory.  All staged, one staged and none staged give bit-identical
+    factors (same values, same summation order), and match the oracle."""
+    P = Problem(40000, (9000, 700, 40), 16, seed=44, heavy_row=3000)
+    U, hist, _ = oracle_ccdpp(P, 2, 0.1, 2)
+    runs = {}
+    # budgets: default (all fit), one column fits (mode 2: 40 values), none
+    for budget in (0, 1024, -1):
+        G, out = engine_run(ctx, P, ctc.CCDPP, 2, precision=ctc.PREC_F32, inner=2, tile_len=tile_len,
+                            smem_budget=budget, **{"lambda": 0.1})
+        runs[budget] = (G, out)
+    for budget in (1024, -1):
+        for m in range(3):
+            assert np.array_equal(runs[budget][0][m], runs[0][0][m]), (budget, m)
+    G, out = runs[0]
     for e, (tr, te) in enumerate(hist):
         assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-5, e
         assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-5, e
