@@ -311,7 +311,7 @@ def run_ours(args):
         "nnz_per_s": {"ccdpp": n_train / (ccd_ms / 1000.0), "sgd": n_train / (sgd_ms / 1000.0)},
         "roofline": {"bound": "hbm", "kernel": "k_ccdpp_pass", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
-                     "traffic": profile_traffic("k_ccdpp_pass"),
+                     "traffic": profile_traffic("k_ccdpp_pass__zipf100m"),
                      "bytes_per_launch": pass_bytes, "launches": pass_n, "avg_launch_ms": pass_avg_ms,
                      "share_of_step": pass_ms / max(total_ms, 1e-9),
                      "layout_bytes_per_launch": layout_bytes, "layout_GBps": layout_gbps,
