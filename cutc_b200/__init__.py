@@ -7,11 +7,11 @@ CUDA/C++ sources (csrc/), the in-tree build (build.py) and the Python
 bindings (api.py).
 """
 from .api import (ALS, CCD, CCDPP, SGD, PREC_F32, PREC_F64, PREC_MIXED, LR_BOLD_DRIVER,
-                  LR_CONSTANT, LR_EXP_DECAY, SGD_HOGWILD, SGD_SEQUENTIAL, Context, CtcError,
+                  LR_CONSTANT, LR_EXP_DECAY, SGD_HOGWILD, SGD_SEQUENTIAL, Batch, Context, CtcError,
                   Dataset, Model, Params, Tensor, ciss_alloc, grad, lib, params, rmse, run, tc_als,
                   tc_ccd, tc_main_ciss, tc_sgd, tt_read)
 
 __all__ = ["ALS", "CCD", "CCDPP", "SGD", "PREC_F32", "PREC_F64", "PREC_MIXED", "LR_BOLD_DRIVER",
-           "LR_CONSTANT", "LR_EXP_DECAY", "SGD_HOGWILD", "SGD_SEQUENTIAL", "Context", "CtcError",
+           "LR_CONSTANT", "LR_EXP_DECAY", "SGD_HOGWILD", "SGD_SEQUENTIAL", "Batch", "Context", "CtcError",
            "Dataset", "Model", "Params", "Tensor", "ciss_alloc", "grad", "lib", "params", "rmse",
            "run", "tc_als", "tc_ccd", "tc_main_ciss", "tc_sgd", "tt_read"]

@@ -66,6 +66,8 @@ class Result(C.Structure):
 
 
 EPOCH_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(EpochStats))
+BATCH_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                       C.c_double)
 
 _lib = None
 
@@ -122,6 +124,11 @@ def lib():
             "ctc_rmse": (C.c_int, [P, P, P, _f64p]),
             "ctc_grad": (C.c_int, [P, P, P, C.c_double, C.POINTER(_f64p), _f64p]),
             "ctc_sse_noalloc": (C.c_int, [P, C.c_uint64, P, P, P, C.c_int, P, P]),
+            "ctc_batch_create": (C.c_int, [P, C.c_int, C.POINTER(P), C.POINTER(P), C.POINTER(Params),
+                                           C.POINTER(P)]),
+            "ctc_batch_free": (C.c_int, [P]),
+            "ctc_batch_info": (C.c_int, [P, C.POINTER(C.c_int), _u64p, _u64p]),
+            "ctc_batch_run": (C.c_int, [P, C.POINTER(P), C.POINTER(Params), BATCH_CB, P, C.POINTER(Result)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -514,3 +521,63 @@ def tc_main_ciss(traina, trainb, trainc, validation, test, algorithm_index: int,
     else:
         out = fn(traina, trainb, trainc, validation, test, mats, best, **kw)
     return mats, best, out
+
+
+@dataclass
+class BatchOutput:
+    """Per-instance RMSE history of a batch run: epochs[k] = (epoch, ms_epoch,
+    rmse_tr[ninst], rmse_te[ninst])."""
+    result: dict
+    epochs: list = field(default_factory=list)
+
+
+class Batch:
+    """Many independent completion problems trained together (ctc_batch):
+    one block-diagonal stacked tensor, one launch per kernel and epoch."""
+
+    def __init__(self, ctx: Context, train, test, p: Params):
+        n = len(train)
+        if test is not None and len(test) != n:
+            raise ValueError("train and test lists differ in length")
+        tr = (C.c_void_p * n)(*[t.h for t in train])
+        te = (C.c_void_p * n)(*[t.h for t in test]) if test is not None else None
+        h = C.c_void_p()
+        _check(lib().ctc_batch_create(ctx.h, n, tr, te, C.byref(p), C.byref(h)))
+        self.h = h
+        self.ctx = ctx
+        self.ninst = n
+
+    def info(self):
+        n = C.c_int()
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(lib().ctc_batch_info(self.h, C.byref(n), C.byref(a), C.byref(b)))
+        return n.value, a.value, b.value
+
+    def run(self, models, p: Params, callback=None) -> BatchOutput:
+        if len(models) != self.ninst:
+            raise ValueError("one model per instance")
+        out = BatchOutput(result={})
+
+        def _cb(_user, epoch, n, rtr, rte, ms):
+            tr = np.array(rtr[:n], dtype=np.float64)
+            te = np.array(rte[:n], dtype=np.float64)
+            out.epochs.append((epoch, ms, tr, te))
+            return int(bool(callback(epoch, ms, tr, te))) if callback else 0
+
+        cb = BATCH_CB(_cb)
+        res = Result()
+        hs = (C.c_void_p * self.ninst)(*[m.h for m in models])
+        _check(lib().ctc_batch_run(self.h, hs, C.byref(p), cb, None, C.byref(res)))
+        out.result = _result_dict(res)
+        return out
+
+    def free(self):
+        if self.h:
+            lib().ctc_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -386,6 +386,10 @@ struct SessionBase {
     virtual void save_best() = 0;
     virtual uint64_t nonspd() = 0;
     virtual void set_params(const ctc_params &p) = 0;
+    // squared error per batch instance over instance-aligned chunks of the
+    // mode-1 training copy (which = 0) or the test tensor (which = 1)
+    virtual void seg_sse(int which, const uint4 *chunks, uint32_t nchunks, const uint32_t *first, int ninst,
+                         double *partial, double *out) = 0;
 };
 
 }  // namespace ctc
@@ -959,10 +963,9 @@ struct Session : SessionBase {
     }
 
     // scalars: 0 train SSE, 2 val SSE, 3 test SSE, 4..6 sum of squares of U
-    void evaluate(ctc_epoch_stats *st) override
+    // row-major device factors (CCD++ keeps them column-major: converted)
+    void row_factors(const T *Urm[3])
     {
-        check_errors();
-        const T *Urm[3];
         for (int m = 0; m < 3; ++m) {
             if (colmajor) {
                 LAUNCH(ctx, k::k_col_to_row<T>, grid_for((uint64_t)dims[m] * R, 256, kSMs * 8), 256, 0,
@@ -972,6 +975,27 @@ struct Session : SessionBase {
                 Urm[m] = U[m].p;
             }
         }
+    }
+
+    void seg_sse(int which, const uint4 *chunks, uint32_t nchunks, const uint32_t *first, int ninst, double *partial,
+                 double *out) override
+    {
+        if (colmajor) fail(CTC_E_UNSUP, "per-instance errors need the record layout (not CCD++)");
+        const DevTensor<T> &t = which == 0 ? D->copy[0] : D->test;
+        const T *Urm[3];
+        row_factors(Urm);
+        if (nchunks)
+            LAUNCH(ctx, k::k_sse_chunks<T, R>, std::min<uint32_t>(nchunks, kSMs * 8), 256, 0, (const uint4 *)t.rec.p,
+                   (const double *)t.v64.p, chunks, nchunks, Urm[0], Urm[1], Urm[2], partial);
+        LAUNCH(ctx, k::k_fold_segments, grid_for((uint64_t)ninst, 128, 64), 128, 0, (const double *)partial, first,
+               ninst, out);
+    }
+
+    void evaluate(ctc_epoch_stats *st) override
+    {
+        check_errors();
+        const T *Urm[3];
+        row_factors(Urm);
         if (colmajor) {
             // copy 0 holds r = x - model: its SSE is the sum of squares
             sumsq_into(D->copy[0].res.p, D->copy[0].nslots, 0);
@@ -1447,5 +1471,298 @@ extern "C" int ctc_grad(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *mode
             constexpr int R = decltype(RC)::value;
             grad_impl<double, R>(ctx, t, model, lambda, grads, obj);
         });
+    });
+}
+
+// ---------------------------------------------------------------------
+// Batches of independent completion problems.  Instance b's tensors are
+// stacked into one block-diagonal tensor: its mode-m indices are shifted by
+// off[m][b] = sum of the earlier instances' dimensions, so rows of different
+// instances never meet.  One dataset over the stacked tensor then trains
+// every instance with one launch per kernel and epoch, the tile plan
+// balancing the work across instance boundaries; the ALS row solves, the
+// SGD updates and the reference CCD+ updates of an instance see only its
+// own nonzeros.  Errors are kept per instance: the mode-1 training copy and
+// the test tensor are instance-contiguous, cut into chunks that never
+// straddle two instances, and summed per instance in chunk order.
+// ---------------------------------------------------------------------
+struct ctc_batch {
+    ctc_ctx *ctx = nullptr;
+    int ninst = 0;
+    ctc_params p{};
+    std::unique_ptr<ctc_dataset> ds;
+    std::vector<uint64_t> off[3], idims[3];
+    std::vector<uint64_t> ntr, nte;
+    bool has_test = false;
+    ctc::DevBuf<uint4> ch_tr, ch_te;
+    ctc::DevBuf<uint32_t> first_tr, first_te;
+    uint32_t nch_tr = 0, nch_te = 0;
+    ctc::DevBuf<double> partial, sse;  // sse: [0, ninst) train, [ninst, 2 ninst) test
+};
+
+namespace ctc {
+
+static constexpr uint32_t kBatchChunk = 16384;
+
+// chunks of [start_b, start_b + n_b) per instance, and each instance's first
+// chunk (ninst + 1 entries)
+static void batch_chunks(const std::vector<uint64_t> &n, std::vector<uint4> &ch, std::vector<uint32_t> &first)
+{
+    ch.clear();
+    first.assign(n.size() + 1, 0);
+    uint64_t start = 0;
+    for (size_t b = 0; b < n.size(); ++b) {
+        first[b] = (uint32_t)ch.size();
+        for (uint64_t s = 0; s < n[b]; s += kBatchChunk)
+            ch.push_back(make_uint4((uint32_t)(start + s), (uint32_t)(start + std::min<uint64_t>(n[b], s + kBatchChunk)),
+                                    (uint32_t)b, 0u));
+        start += n[b];
+    }
+    first[n.size()] = (uint32_t)ch.size();
+}
+
+static void batch_eval(ctc_batch *B, SessionBase *S, std::vector<double> &rtr, std::vector<double> &rte)
+{
+    const int n = B->ninst;
+    S->seg_sse(0, B->ch_tr.p, B->nch_tr, B->first_tr.p, n, B->partial.p, B->sse.p);
+    if (B->has_test) S->seg_sse(1, B->ch_te.p, B->nch_te, B->first_te.p, n, B->partial.p, B->sse.p + n);
+    std::vector<double> h(2 * (size_t)n, 0.0);
+    CK(cudaMemcpyAsync(h.data(), B->sse.p, (B->has_test ? 2 : 1) * (size_t)n * sizeof(double),
+                       cudaMemcpyDeviceToHost, B->ctx->stream));
+    CK(cudaStreamSynchronize(B->ctx->stream));
+    rtr.resize(n);
+    rte.resize(n);
+    for (int b = 0; b < n; ++b) {
+        rtr[b] = B->ntr[b] ? std::sqrt(h[b] / (double)B->ntr[b]) : 0.0;
+        rte[b] = (B->has_test && B->nte[b]) ? std::sqrt(h[n + b] / (double)B->nte[b]) : -1.0;
+        if (!std::isfinite(rtr[b])) fail(CTC_E_NUMERIC, "instance %d: training error is not finite", b);
+    }
+}
+
+}  // namespace ctc
+
+extern "C" int ctc_batch_create(ctc_ctx *ctx, int ninst, const ctc_tensor *const *train,
+                                const ctc_tensor *const *test, const ctc_params *p, ctc_batch **out)
+{
+    return guarded([&] {
+        if (!ctx || !train || !out || ninst <= 0) fail(CTC_E_ARG, "null argument or no instances");
+        check_params(p);
+        if (p->alg == CTC_ALG_CCDPP) fail(CTC_E_UNSUP, "batches run ALS, CCD and SGD");
+        if (p->compat) fail(CTC_E_UNSUP, "batches run the plain update rules (compat = 0)");
+        CK(cudaSetDevice(ctx->device));
+        auto B = std::make_unique<ctc_batch>();
+        B->ctx = ctx;
+        B->ninst = ninst;
+        B->p = *p;
+        B->has_test = test != nullptr;
+        uint64_t ntot = 0, ttot = 0;
+        for (int m = 0; m < 3; ++m) {
+            B->off[m].assign(ninst + 1, 0);
+            B->idims[m].assign(ninst, 0);
+        }
+        B->ntr.assign(ninst, 0);
+        B->nte.assign(ninst, 0);
+        for (int b = 0; b < ninst; ++b) {
+            const ctc_tensor *tr = train[b], *te = test ? test[b] : nullptr;
+            if (!tr || tr->nmodes != 3 || tr->nnz == 0) fail(CTC_E_ARG, "instance %d: empty or not order-3 training tensor", b);
+            if (test && (!te || te->nmodes != 3)) fail(CTC_E_ARG, "instance %d: missing or not order-3 test tensor", b);
+            for (int m = 0; m < 3; ++m) {
+                B->idims[m][b] = std::max(tr->dims[m], te ? te->dims[m] : 0);
+                B->off[m][b + 1] = B->off[m][b] + B->idims[m][b];
+            }
+            B->ntr[b] = tr->nnz;
+            B->nte[b] = te ? te->nnz : 0;
+            ntot += tr->nnz;
+            ttot += B->nte[b];
+        }
+        for (int m = 0; m < 3; ++m)
+            if (B->off[m][ninst] >= 0xfffffff0ull) fail(CTC_E_UNSUP, "stacked dimension %d exceeds 2^32", m + 1);
+        if (ntot >= 0x7fffffffull || ttot >= 0x7fffffffull) fail(CTC_E_UNSUP, "more than 2^31 stacked nonzeros");
+        // stacked tensors (1-based indices shifted by the instance offsets)
+        auto stack = [&](const ctc_tensor *const *src, uint64_t total, const std::vector<uint64_t> &cnt) {
+            auto t = std::make_unique<ctc_tensor>();
+            t->nmodes = 3;
+            t->nnz = total;
+            for (int m = 0; m < 3; ++m) {
+                t->dims[m] = B->off[m][ninst];
+                t->ind[m].resize(total);
+            }
+            t->vals.resize(total);
+            std::vector<uint64_t> start(ninst + 1, 0);
+            for (int b = 0; b < ninst; ++b) start[b + 1] = start[b] + cnt[b];
+            // (indices were checked against the instance dims, which are
+            // their maxima; 0 is the one bad value left)
+            std::atomic<int> bad{-1};
+            for (int b = 0; b < ninst; ++b) {
+                const ctc_tensor *s = src[b];
+                for (int m = 0; m < 3; ++m) {
+                    const uint64_t o = B->off[m][b];
+                    const uint64_t *in = s->ind[m].data();
+                    uint64_t *dst = t->ind[m].data() + start[b];
+                    par_for(cnt[b], [&](uint64_t i0, uint64_t i1) {
+                        for (uint64_t i = i0; i < i1; ++i) {
+                            if (in[i] == 0) bad = b;
+                            dst[i] = in[i] + o;
+                        }
+                    });
+                }
+                std::copy(s->vals.begin(), s->vals.end(), t->vals.begin() + start[b]);
+            }
+            if (bad >= 0) fail(CTC_E_ARG, "instance %d: 0 index in a 1-based tensor", bad.load());
+            return t;
+        };
+        std::unique_ptr<ctc_tensor> st = stack(train, ntot, B->ntr);
+        // mode-1 order of the stacked tensor is instance-major: instance b's
+        // training nonzeros are [sum of earlier counts, + ntr[b]) in copy 0
+        if (ctc_tensor_sort(st.get(), 0) != CTC_OK) fail(CTC_E_ARG, "%s", ctc_last_error());
+        std::unique_ptr<ctc_tensor> tt;
+        if (test) tt = stack(test, ttot, B->nte);
+        auto ds = std::make_unique<ctc_dataset>();
+        ds->ctx = ctx;
+        ds->p = *p;
+        for (int m = 0; m < 3; ++m) ds->dims[m] = B->off[m][ninst];
+        ds->nnz_train = ntot;
+        ds->has_val = false;
+        ds->has_test = test != nullptr;
+        const ctc_tensor *tr3[3] = {st.get(), nullptr, nullptr};
+        if (p->precision == CTC_PREC_F64) build_dataset<double>(ds.get(), tr3, nullptr, tt.get());
+        else build_dataset<float>(ds.get(), tr3, nullptr, tt.get());
+        B->ds = std::move(ds);
+        std::vector<uint4> ch;
+        std::vector<uint32_t> first;
+        batch_chunks(B->ntr, ch, first);
+        B->nch_tr = (uint32_t)ch.size();
+        B->ch_tr.upload(ch.data(), ch.size(), ctx->stream);
+        B->first_tr.upload(first.data(), first.size(), ctx->stream);
+        size_t nparts = ch.size();
+        if (test) {
+            batch_chunks(B->nte, ch, first);
+            B->nch_te = (uint32_t)ch.size();
+            B->ch_te.upload(ch.data(), ch.size(), ctx->stream);
+            B->first_te.upload(first.data(), first.size(), ctx->stream);
+            nparts = std::max(nparts, ch.size());
+        }
+        B->partial.alloc(std::max<size_t>(nparts, 1));
+        B->sse.alloc(2 * (size_t)ninst);
+        CK(cudaStreamSynchronize(ctx->stream));
+        *out = B.release();
+    });
+}
+
+extern "C" int ctc_batch_free(ctc_batch *b)
+{
+    if (b) {
+        cudaSetDevice(b->ctx->device);
+        cudaStreamSynchronize(b->ctx->stream);
+        delete b;
+    }
+    return CTC_OK;
+}
+
+extern "C" int ctc_batch_info(const ctc_batch *b, int *ninst, uint64_t *nnz_train, uint64_t *nnz_test)
+{
+    return guarded([&] {
+        if (!b) fail(CTC_E_ARG, "null batch");
+        if (ninst) *ninst = b->ninst;
+        uint64_t a = 0, c = 0;
+        for (int i = 0; i < b->ninst; ++i) {
+            a += b->ntr[i];
+            c += b->nte[i];
+        }
+        if (nnz_train) *nnz_train = a;
+        if (nnz_test) *nnz_test = c;
+    });
+}
+
+extern "C" int ctc_batch_run(ctc_batch *B, ctc_model *const *models, const ctc_params *p, ctc_batch_cb cb,
+                             void *user, ctc_result *res)
+{
+    return guarded([&] {
+        if (!B || !models) fail(CTC_E_ARG, "null argument");
+        check_params(p);
+        if (p->alg != B->p.alg || p->precision != B->p.precision || p->compat != B->p.compat ||
+            p->tile_len != B->p.tile_len)
+            fail(CTC_E_ARG, "parameters differ from the batch's (alg/precision/compat/tile_len)");
+        const int n = B->ninst, R = p->rank;
+        // the stacked model: instance b's rows at off[m][b]
+        ctc_model sm;
+        sm.nmodes = 3;
+        sm.rank = R;
+        for (int m = 0; m < 3; ++m) {
+            sm.dims[m] = B->off[m][n];
+            sm.U[m].assign(sm.dims[m] * (uint64_t)R, 0.0);
+        }
+        for (int b = 0; b < n; ++b) {
+            const ctc_model *mb = models[b];
+            if (!mb || mb->nmodes != 3 || mb->rank != R) fail(CTC_E_ARG, "instance %d: model missing or of another rank", b);
+            for (int m = 0; m < 3; ++m) {
+                if (mb->dims[m] < B->idims[m][b]) fail(CTC_E_ARG, "instance %d: model smaller than its tensors", b);
+                std::copy(mb->U[m].begin(), mb->U[m].begin() + B->idims[m][b] * R,
+                          sm.U[m].begin() + B->off[m][b] * R);
+            }
+        }
+        ctc_ctx *ctx = B->ctx;
+        CK(cudaSetDevice(ctx->device));
+        B->ds->p = *p;
+        SessionBase *S = session_for(B->ds.get(), R);
+        S->set_params(*p);
+        S->set_model(&sm);
+        double lr_base = p->lr, total_ms = 0, prev_obj = 0;
+        const double scale = p->lr_scale > 0 ? p->lr_scale : 1.0;
+        std::vector<double> rtr, rte;
+        auto report = [&](int epoch, double ms) -> bool {
+            batch_eval(B, S, rtr, rte);
+            return cb ? cb(user, epoch, n, rtr.data(), rte.data(), ms) != 0 : false;
+        };
+        bool stop = report(0, 0.0);
+        int e = 1;
+        for (; !stop && e <= p->iters; ++e) {
+            CK(cudaEventRecord(ctx->ev0, ctx->stream));
+            S->epochs(1);
+            CK(cudaEventRecord(ctx->ev1, ctx->stream));
+            CK(cudaEventSynchronize(ctx->ev1));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            total_ms += ms;
+            const bool bold = p->alg == CTC_ALG_SGD && p->lr_schedule == CTC_LR_BOLD_DRIVER;
+            if (bold || e == p->iters || (p->eval_every > 0 && e % p->eval_every == 0)) stop = report(e, ms);
+            if (p->alg == CTC_ALG_SGD) {
+                if (bold) {
+                    // the schedule follows the summed training error of all instances
+                    double obj = 0;
+                    for (int b = 0; b < n; ++b) obj += rtr[b] * rtr[b] * (double)B->ntr[b];
+                    if (e > 1) lr_base *= (obj < prev_obj) ? 1.05 : 0.50;
+                    prev_obj = obj;
+                } else if (p->lr_schedule == CTC_LR_EXP_DECAY) {
+                    lr_base *= p->lr_decay;
+                }
+                S->set_lr(lr_base * scale);
+            }
+        }
+        S->get_model(&sm, false);
+        for (int b = 0; b < n; ++b)
+            for (int m = 0; m < 3; ++m)
+                std::copy(sm.U[m].begin() + B->off[m][b] * R, sm.U[m].begin() + (B->off[m][b] + B->idims[m][b]) * R,
+                          models[b]->U[m].begin());
+        if (res) {
+            *res = ctc_result{};
+            res->epochs_run = e - 1;
+            res->total_ms = total_ms;
+            res->best_epoch = e - 1;
+            double se_tr = 0, se_te = 0, ntr = 0, nte = 0;
+            for (int b = 0; b < n; ++b) {
+                se_tr += rtr[b] * rtr[b] * (double)B->ntr[b];
+                ntr += (double)B->ntr[b];
+                if (B->has_test) {
+                    se_te += rte[b] * rte[b] * (double)B->nte[b];
+                    nte += (double)B->nte[b];
+                }
+            }
+            res->final_rmse_tr = ntr > 0 ? std::sqrt(se_tr / ntr) : 0.0;
+            res->final_rmse_te = nte > 0 ? std::sqrt(se_te / nte) : -1.0;
+            res->final_rmse_vl = -1.0;
+            res->best_rmse = res->final_rmse_tr;
+            res->nonspd_rows = S->nonspd();
+        }
     });
 }

@@ -133,6 +133,54 @@ __global__ void __launch_bounds__(256) k_sse(const uint4 *__restrict__ rec,
     if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
 
+// Squared error over chunks that each lie inside one instance of a batch
+// (chunk = {begin, end, instance, 0}): block per chunk, one double partial
+// per chunk; k_fold_segments sums each instance's chunks in order.
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_sse_chunks(const uint4 *__restrict__ rec, const double *__restrict__ v64,
+                                                    const uint4 *__restrict__ chunks, uint32_t nchunks,
+                                                    const T *__restrict__ U0, const T *__restrict__ U1,
+                                                    const T *__restrict__ U2, double *__restrict__ partial)
+{
+    using V = typename Vec<T>::type;
+    constexpr int VN = Vec<T>::n;
+    for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const uint4 ch = chunks[c];
+        double acc = 0;
+        for (uint32_t idx = ch.x + threadIdx.x; idx < ch.y; idx += blockDim.x) {
+            const uint4 r = rec[idx];
+            const T x = value_of<T>(r, v64, idx);
+            const V *a = reinterpret_cast<const V *>(U0 + (size_t)r.x * R);
+            const V *b = reinterpret_cast<const V *>(U1 + (size_t)r.y * R);
+            const V *cc = reinterpret_cast<const V *>(U2 + (size_t)r.z * R);
+            T pr = 0;
+#pragma unroll
+            for (int q = 0; q < R / VN; ++q) {
+                const V va = a[q], vb = b[q], vc = cc[q];
+#pragma unroll
+                for (int v = 0; v < VN; ++v) pr += vget(va, v) * vget(vb, v) * vget(vc, v);
+            }
+            const T e = x - pr;
+            acc += (double)e * (double)e;
+        }
+        acc = block_sum(acc);
+        if (threadIdx.x == 0) partial[c] = acc;
+        __syncthreads();  // block_sum's shared slots are reused by the next chunk
+    }
+}
+
+// out[i] = sum of partial[first[i] .. first[i+1]) in order (thread per
+// instance)
+__global__ void k_fold_segments(const double *__restrict__ partial, const uint32_t *__restrict__ first, int ninst,
+                                double *__restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ninst; i += gridDim.x * blockDim.x) {
+        double acc = 0;
+        for (uint32_t c = first[i]; c < first[i + 1]; ++c) acc += partial[c];
+        out[i] = acc;
+    }
+}
+
 // Sum of squares of a dense array (for lambda * ||U||^2).
 template <typename T>
 __global__ void __launch_bounds__(256) k_sumsq(const T *__restrict__ x, uint64_t n,

@@ -124,6 +124,46 @@ def generate(w: Workload, seed: int = 0, device: str = "cpu", train_frac: float 
     return dict(train=pack(train_mask), test=pack(~train_mask), dims=tuple(w.dims))
 
 
+@dataclass
+class BatchWorkload:
+    name: str
+    ninst: int
+    dim_range: tuple   # each mode dimension log-uniform in [lo, hi]
+    nnz_range: tuple   # nonzeros per instance log-uniform in [lo, hi]
+    cp_rank: int
+    rank: int
+    sigma: float
+
+
+BATCH_WORKLOADS = {
+    # 256 instances, dims log-U[1e3, 5e4], nnz log-U[1e4, 5e6], uniform
+    # distinct cells, CP rank 8 + N(0, 0.1^2), R = 16
+    "batch-256": BatchWorkload("batch-256", 256, (1_000, 50_000), (10_000, 5_000_000), 8, 16, 0.1),
+}
+
+
+def batch_shapes(bw: BatchWorkload, seed: int = 0):
+    """Per-instance (dims, nnz), drawn log-uniformly from a seeded numpy
+    generator (the shapes do not depend on the device)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(bw.dim_range[0]), np.log(bw.dim_range[1])
+    dims = np.exp(rng.uniform(lo, hi, (bw.ninst, 3))).astype(np.int64)
+    lo, hi = np.log(bw.nnz_range[0]), np.log(bw.nnz_range[1])
+    nnz = np.exp(rng.uniform(lo, hi, bw.ninst)).astype(np.int64)
+    cells = dims.prod(axis=1)
+    nnz = np.minimum(nnz, cells // 2)  # distinct cells stay drawable
+    return [(tuple(int(x) for x in d), int(n)) for d, n in zip(dims, nnz)]
+
+
+def generate_batch(bw: BatchWorkload, seed: int = 0, device: str = "cpu", train_frac: float = 0.9):
+    """Yields one dict(train=(ind, vals), test=(ind, vals), dims) per
+    instance: uniform distinct cells, values from the instance's own rank-k
+    CP model mapped to [1, 5] plus N(0, sigma^2) noise (not clipped)."""
+    for b, (dims, nnz) in enumerate(batch_shapes(bw, seed)):
+        w = Workload(f"{bw.name}#{b}", dims, nnz, bw.cp_rank, bw.rank, bw.sigma, False, None)
+        yield generate(w, seed=seed * 100_003 + b + 1, device=device, train_frac=train_frac)
+
+
 def sort_for_mode(ind, vals, mode):
     """Stable sort by (ind[mode], ind[(mode+1)%3]) -- the reference's file order."""
     order = np.lexsort((ind[(mode + 1) % 3], ind[mode]))

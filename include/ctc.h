@@ -258,6 +258,30 @@ int ctc_dataset_set_lr(ctc_dataset *d, double lr);
 int ctc_dataset_evaluate(ctc_dataset *d, ctc_epoch_stats *st);
 int ctc_dataset_get_model(ctc_dataset *d, ctc_model *model);
 
+/* Batches of independent completion problems (no reference counterpart;
+ * the reference runs one problem per process).  Instance b's training and
+ * test tensors (1-based indices, any order) are stacked into one
+ * block-diagonal tensor whose mode-m rows of instance b start after the
+ * rows of instances 0..b-1, so each epoch is one launch per kernel over all
+ * instances, load-balanced by one tile plan.  ALS, CCD and SGD (not CCD++,
+ * not compat).  Instance dims are the maximum index over its train/test
+ * tensors.  test may be NULL. */
+typedef struct ctc_batch ctc_batch;
+int ctc_batch_create(ctc_ctx *ctx, int ninst, const ctc_tensor *const *train,
+                     const ctc_tensor *const *test, const ctc_params *p, ctc_batch **out);
+int ctc_batch_free(ctc_batch *b);
+int ctc_batch_info(const ctc_batch *b, int *ninst, uint64_t *nnz_train, uint64_t *nnz_test);
+/* Called after every evaluated epoch with each instance's train and test
+ * RMSE (test: -1 without test tensors); non-zero stops the run. */
+typedef int (*ctc_batch_cb)(void *user, int epoch, int ninst, const double *rmse_tr,
+                            const double *rmse_te, double ms_epoch);
+/* Runs p->iters epochs of all instances.  models[b]: instance b's initial
+ * factors (rank p->rank, at least its dims), replaced by the final ones.
+ * The SGD schedule is shared; the bold driver follows the summed training
+ * error.  res (may be NULL): totals over all instances. */
+int ctc_batch_run(ctc_batch *b, ctc_model *const *models, const ctc_params *p, ctc_batch_cb cb,
+                  void *user, ctc_result *res);
+
 /* Per-kernel device time: with profiling on, every launch of this library
  * on the context is bracketed by a CUDA event pair; kernel_time sums the
  * launches whose kernel name contains `name` (count, milliseconds).  No
