@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip e2e / time-to-RMSE / CPU legs")
     ap.add_argument("--ccdpp-tile", type=int, default=0, help="CCD++ tile length (0 = library default)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 256-instance leg")
+    ap.add_argument("--instances", type=int, default=0, help="batch workloads: a K-instance sample of the same distribution")
     return ap.parse_args()
 
 
@@ -355,6 +356,9 @@ def batch_leg(ctc, ctx, args, device):
     1.005 x its own final test RMSE."""
     from cutc_b200 import synth
     bw = synth.BATCH_WORKLOADS["batch-256"]
+    if args.instances:
+        bw = synth.BatchWorkload(bw.name + f"@{args.instances}", args.instances, bw.dim_range, bw.nnz_range,
+                                 bw.cp_rank, bw.rank, bw.sigma)
     R = bw.rank
     t0 = time.time()
     train, test, idims = [], [], []
@@ -492,9 +496,32 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def run_batch_only(args):
+    """--workload batch-256: the batched leg alone, as its own JSON line."""
+    import torch
+
+    import cutc_b200 as ctc
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    ctx = ctc.Context(local)
+    b = batch_leg(ctc, ctx, args, f"cuda:{local}")
+    ntr = b["nnz_train"]
+    step_s = (b["als"]["epoch_ms"] + b["sgd"]["epoch_ms"]) / 1000.0
+    print(json.dumps({"metric": "batched training nnz/s (one ALS + one SGD epoch of all instances per step)",
+                      "value": 2 * ntr / step_s, "unit": UNIT, "n_gpus": 1, "steps": 10, "warmup": 0,
+                      "ms_per_step": 1000.0 * step_s, "higher_is_better": True, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform CP instances)",
+                      "config": {"workload": b["workload"]}, "batched": b}))
+    ctx.close()
+
+
 if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload.startswith("batch"):
+        run_batch_only(a)
     else:
         run_ours(a)

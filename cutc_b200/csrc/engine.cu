@@ -551,7 +551,8 @@ struct Session : SessionBase {
         if (p.alg == CTC_ALG_ALS) {
             using Sh = k::AlsShape<R>;
             const int smem = (int)(4 * Sh::smem_doubles * sizeof(double));
-            CK(cudaFuncSetAttribute(k::k_als_tile<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            const int smem_tile = (int)(4 * k::AlsBatch<T, R>::warp_doubles * sizeof(double));
+            CK(cudaFuncSetAttribute(k::k_als_tile<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_tile));
             CK(cudaFuncSetAttribute(k::k_als_fix<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         }
         CK(cudaStreamSynchronize(ctx->stream));
@@ -722,7 +723,8 @@ struct Session : SessionBase {
             const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
             DevTensor<T> &c = D->copy[m];
             CK(cudaMemsetAsync(U[m].p, 0, (size_t)dims[m] * R * sizeof(T), ctx->stream));
-            LAUNCH(ctx, k::k_als_tile<T, R>, grid_for(c.ntiles, 4, kSMs * 16), 128, smem, (const int4 *)c.tiles.p,
+            LAUNCH(ctx, k::k_als_tile<T, R>, grid_for(c.ntiles, 4, kSMs * 16), 128,
+                   4 * k::AlsBatch<T, R>::warp_doubles * sizeof(double), (const int4 *)c.tiles.p,
                    c.ntiles, (const uint4 *)c.rec.p, (const double *)c.v64.p,
                    (const T *)(c.has_w ? c.w.p : nullptr), m, U[m].p, (const T *)U[m1].p, (const T *)U[m2].p,
                    (T)p.lambda, slot.p, nonspd_dev.p, tc ? 1 : 0);

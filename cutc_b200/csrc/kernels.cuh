@@ -966,6 +966,135 @@ __device__ __forceinline__ int als_solve_warp(const T (&G)[R][AlsShape<R>::C], c
     return bad;
 }
 
+// Batched row solves of the light tiles: a warp parks the regularised
+// systems of NS rows in shared memory and factors them together, one group
+// of GS lanes per system (FP64 right-looking Cholesky on the packed lower
+// triangle, forward/back substitution, one refinement step against the
+// FP32/FP64 Gram as accumulated).  Per system: factor (TRI doubles), b, y,
+// u (R doubles each), the Gram (TRI of T); per warp also NS row ids.
+template <typename T, int R>
+struct AlsBatch {
+    static constexpr int GS = R >= 64 ? 32 : (R >= 8 ? R / 4 : 2);
+    static constexpr int NS = 32 / GS;
+    static constexpr int TRI = R * (R + 1) / 2;
+    static constexpr int gram_doubles = (TRI * (int)sizeof(T) + 7) / 8;
+    static constexpr int sys_doubles = TRI + 3 * R + gram_doubles;
+    static constexpr int warp_doubles = NS * sys_doubles + (NS + 1) / 2;
+};
+
+__device__ __forceinline__ int tri_idx(int i, int k) { return i * (i + 1) / 2 + k; }
+
+// Factor and solve the k (<= NS) parked systems of this warp; writes u into
+// the rows' factor rows.  Returns the number of systems whose pivot was not
+// positive (diagonal shifted), counted once per system.
+template <typename T, int R>
+__device__ __forceinline__ int als_solve_parked(double *W, int k, T lambda, T *Um)
+{
+    using B = AlsBatch<T, R>;
+    constexpr int GS = B::GS;
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / GS, sl = lane % GS;
+    const bool act = grp < k;
+    double *fac = W + (size_t)(act ? grp : 0) * B::sys_doubles;
+    double *bb = fac + B::TRI;
+    double *yy = bb + R;
+    double *uu = yy + R;
+    const T *gram = reinterpret_cast<const T *>(uu + R);
+    const uint32_t *rows = reinterpret_cast<const uint32_t *>(W + (size_t)B::NS * B::sys_doubles);
+    int bad = 0;
+    for (int j = 0; j < R; ++j) {
+        double d = act ? fac[tri_idx(j, j)] : 1.0;
+        if (act && !(d > 0.0)) {
+            bad = 1;
+            d = 1e-300 + fabs(d) + 1e-12 * (double)lambda + 1e-30;
+        }
+        const double ljj = sqrt(d);
+        __syncwarp();
+        if (act) {
+            if (sl == 0) fac[tri_idx(j, j)] = ljj;
+            for (int i = j + 1 + sl; i < R; i += GS) fac[tri_idx(i, j)] /= ljj;
+        }
+        __syncwarp();
+        if (act)
+            for (int i = j + 1 + sl; i < R; i += GS) {
+                const double lij = fac[tri_idx(i, j)];
+                for (int k2 = j + 1; k2 <= i; ++k2) fac[tri_idx(i, k2)] -= lij * fac[tri_idx(k2, j)];
+            }
+        __syncwarp();
+    }
+    for (int it = 0; it < 2; ++it) {
+        for (int i = 0; i < R; ++i) {  // L z = y
+            const double zi = act ? yy[i] / fac[tri_idx(i, i)] : 0.0;
+            __syncwarp();
+            if (act) {
+                if (sl == 0) yy[i] = zi;
+                for (int k2 = i + 1 + sl; k2 < R; k2 += GS) yy[k2] -= fac[tri_idx(k2, i)] * zi;
+            }
+            __syncwarp();
+        }
+        for (int i = R - 1; i >= 0; --i) {  // L^T v = z
+            const double vi = act ? yy[i] / fac[tri_idx(i, i)] : 0.0;
+            __syncwarp();
+            if (act) {
+                if (sl == 0) yy[i] = vi;
+                for (int k2 = sl; k2 < i; k2 += GS) yy[k2] -= fac[tri_idx(i, k2)] * vi;
+            }
+            __syncwarp();
+        }
+        if (it == 0) {
+            if (act)
+                for (int a = sl; a < R; a += GS) uu[a] = yy[a];
+            __syncwarp();
+            // residual b - (G + lambda I) u with the Gram as accumulated
+            if (act)
+                for (int a = sl; a < R; a += GS) {
+                    double acc = bb[a] - (double)lambda * uu[a];
+                    for (int c = 0; c < R; ++c)
+                        acc -= (double)gram[a >= c ? tri_idx(a, c) : tri_idx(c, a)] * uu[c];
+                    yy[a] = acc;
+                }
+            __syncwarp();
+        } else if (act) {
+            T *dst = Um + (size_t)rows[grp] * R;
+            for (int a = sl; a < R; a += GS) dst[a] = (T)(uu[a] + yy[a]);
+        }
+    }
+    __syncwarp();
+    return (act && sl == 0) ? bad : 0;
+}
+
+// Park the row's system (Gram G and right-hand side b as left by
+// als_accumulate: lane gl < L holds columns gl + L*c) in slot k.
+template <typename T, int R>
+__device__ __forceinline__ void als_park(double *W, int k, uint32_t row, const T (&G)[R][AlsShape<R>::C],
+                                         const T (&b)[AlsShape<R>::C], T lambda)
+{
+    using B = AlsBatch<T, R>;
+    using Sh = AlsShape<R>;
+    constexpr int L = Sh::L, C = Sh::C;
+    const int lane = threadIdx.x & 31;
+    double *fac = W + (size_t)k * B::sys_doubles;
+    double *bb = fac + B::TRI;
+    double *yy = bb + R;
+    T *gram = reinterpret_cast<T *>(yy + 2 * R);
+    if (lane < L) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const int col = lane + L * c;
+#pragma unroll
+            for (int a = 0; a < R; ++a)
+                if (a >= col) {
+                    fac[tri_idx(a, col)] = (double)G[a][c] + (a == col ? (double)lambda : 0.0);
+                    gram[tri_idx(a, col)] = G[a][c];
+                }
+            bb[col] = (double)b[c];
+            yy[col] = (double)b[c];
+        }
+    }
+    if (lane == 0) reinterpret_cast<uint32_t *>(W + (size_t)B::NS * B::sys_doubles)[k] = row;
+    __syncwarp();
+}
+
 template <typename T, int R>
 __device__ __forceinline__ void als_accumulate(const uint4 *__restrict__ rec,
                                                const double *__restrict__ v64,
@@ -1036,15 +1165,16 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
                                                   unsigned long long *nonspd, int skip_heavy)
 {
     using Sh = AlsShape<R>;
+    using Bt = AlsBatch<T, R>;
     constexpr int L = Sh::L, C = Sh::C;
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    double *S = smem + (size_t)wib * Sh::smem_doubles;
+    double *W = smem + (size_t)wib * Bt::warp_doubles;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const int gl = lane % L;
-    int bad = 0;
+    int bad = 0, parked = 0;
     T G[R][C];
     T b[C];
     for (uint64_t tile = warp; tile < ntiles; tile += nwarps) {
@@ -1067,14 +1197,29 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
         }
         uint32_t s = start;
         while (s < end) {
+            // the row's extent: 32 keys at a time, first mismatch by ballot
             const uint32_t key = key_of(rec[s], m);
             uint32_t e = s + 1;
-            while (e < end && key_of(rec[e], m) == key) ++e;
+            for (;;) {
+                const uint32_t q = e + lane;
+                const unsigned same = __ballot_sync(0xffffffffu, q < end && key_of(rec[q], m) == key);
+                if (same != 0xffffffffu) {
+                    e += __ffs(~same) - 1;
+                    break;
+                }
+                e += 32;
+            }
             als_accumulate<T, R>(rec, v64, w, m, Ua, Ub, s, e, G, b);
-            bad += als_solve_warp<T, R>(G, b, lambda, S, Um + (size_t)key * R);
+            als_park<T, R>(W, parked, key, G, b, lambda);
+            if (++parked == Bt::NS) {
+                bad += als_solve_parked<T, R>(W, parked, lambda, Um);
+                parked = 0;
+            }
             s = e;
         }
     }
+    if (parked) bad += als_solve_parked<T, R>(W, parked, lambda, Um);
+    bad = __reduce_add_sync(0xffffffffu, bad);
     if (lane == 0 && bad) atomicAdd(nonspd, (unsigned long long)bad);
 }
 

@@ -65,22 +65,25 @@ def test_batch_als_f64_matches_single_runs_and_oracle(ctx):
 
 
 def test_batch_als_f32_per_instance_rmse(ctx):
-    # rows of at least ~80 nonzeros: well-conditioned rank-32 systems, so
-    # FP32 summation order (tile packing differs between the stacked and the
-    # single runs) stays at rounding level in the factors
+    """FP32: per-iteration test RMSE of every instance within 1e-5 of the
+    FP64 oracle, factors after one iteration within 1e-4 (later iterations
+    compound FP32 Gram rounding), and the same RMSE as the instance alone."""
     probs = instances(7, 32, seed=2, nnz_range=(6000, 20000), dim_range=(20, 60))
-    Gb, ob = run_batch(ctx, probs, ctc.ALS, 3, precision=ctc.PREC_F32, **{"lambda": 0.05})
+    lam = {"lambda": 0.05}
+    G1, _ = run_batch(ctx, probs, ctc.ALS, 1, precision=ctc.PREC_F32, **lam)
+    Gb, ob = run_batch(ctx, probs, ctc.ALS, 3, precision=ctc.PREC_F32, **lam)
     for b, P in enumerate(probs):
-        # the FP64 oracle: factors within 1e-4
         U = P.factors()
-        for _ in range(3):
+        te = []
+        for it in range(3):
             for m in range(3):
                 po.als_mode(P.o_sorted(m), m, U, 0.05)
-        assert max_factor_rel(Gb[b], U) < 1e-4, b
-        # the same instance alone in FP32 (another summation order: each run
-        # is within 1e-4 of FP64, so the two are within 2e-4 of each other)
-        Ga, oa = run_alone(ctx, P, ctc.ALS, 3, precision=ctc.PREC_F32, **{"lambda": 0.05})
-        assert max_factor_rel(Gb[b], Ga) < 3e-4, b
+            if it == 0:
+                assert max_factor_rel(G1[b], U) < 1e-4, b
+            te.append(po.rmse(P.o_test(), U))
+        for it in range(3):
+            assert abs(ob.epochs[it + 1][3][b] - te[it]) / te[it] < 1e-5, (b, it)
+        Ga, oa = run_alone(ctx, P, ctc.ALS, 3, precision=ctc.PREC_F32, **lam)
         te_b, te_a = ob.epochs[-1][3][b], oa.epochs[-1]["rmse_te"]
         assert abs(te_b - te_a) / te_a < 1e-5, b
 
