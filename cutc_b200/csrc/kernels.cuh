@@ -874,9 +874,12 @@ __global__ void __launch_bounds__(128) k_ccdc_fix(const uint4 *__restrict__ heav
 // ---------------------------------------------------------------------
 template <int R>
 struct AlsShape {
-    static constexpr int L = R < 32 ? R : 32;
+    // C Gram columns per lane (lane gl holds columns gl + L*c), L = R / C
+    // lanes per nonzero, NG = 32 / L nonzeros per warp step: more columns
+    // per lane mean fewer shuffles per nonzero (R / C broadcasts of h)
+    static constexpr int C = R <= 8 ? 2 : (R <= 16 ? 4 : 2);
+    static constexpr int L = R / C;
     static constexpr int NG = 32 / L;
-    static constexpr int C = R / L;
     static constexpr int smem_doubles = R * R + 2 * R;  // per warp
 };
 
@@ -1077,16 +1080,20 @@ __device__ __forceinline__ void als_park(double *W, int k, uint32_t row, const T
     double *bb = fac + B::TRI;
     double *yy = bb + R;
     T *gram = reinterpret_cast<T *>(yy + 2 * R);
-    if (lane < L) {
+    // every group of L lanes holds the row's full sums; group g writes the
+    // Gram rows a with a % NG == g
+    constexpr int NG = Sh::NG;
+    const int gl = lane % L, g = lane / L;
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-            const int col = lane + L * c;
+    for (int c = 0; c < C; ++c) {
+        const int col = gl + L * c;
 #pragma unroll
-            for (int a = 0; a < R; ++a)
-                if (a >= col) {
-                    fac[tri_idx(a, col)] = (double)G[a][c] + (a == col ? (double)lambda : 0.0);
-                    gram[tri_idx(a, col)] = G[a][c];
-                }
+        for (int a = 0; a < R; ++a)
+            if (a % NG == g && a >= col) {
+                fac[tri_idx(a, col)] = (double)G[a][c] + (a == col ? (double)lambda : 0.0);
+                gram[tri_idx(a, col)] = G[a][c];
+            }
+        if (g == 0) {
             bb[col] = (double)b[c];
             yy[col] = (double)b[c];
         }
@@ -1117,7 +1124,7 @@ __device__ __forceinline__ void als_accumulate(const uint4 *__restrict__ rec,
     for (uint32_t base = s; base < e; base += NG) {
         const uint32_t p = base + g;
         const bool valid = p < e;
-        T hc[C];
+        T hc[C], hw[C];
         T wx = 0, wn = 0;
         if (valid) {
             const uint4 r = rec[p];
@@ -1132,13 +1139,15 @@ __device__ __forceinline__ void als_accumulate(const uint4 *__restrict__ rec,
             for (int c = 0; c < C; ++c) hc[c] = 0;
         }
 #pragma unroll
-        for (int c = 0; c < C; ++c) b[c] += wx * hc[c];
+        for (int c = 0; c < C; ++c) {
+            b[c] += wx * hc[c];
+            hw[c] = wn * hc[c];  // the multiplicity folded into the lane's own columns
+        }
 #pragma unroll
         for (int a = 0; a < R; ++a) {
             const T ha = __shfl_sync(0xffffffffu, hc[a / L], g * L + (a % L));
-            const T wa = wn * ha;
 #pragma unroll
-            for (int c = 0; c < C; ++c) G[a][c] += wa * hc[c];
+            for (int c = 0; c < C; ++c) G[a][c] += ha * hw[c];
         }
     }
     if constexpr (NG > 1) {
