@@ -65,6 +65,12 @@ class Result(C.Structure):
                 ("nonspd_rows", C.c_uint64)]
 
 
+class TuneTrial(C.Structure):
+    _fields_ = [("tile_len", C.c_int), ("threads_per_row", C.c_int), ("smem_budget", C.c_int),
+                ("ms_epoch", C.c_double), ("cached", C.c_int)]
+
+
+TUNE_FORCE, TUNE_NO_WRITE = 1, 2
 EPOCH_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(EpochStats))
 BATCH_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                        C.c_double)
@@ -127,6 +133,10 @@ def lib():
             "ctc_batch_create": (C.c_int, [P, C.c_int, C.POINTER(P), C.POINTER(P), C.POINTER(Params),
                                            C.POINTER(P)]),
             "ctc_batch_free": (C.c_int, [P]),
+            "ctc_autotune": (C.c_int, [P, C.POINTER(P), C.POINTER(Params), C.c_char_p, C.c_int, C.POINTER(Params),
+                                       C.POINTER(TuneTrial), C.c_int, C.POINTER(C.c_int)]),
+            "ctc_tune_lookup": (C.c_int, [C.c_char_p, P, C.POINTER(Params), C.c_int, C.POINTER(Params)]),
+            "ctc_tune_key": (C.c_int, [P, C.POINTER(Params), C.c_int, C.c_char_p, C.c_int]),
             "ctc_batch_info": (C.c_int, [P, C.POINTER(C.c_int), _u64p, _u64p]),
             "ctc_batch_run": (C.c_int, [P, C.POINTER(P), C.POINTER(Params), BATCH_CB, P, C.POINTER(Result)]),
         }
@@ -581,3 +591,32 @@ class Batch:
             self.free()
         except Exception:
             pass
+
+
+def autotune(ctx: Context, train, p: Params, cache_path: str | None = None, force: bool = False,
+             write: bool = True):
+    """ctc_autotune: tuned copy of `p` for the shape of train[0] and the
+    list of timed trials (dicts)."""
+    out = Params()
+    trials = (TuneTrial * 64)()
+    n = C.c_int()
+    flags = (TUNE_FORCE if force else 0) | (0 if write else TUNE_NO_WRITE)
+    _check(lib().ctc_autotune(ctx.h, _train_ptrs(train), C.byref(p), cache_path.encode() if cache_path else None,
+                              flags, C.byref(out), trials, 64, C.byref(n)))
+    return out, [{k: getattr(trials[i], k) for k, _ in TuneTrial._fields_} for i in range(min(n.value, 64))]
+
+
+def tune_lookup(cache_path: str, train: Tensor, p: Params, sm_count: int = 148):
+    """The cached tuned parameters for this shape, or None."""
+    out = Params()
+    rc = lib().ctc_tune_lookup(cache_path.encode(), train.h, C.byref(p), sm_count, C.byref(out))
+    if rc == -9:
+        return None
+    _check(rc)
+    return out
+
+
+def tune_key(train: Tensor, p: Params, sm_count: int = 148) -> str:
+    buf = C.create_string_buffer(512)
+    _check(lib().ctc_tune_key(train.h, C.byref(p), sm_count, buf, 512))
+    return buf.value.decode()

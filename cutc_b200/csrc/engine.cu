@@ -1768,3 +1768,228 @@ extern "C" int ctc_batch_run(ctc_batch *B, ctc_model *const *models, const ctc_p
         }
     });
 }
+
+// ---------------------------------------------------------------------
+// Autotuner: per tensor shape, the tile length (all algorithms), the lanes
+// per nonzero (SGD) and the shared-memory staging budget (CCD++) are
+// searched by timing update epochs on the device, and the winner is cached
+// in a text file -- this project's replacement for the reference's offline
+// genetic search over tile length and block size (ga/, fitness.c:67-79).
+// ---------------------------------------------------------------------
+namespace ctc {
+
+struct TuneCand {
+    int tile_len = 0, threads_per_row = 0, smem_budget = 0;
+};
+
+// shape key: algorithm, precision, rank, compat, SGD order, dimensions and
+// nonzeros rounded to half powers of two, and the device's SM count
+static std::string tune_key(const ctc_params &p, const uint64_t dims[3], uint64_t nnz, int sms)
+{
+    auto b = [](uint64_t x) { return (long)std::lround(2.0 * std::log2((double)std::max<uint64_t>(x, 1))); };
+    char buf[256];
+    snprintf(buf, sizeof buf, "alg=%d,prec=%d,rank=%d,compat=%d,order=%d,I=%ld,J=%ld,K=%ld,nnz=%ld,sms=%d", p.alg,
+             p.precision, p.rank, p.compat, p.alg == CTC_ALG_SGD ? p.sgd_order : 0, b(dims[0]), b(dims[1]),
+             b(dims[2]), b(nnz), sms);
+    return buf;
+}
+
+// cache lines: "<key> tile_len=<t> threads_per_row=<c> smem_budget=<s> ms=<x>"
+static bool tune_read(const char *path, const std::string &key, TuneCand &c, double &ms)
+{
+    if (!path) return false;
+    FILE *f = fopen(path, "r");
+    if (!f) return false;
+    char line[512];
+    bool found = false;
+    while (fgets(line, sizeof line, f)) {
+        char k[300];
+        TuneCand t;
+        double x = 0;
+        if (sscanf(line, "%299s tile_len=%d threads_per_row=%d smem_budget=%d ms=%lf", k, &t.tile_len,
+                   &t.threads_per_row, &t.smem_budget, &x) == 5 &&
+            key == k) {
+            c = t;  // the last entry for a key wins
+            ms = x;
+            found = true;
+        }
+    }
+    fclose(f);
+    return found;
+}
+
+static void tune_write(const char *path, const std::string &key, const TuneCand &c, double ms)
+{
+    if (!path) return;
+    std::vector<std::string> keep;
+    if (FILE *f = fopen(path, "r")) {
+        char line[512];
+        while (fgets(line, sizeof line, f)) {
+            char k[300];
+            if (sscanf(line, "%299s", k) == 1 && key == k) continue;
+            keep.emplace_back(line);
+        }
+        fclose(f);
+    }
+    FILE *f = fopen(path, "w");
+    if (!f) fail(CTC_E_IO, "cannot write the tuning cache %s", path);
+    for (const std::string &l : keep) fputs(l.c_str(), f);
+    fprintf(f, "%s tile_len=%d threads_per_row=%d smem_budget=%d ms=%.6f\n", key.c_str(), c.tile_len,
+            c.threads_per_row, c.smem_budget, ms);
+    fclose(f);
+}
+
+static std::vector<TuneCand> tune_space(const ctc_params &p)
+{
+    std::vector<TuneCand> v;
+    auto add = [&](int t, int c, int s) {
+        TuneCand x;
+        x.tile_len = t;
+        x.threads_per_row = c;
+        x.smem_budget = s;
+        v.push_back(x);
+    };
+    switch (p.alg) {
+    case CTC_ALG_ALS:
+        for (int t : {256, 512, 1024, 2048}) add(t, 0, 0);
+        break;
+    case CTC_ALG_CCD:
+        if (p.compat) add(32, 0, 0);  // the reference multiplicities need 32-long tiles
+        else
+            for (int t : {256, 512, 1024}) add(t, 0, 0);
+        break;
+    case CTC_ALG_CCDPP:
+        for (int t : {128, 256, 512})
+            for (int s : {0, -1}) add(t, 0, s);
+        break;
+    case CTC_ALG_SGD: {
+        const int base = p.rank / (p.precision == CTC_PREC_F64 ? 2 : 4);  // lanes at one vector each
+        if (p.sgd_order == CTC_SGD_SEQUENTIAL) {
+            add(p.tile_len, 0, 0);
+            break;
+        }
+        for (int t : {128, 256, 512, 1024})
+            for (int c : {base, base / 2, base / 4})
+                if (c >= 1) add(t, c, 0);
+        break;
+    }
+    }
+    return v;
+}
+
+static int device_sms(int dev)
+{
+    int n = 0;
+    CK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    return n;
+}
+
+}  // namespace ctc
+
+extern "C" int ctc_tune_key(const ctc_tensor *train, const ctc_params *p, int sm_count, char *buf, int len)
+{
+    return guarded([&] {
+        if (!train || !p || !buf || len <= 0) fail(CTC_E_ARG, "null argument");
+        const std::string key = tune_key(*p, train->dims, train->nnz, sm_count);
+        if ((int)key.size() >= len) fail(CTC_E_ARG, "buffer of %d bytes is too small", len);
+        memcpy(buf, key.c_str(), key.size() + 1);
+    });
+}
+
+extern "C" int ctc_tune_lookup(const char *cache_path, const ctc_tensor *train, const ctc_params *p, int sm_count,
+                               ctc_params *out)
+{
+    return guarded([&] {
+        if (!cache_path || !train || !p || !out) fail(CTC_E_ARG, "null argument");
+        const std::string key = tune_key(*p, train->dims, train->nnz, sm_count);
+        TuneCand c;
+        double ms = 0;
+        if (!tune_read(cache_path, key, c, ms)) fail(CTC_E_NOTFOUND, "no tuned entry for %s", key.c_str());
+        *out = *p;
+        out->tile_len = c.tile_len;
+        out->threads_per_row = c.threads_per_row;
+        out->smem_budget = c.smem_budget;
+    });
+}
+
+extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], const ctc_params *p,
+                            const char *cache_path, int flags, ctc_params *out, ctc_tune_trial *trials,
+                            int max_trials, int *ntrials)
+{
+    return guarded([&] {
+        if (!ctx || !train || !train[0] || !p || !out) fail(CTC_E_ARG, "null argument");
+        check_params(p);
+        CK(cudaSetDevice(ctx->device));
+        const int sms = device_sms(ctx->device);
+        const std::string key = tune_key(*p, train[0]->dims, train[0]->nnz, sms);
+        *out = *p;
+        int nt = 0;
+        TuneCand best;
+        double best_ms = 0;
+        if (!(flags & CTC_TUNE_FORCE) && tune_read(cache_path, key, best, best_ms)) {
+            if (trials && max_trials > 0) {
+                trials[0] = ctc_tune_trial{best.tile_len, best.threads_per_row, best.smem_budget, best_ms, 1};
+                nt = 1;
+            }
+        } else {
+            const std::vector<TuneCand> space = tune_space(*p);
+            best_ms = 1e300;
+            std::vector<int> tiles;
+            for (const TuneCand &c : space)
+                if (std::find(tiles.begin(), tiles.end(), c.tile_len) == tiles.end()) tiles.push_back(c.tile_len);
+            for (int tl : tiles) {
+                // one staging per tile length; the other knobs are run-time
+                ctc_params q = *p;
+                q.tile_len = tl;
+                q.early_stop = 0;
+                q.use_graph = 0;
+                auto ds = std::make_unique<ctc_dataset>();
+                ds->ctx = ctx;
+                ds->p = q;
+                for (int m = 0; m < 3; ++m) ds->dims[m] = train[0]->dims[m];
+                ds->nnz_train = train[0]->nnz;
+                if (q.precision == CTC_PREC_F64) build_dataset<double>(ds.get(), train, nullptr, nullptr);
+                else build_dataset<float>(ds.get(), train, nullptr, nullptr);
+                ctc_model mdl;
+                mdl.nmodes = 3;
+                mdl.rank = q.rank;
+                for (int m = 0; m < 3; ++m) {
+                    mdl.dims[m] = ds->dims[m];
+                    mdl.U[m].resize(mdl.dims[m] * (uint64_t)q.rank);
+                }
+                if (ctc_model_init_uniform(&mdl, 12345, 1.0 / std::sqrt((double)q.rank)) != CTC_OK)
+                    fail(CTC_E_ARG, "%s", ctc_last_error());
+                SessionBase *S = session_for(ds.get(), q.rank);
+                for (const TuneCand &c : space) {
+                    if (c.tile_len != tl) continue;
+                    q.threads_per_row = c.threads_per_row;
+                    q.smem_budget = c.smem_budget;
+                    ds->p = q;
+                    S->set_params(q);
+                    S->set_model(&mdl);
+                    S->epochs(1);  // warm-up
+                    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+                    S->epochs(2);
+                    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+                    CK(cudaEventSynchronize(ctx->ev1));
+                    float ms = 0;
+                    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+                    const double per = ms / 2.0;
+                    if (trials && nt < max_trials)
+                        trials[nt] = ctc_tune_trial{c.tile_len, c.threads_per_row, c.smem_budget, per, 0};
+                    ++nt;
+                    if (per < best_ms) {
+                        best_ms = per;
+                        best = c;
+                    }
+                }
+                ds.reset();
+            }
+            if (!(flags & CTC_TUNE_NO_WRITE)) tune_write(cache_path, key, best, best_ms);
+        }
+        out->tile_len = best.tile_len;
+        out->threads_per_row = best.threads_per_row;
+        out->smem_budget = best.smem_budget;
+        if (ntrials) *ntrials = nt;
+    });
+}

@@ -37,6 +37,7 @@ extern "C" {
 #define CTC_E_NUMERIC (-6)  /* non-finite result                          */
 #define CTC_E_TIMEOUT (-7)  /* bounded device wait expired                */
 #define CTC_E_NOGPU (-8)    /* no CUDA device                             */
+#define CTC_E_NOTFOUND (-9) /* no entry (tuning cache lookup)             */
 
 typedef struct ctc_ctx ctc_ctx;
 typedef struct ctc_tensor ctc_tensor;
@@ -281,6 +282,35 @@ typedef int (*ctc_batch_cb)(void *user, int epoch, int ninst, const double *rmse
  * error.  res (may be NULL): totals over all instances. */
 int ctc_batch_run(ctc_batch *b, ctc_model *const *models, const ctc_params *p, ctc_batch_cb cb,
                   void *user, ctc_result *res);
+
+/* Autotuner (replaces the reference's offline genetic search over tile
+ * length and threads per block, ga/ciss.c:69-75, ga/sgd.cu:66-78,
+ * fitness.c:67-79).  For the shape of train[0] (dims, nonzeros, rounded to
+ * half powers of two), the algorithm, precision and rank of `p` and this
+ * device's SM count, it times update epochs over a candidate set: tile
+ * length (ALS, CCD, CCD++, SGD), lanes per nonzero (SGD threads_per_row),
+ * CCD++ column staging on/off (smem_budget), and writes the fastest into
+ * `out` (a copy of `p` with those fields replaced).  With cache_path, a
+ * cached entry for the shape is returned without a search (unless
+ * CTC_TUNE_FORCE), and a search stores its winner there (unless
+ * CTC_TUNE_NO_WRITE).  trials (may be NULL) receives up to max_trials
+ * timings; ntrials the number run (1 with cached = 1 on a cache hit). */
+#define CTC_TUNE_FORCE 1
+#define CTC_TUNE_NO_WRITE 2
+typedef struct {
+    int tile_len, threads_per_row, smem_budget;
+    double ms_epoch;   /* device time of one update epoch */
+    int cached;
+} ctc_tune_trial;
+int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], const ctc_params *p,
+                 const char *cache_path, int flags, ctc_params *out, ctc_tune_trial *trials,
+                 int max_trials, int *ntrials);
+/* The cached entry for the shape of `train` on a device with sm_count SMs,
+ * without a device: CTC_E_NOTFOUND when there is none. */
+int ctc_tune_lookup(const char *cache_path, const ctc_tensor *train, const ctc_params *p, int sm_count,
+                    ctc_params *out);
+/* The cache key of that shape (NUL-terminated, at most len bytes). */
+int ctc_tune_key(const ctc_tensor *train, const ctc_params *p, int sm_count, char *buf, int len);
 
 /* Per-kernel device time: with profiling on, every launch of this library
  * on the context is bracketed by a CUDA event pair; kernel_time sums the

@@ -1,0 +1,43 @@
+"""Autotuner cache (host only): shape keys and lookups of tuned entries."""
+from __future__ import annotations
+
+import numpy as np
+
+import cutc_b200 as ctc
+from cutc_b200 import synth
+
+
+def _tensor(nnz, dims, seed=0):
+    ind, vals = synth.random_small(nnz, dims, seed=seed)
+    return ctc.Tensor.from_coo(ind, vals, dims=dims)
+
+
+def test_key_buckets_shapes():
+    p = ctc.params(ctc.SGD, rank=16)
+    k1 = ctc.tune_key(_tensor(1000, (50, 40, 30)), p)
+    k2 = ctc.tune_key(_tensor(1010, (50, 40, 30), seed=1), p)
+    k3 = ctc.tune_key(_tensor(2000, (50, 40, 30)), p)
+    assert k1 == k2            # same half-power-of-two bucket
+    assert k1 != k3            # twice the nonzeros: another shape
+    assert "alg=1" in k1 and "rank=16" in k1 and "sms=148" in k1
+    assert ctc.tune_key(_tensor(1000, (50, 40, 30)), p, sm_count=132) != k1
+    assert ctc.tune_key(_tensor(1000, (50, 40, 30)), ctc.params(ctc.ALS, rank=16)) != k1
+
+
+def test_lookup_hit_miss_and_last_entry_wins(tmp_path):
+    t = _tensor(3000, (60, 50, 40))
+    p = ctc.params(ctc.CCDPP, rank=32)
+    path = str(tmp_path / "tune.txt")
+    assert ctc.tune_lookup(str(tmp_path / "missing.txt"), t, p) is None
+    key = ctc.tune_key(t, p)
+    with open(path, "w") as f:
+        f.write("garbage line\n")
+        f.write("alg=9,other 1 2 3\n")
+        f.write(f"{key} tile_len=128 threads_per_row=0 smem_budget=-1 ms=1.5\n")
+        f.write(f"{key} tile_len=512 threads_per_row=0 smem_budget=0 ms=1.2\n")
+    q = ctc.tune_lookup(path, t, p)
+    assert q is not None
+    assert (q.tile_len, q.threads_per_row, q.smem_budget) == (512, 0, 0)
+    # everything else is the caller's
+    assert q.rank == 32 and q.alg == ctc.CCDPP and abs(q.lambda_ - p.lambda_) == 0
+    assert ctc.tune_lookup(path, t, ctc.params(ctc.CCDPP, rank=16)) is None
