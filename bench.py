@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--ccdpp-tile", type=int, default=0, help="CCD++ tile length (0 = library default)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 256-instance leg")
     ap.add_argument("--instances", type=int, default=0, help="batch workloads: a K-instance sample of the same distribution")
+    ap.add_argument("--tune-cache", default="", help="autotuner cache file (default: a fresh temporary one)")
+    ap.add_argument("--no-tune", action="store_true", help="library defaults instead of autotuned parameters")
     return ap.parse_args()
 
 
@@ -232,6 +234,19 @@ def run_ours(args):
                        **{"lambda": 0.1})
     p_sgd = ctc.params("sgd", rank=R, lr=1e-3, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY, lr_decay=0.95,
                        early_stop=0, iters=20, **{"lambda": 0.01})
+    # autotuned tile length / lanes per nonzero / column staging for this
+    # shape (the library defaults are among the candidates: their epoch
+    # times are reported as the plain form)
+    tuned = None
+    if not args.no_tune and not args.ccdpp_tile:
+        import tempfile
+        cache = args.tune_cache or os.path.join(tempfile.mkdtemp(), "tune.txt")
+        t0 = time.time()
+        p_ccd, tr_ccd = ctc.autotune(ctx, tr, p_ccd, cache_path=cache)
+        p_sgd, tr_sgd = ctc.autotune(ctx, [tr[0]], p_sgd, cache_path=cache)
+        tuned = {"search_s": time.time() - t0, "cache_hit": bool(tr_ccd and tr_ccd[0]["cached"]),
+                 "ccdpp": {"tile_len": p_ccd.tile_len, "smem_budget": p_ccd.smem_budget, "trials": tr_ccd},
+                 "sgd": {"tile_len": p_sgd.tile_len, "threads_per_row": p_sgd.threads_per_row, "trials": tr_sgd}}
     ds_ccd = ctc.Dataset(ctx, tr, None, te, p_ccd)
     ds_sgd = ctc.Dataset(ctx, [tr[0]], None, te, p_sgd)
     mdims = ds_ccd.dims()
@@ -323,6 +338,7 @@ def run_ours(args):
                        "frac_hbm": sgd_bytes / (sgd_avg_ms / 1000.0) / 1e9 / peak},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "tuned": tuned,
     }
 
     if rank == 0 and not args.no_extras:

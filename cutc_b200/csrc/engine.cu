@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -96,6 +97,29 @@ static void with_rank(int R, F &&f)
 constexpr int kSMs = 148;
 constexpr int kMaxPartials = kSMs * 8;
 constexpr int kScalars = 16;
+
+// CTC_TRACE=1 in the environment prints the host staging phases' wall
+// times to stderr
+static bool trace_on()
+{
+    static const bool on = [] {
+        const char *e = getenv("CTC_TRACE");
+        return e && *e && *e != '0';
+    }();
+    return on;
+}
+
+struct TracePhase {
+    const char *what;
+    std::chrono::steady_clock::time_point t0;
+    explicit TracePhase(const char *w) : what(w), t0(std::chrono::steady_clock::now()) {}
+    ~TracePhase()
+    {
+        if (trace_on())
+            fprintf(stderr, "[ctc] %-28s %8.3f s\n", what,
+                    std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+    }
+};
 
 static unsigned grid_for(uint64_t work, unsigned per_block, unsigned cap)
 {
@@ -231,8 +255,14 @@ static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t 
     const uint64_t ntiles = plan.ntiles();
     const uint64_t nslots = ntiles * S;
     if (nslots >= 0xfffffff0ull) fail(CTC_E_UNSUP, "CCD++: more than 2^32 slot entries");
-    std::vector<uint64_t> keys(nslots, k::kPadKey);
-    std::vector<T> x(nslots, T(0));
+    // (uninitialised buffers, filled in parallel: a zero-initialised vector
+    // would first clear them on one thread)
+    std::unique_ptr<uint64_t[]> keys(new uint64_t[nslots]);
+    std::unique_ptr<T[]> x(new T[nslots]);
+    par_for(nslots, [&](uint64_t b, uint64_t e) {
+        std::fill(keys.get() + b, keys.get() + e, k::kPadKey);
+        std::fill(x.get() + b, x.get() + e, T(0));
+    });
     const uint32_t s_row = d.ks.s_row, s_q1 = d.ks.s_q1;
     par_for(ntiles, [&](uint64_t tb, uint64_t te) {
         for (uint64_t tt = tb; tt < te; ++tt) {
@@ -272,8 +302,8 @@ static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t 
     d.heavy.upload(reinterpret_cast<const uint4 *>(hv.data()), hv.size() / 4, ctx->stream);
     d.n = (uint32_t)t->nnz;
     d.nslots = (uint32_t)nslots;
-    d.keys.upload(keys.data(), nslots, ctx->stream);
-    d.x.upload(x.data(), nslots, ctx->stream);
+    d.keys.upload(keys.get(), nslots, ctx->stream);
+    d.x.upload(x.get(), nslots, ctx->stream);
     d.res.alloc(nslots);
     CK(cudaMemsetAsync(d.res.p, 0, nslots * sizeof(T), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -312,7 +342,7 @@ template <typename T>
 static void stage_tensor(ctc_ctx *ctx, const ctc_tensor *t, bool trunc, DevTensor<T> &d)
 {
     const uint64_t n = t->nnz;
-    std::vector<uint4> rec(n);
+    std::unique_ptr<uint4[]> rec(new uint4[std::max<uint64_t>(n, 1)]);  // filled below, in parallel
     std::vector<double> v64(std::is_same<T, double>::value ? n : 0);
     par_for(n, [&](uint64_t b, uint64_t e) {
         for (uint64_t i = b; i < e; ++i) {
@@ -327,7 +357,7 @@ static void stage_tensor(ctc_ctx *ctx, const ctc_tensor *t, bool trunc, DevTenso
         }
     });
     d.n = (uint32_t)n;
-    d.rec.upload(rec.data(), n, ctx->stream);
+    d.rec.upload(rec.get(), n, ctx->stream);
     if (!v64.empty()) d.v64.upload(v64.data(), n, ctx->stream);
     CK(cudaStreamSynchronize(ctx->stream));
 }
@@ -340,9 +370,15 @@ static TilePlan stage_plan(ctc_ctx *ctx, const ctc_tensor *t, int mode, uint32_t
     par_for(n, [&](uint64_t b, uint64_t e) {
         for (uint64_t i = b; i < e; ++i) rows[i] = (uint32_t)(t->ind[mode][i] - 1);
     });
-    for (uint64_t i = 1; i < n; ++i)
-        if (rows[i] < rows[i - 1])
-            fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", mode + 1, mode + 1);
+    std::atomic<int> unsorted{0};
+    par_for(n > 0 ? n - 1 : 0, [&](uint64_t b, uint64_t e) {
+        for (uint64_t i = b + 1; i <= e; ++i)
+            if (rows[i] < rows[i - 1]) {
+                unsorted = 1;
+                return;
+            }
+    });
+    if (unsorted) fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", mode + 1, mode + 1);
     if (n >= 0x7fffffffull) fail(CTC_E_UNSUP, "tile plans index at most 2^31 - 1 nonzeros");
     TilePlan p = plan_tiles(rows.data(), n, tile_len);
     d.mode = mode;
@@ -450,12 +486,24 @@ static void build_dataset(ctc_dataset *ds, const ctc_tensor *const train[3], con
             srt[m] = own[m].get();
         }
         if (srt[m]->nnz != train[0]->nnz) fail(CTC_E_ARG, "training copies differ in size");
-        validate_tensor(srt[m], ds->dims, "training tensor");
+        {
+            TracePhase tp("validate training copy");
+            validate_tensor(srt[m], ds->dims, "training tensor");
+        }
         if (p.alg == CTC_ALG_CCDPP) {
-            const TilePlan plan = stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
+            TilePlan plan;
+            {
+                TracePhase tp("tile plan");
+                plan = stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
+            }
+            TracePhase tp("CCD++ slots + upload");
             stage_keys<T>(ctx, srt[m], m, ds->dims, trunc, plan, (int)(tl / 32), impl->copy[m]);
         } else {
-            stage_tensor<T>(ctx, srt[m], trunc, impl->copy[m]);
+            {
+                TracePhase tp("records + upload");
+                stage_tensor<T>(ctx, srt[m], trunc, impl->copy[m]);
+            }
+            TracePhase tp("tile plan");
             if (p.alg != CTC_ALG_SGD) stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
         }
         if (trunc && (p.alg == CTC_ALG_ALS || p.alg == CTC_ALG_CCD))
@@ -465,17 +513,35 @@ static void build_dataset(ctc_dataset *ds, const ctc_tensor *const train[3], con
         // SGD tiles are plain chunks of the mode-1 order (sgpu/sgd.cu:32-34)
         impl->copy[0].mode = 0;
         impl->copy[0].ntiles = (uint32_t)((impl->copy[0].n + tl - 1) / tl);
+        TracePhase tp("SGD row counts");
         for (int m = 0; m < 3; ++m) {
-            impl->rowcnt[m].assign(ds->dims[m], 0);
+            // per-thread histograms, summed
+            const uint64_t d = ds->dims[m];
             const uint64_t *ind = srt[0]->ind[m].data();
-            for (uint64_t i = 0; i < srt[0]->nnz; ++i) impl->rowcnt[m][ind[i] - 1]++;
+            const int P = std::max(1, std::min(host_threads(), 64));
+            std::vector<std::vector<uint32_t>> part(P);
+            std::vector<std::thread> th;
+            for (int q = 0; q < P; ++q)
+                th.emplace_back([&, q] {
+                    part[q].assign(d, 0);
+                    const uint64_t b = srt[0]->nnz * q / P, e = srt[0]->nnz * (q + 1) / P;
+                    for (uint64_t i = b; i < e; ++i) part[q][ind[i] - 1]++;
+                });
+            for (auto &t : th) t.join();
+            impl->rowcnt[m].assign(d, 0);
+            par_for(d, [&](uint64_t b, uint64_t e) {
+                for (int q = 0; q < P; ++q)
+                    for (uint64_t r = b; r < e; ++r) impl->rowcnt[m][r] += part[q][r];
+            });
         }
     }
     if (val) {
+        TracePhase tp("validation tensor");
         validate_tensor(val, ds->dims, "validation tensor");
         stage_tensor<T>(ctx, val, false, impl->val);
     }
     if (test) {
+        TracePhase tp("test tensor");
         validate_tensor(test, ds->dims, "test tensor");
         stage_tensor<T>(ctx, test, false, impl->test);
     }
