@@ -53,6 +53,7 @@ struct TilePlan {
     uint32_t nheavy() const { return (uint32_t)(heavy_rows.size() / 4); }
 };
 TilePlan plan_tiles(const uint32_t *rows, uint64_t n, uint32_t tile_len);
+TilePlan plan_tiles_chunked(const uint32_t *rows, uint64_t n, uint32_t tile_len);
 
 // Reference warp-kernel multiplicity of each nonzero (see ciss.cpp).
 void compat_weights(const ctc_ciss &c, int kernel, std::vector<double> &w);

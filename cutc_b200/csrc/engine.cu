@@ -151,9 +151,38 @@ struct ctc_ctx {
     double *h_scalars = nullptr;  // pinned mirror
     bool capturing = false;
     KernelTimes kt;
+    // pinned double buffer for host-to-device staging (first use allocates)
+    unsigned char *pin[2] = {nullptr, nullptr};
+    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
 };
 
 namespace ctc {
+
+// Host-to-device staging through the context's pinned double buffer:
+// fill(b, e, h) writes elements [b, e) of the device array to h (pinned
+// host memory, element b at h[0]); the copy of one chunk runs while the
+// next one is filled on the host threads.
+constexpr size_t kPinBytes = (size_t)32 << 20;
+
+template <typename E, typename F>
+static void upload_filled(ctc_ctx *ctx, E *dev, uint64_t n, F &&fill)
+{
+    if (!ctx->pin[0])
+        for (int q = 0; q < 2; ++q) {
+            CK(cudaMallocHost(&ctx->pin[q], kPinBytes));
+            CK(cudaEventCreateWithFlags(&ctx->pin_ev[q], cudaEventDisableTiming));
+        }
+    const uint64_t per = kPinBytes / sizeof(E);
+    int q = 0;
+    for (uint64_t b = 0; b < n; b += per, q ^= 1) {
+        const uint64_t e = std::min(n, b + per);
+        CK(cudaEventSynchronize(ctx->pin_ev[q]));  // this buffer's previous copy is done
+        E *h = reinterpret_cast<E *>(ctx->pin[q]);
+        par_for(e - b, [&](uint64_t i0, uint64_t i1) { fill(b + i0, b + i1, h + i0); });
+        CK(cudaMemcpyAsync(dev + b, h, (e - b) * sizeof(E), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaEventRecord(ctx->pin_ev[q], ctx->stream));
+    }
+}
 
 static void kt_flush(ctc_ctx *ctx)
 {
@@ -255,24 +284,29 @@ static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t 
     const uint64_t ntiles = plan.ntiles();
     const uint64_t nslots = ntiles * S;
     if (nslots >= 0xfffffff0ull) fail(CTC_E_UNSUP, "CCD++: more than 2^32 slot entries");
-    // (uninitialised buffers, filled in parallel: a zero-initialised vector
-    // would first clear them on one thread)
-    std::unique_ptr<uint64_t[]> keys(new uint64_t[nslots]);
-    std::unique_ptr<T[]> x(new T[nslots]);
-    par_for(nslots, [&](uint64_t b, uint64_t e) {
-        std::fill(keys.get() + b, keys.get() + e, k::kPadKey);
-        std::fill(x.get() + b, x.get() + e, T(0));
-    });
     const uint32_t s_row = d.ks.s_row, s_q1 = d.ks.s_q1;
-    par_for(ntiles, [&](uint64_t tb, uint64_t te) {
-        for (uint64_t tt = tb; tt < te; ++tt) {
-            const uint64_t start = (uint64_t)plan.tiles[4 * tt], len = (uint64_t)plan.tiles[4 * tt + 1];
-            for (uint64_t q = 0; q < len; ++q) {
-                const uint64_t i = start + q, dst = tt * S + (q % E) * 32 + q / E;
-                keys[dst] = ((t->ind[m][i] - 1) << s_row) | ((t->ind[m1][i] - 1) << s_q1) | (t->ind[m2][i] - 1);
-                const double v = trunc ? ctc_value_through_idx(t->vals[i]) : t->vals[i];
-                x[dst] = (T)v;
-            }
+    const uint64_t *im = t->ind[m].data(), *im1 = t->ind[m1].data(), *im2 = t->ind[m2].data();
+    const double *vals = t->vals.data();
+    // slot s: tile s / S, lane (s % S) % 32, step (s % S) / 32, i.e. entry
+    // lane * E + step of the tile (or a pad past its length)
+    auto source = [&](uint64_t sidx) -> int64_t {
+        const uint64_t tt = sidx / S, o = sidx % S;
+        const uint64_t q = (o % 32) * (uint64_t)E + o / 32;
+        if (q >= (uint64_t)plan.tiles[4 * tt + 1]) return -1;
+        return (int64_t)((uint64_t)plan.tiles[4 * tt] + q);
+    };
+    d.keys.alloc(nslots);
+    upload_filled(ctx, d.keys.p, nslots, [&](uint64_t b, uint64_t e, uint64_t *h) {
+        for (uint64_t sidx = b; sidx < e; ++sidx) {
+            const int64_t i = source(sidx);
+            h[sidx - b] = i < 0 ? k::kPadKey : ((im[i] - 1) << s_row) | ((im1[i] - 1) << s_q1) | (im2[i] - 1);
+        }
+    });
+    d.x.alloc(nslots);
+    upload_filled(ctx, d.x.p, nslots, [&](uint64_t b, uint64_t e, T *h) {
+        for (uint64_t sidx = b; sidx < e; ++sidx) {
+            const int64_t i = source(sidx);
+            h[sidx - b] = i < 0 ? T(0) : (T)(trunc ? ctc_value_through_idx(vals[i]) : vals[i]);
         }
     });
     // warp tasks: a light tile, or up to kCcdppGroup consecutive pieces of a
@@ -302,8 +336,6 @@ static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t 
     d.heavy.upload(reinterpret_cast<const uint4 *>(hv.data()), hv.size() / 4, ctx->stream);
     d.n = (uint32_t)t->nnz;
     d.nslots = (uint32_t)nslots;
-    d.keys.upload(keys.get(), nslots, ctx->stream);
-    d.x.upload(x.get(), nslots, ctx->stream);
     d.res.alloc(nslots);
     CK(cudaMemsetAsync(d.res.p, 0, nslots * sizeof(T), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -342,23 +374,26 @@ template <typename T>
 static void stage_tensor(ctc_ctx *ctx, const ctc_tensor *t, bool trunc, DevTensor<T> &d)
 {
     const uint64_t n = t->nnz;
-    std::unique_ptr<uint4[]> rec(new uint4[std::max<uint64_t>(n, 1)]);  // filled below, in parallel
-    std::vector<double> v64(std::is_same<T, double>::value ? n : 0);
-    par_for(n, [&](uint64_t b, uint64_t e) {
+    d.n = (uint32_t)n;
+    d.rec.alloc(n);
+    const uint64_t *i0 = t->ind[0].data(), *i1 = t->ind[1].data(), *i2 = t->ind[2].data();
+    const double *vals = t->vals.data();
+    upload_filled(ctx, d.rec.p, n, [&](uint64_t b, uint64_t e, uint4 *h) {
         for (uint64_t i = b; i < e; ++i) {
-            double v = t->vals[i];
+            double v = vals[i];
             if (trunc) v = ctc_value_through_idx(v);
-            float vf = (float)v;
+            const float vf = (float)v;
             uint32_t bits;
             memcpy(&bits, &vf, 4);
-            rec[i] = make_uint4((uint32_t)(t->ind[0][i] - 1), (uint32_t)(t->ind[1][i] - 1),
-                                (uint32_t)(t->ind[2][i] - 1), bits);
-            if (!v64.empty()) v64[i] = v;
+            h[i - b] = make_uint4((uint32_t)(i0[i] - 1), (uint32_t)(i1[i] - 1), (uint32_t)(i2[i] - 1), bits);
         }
     });
-    d.n = (uint32_t)n;
-    d.rec.upload(rec.get(), n, ctx->stream);
-    if (!v64.empty()) d.v64.upload(v64.data(), n, ctx->stream);
+    if (std::is_same<T, double>::value) {
+        d.v64.alloc(n);
+        upload_filled(ctx, d.v64.p, n, [&](uint64_t b, uint64_t e, double *h) {
+            for (uint64_t i = b; i < e; ++i) h[i - b] = trunc ? ctc_value_through_idx(vals[i]) : vals[i];
+        });
+    }
     CK(cudaStreamSynchronize(ctx->stream));
 }
 
@@ -366,7 +401,7 @@ template <typename T>
 static TilePlan stage_plan(ctc_ctx *ctx, const ctc_tensor *t, int mode, uint32_t tile_len, DevTensor<T> &d)
 {
     const uint64_t n = t->nnz;
-    std::vector<uint32_t> rows(n);
+    std::unique_ptr<uint32_t[]> rows(new uint32_t[std::max<uint64_t>(n, 1)]);  // filled in parallel
     par_for(n, [&](uint64_t b, uint64_t e) {
         for (uint64_t i = b; i < e; ++i) rows[i] = (uint32_t)(t->ind[mode][i] - 1);
     });
@@ -380,7 +415,7 @@ static TilePlan stage_plan(ctc_ctx *ctx, const ctc_tensor *t, int mode, uint32_t
     });
     if (unsorted) fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", mode + 1, mode + 1);
     if (n >= 0x7fffffffull) fail(CTC_E_UNSUP, "tile plans index at most 2^31 - 1 nonzeros");
-    TilePlan p = plan_tiles(rows.data(), n, tile_len);
+    TilePlan p = plan_tiles_chunked(rows.get(), n, tile_len);
     d.mode = mode;
     d.ntiles = p.ntiles();
     d.nheavy = p.nheavy();
@@ -1239,6 +1274,10 @@ extern "C" int ctc_ctx_destroy(ctc_ctx *ctx)
     ctx->partial.release();
     ctx->scalars.release();
     if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
+    for (int q = 0; q < 2; ++q) {
+        if (ctx->pin[q]) cudaFreeHost(ctx->pin[q]);
+        if (ctx->pin_ev[q]) cudaEventDestroy(ctx->pin_ev[q]);
+    }
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

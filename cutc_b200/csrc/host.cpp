@@ -406,6 +406,53 @@ TilePlan plan_tiles(const uint32_t *rows, uint64_t n, uint32_t T)
     return p;
 }
 
+// The same plan built over 64 row-aligned chunks in parallel (the chunk
+// count is fixed, so the plan does not depend on the host's core count);
+// light tiles do not straddle a chunk boundary.
+TilePlan plan_tiles_chunked(const uint32_t *rows, uint64_t n, uint32_t T)
+{
+    constexpr int K = 64;
+    if (n < ((uint64_t)1 << 20)) return plan_tiles(rows, n, T);
+    std::vector<uint64_t> cut(K + 1, 0);
+    cut[K] = n;
+    for (int c = 1; c < K; ++c) {
+        uint64_t x = std::max<uint64_t>(n * (uint64_t)c / K, cut[c - 1]);
+        while (x > 0 && x < n && rows[x] == rows[x - 1]) ++x;
+        cut[c] = x;
+    }
+    std::vector<TilePlan> part(K);
+    {
+        const int P = std::max(1, std::min(host_threads(), K));
+        std::vector<std::thread> th;
+        for (int q = 0; q < P; ++q)
+            th.emplace_back([&, q] {
+                for (int c = q; c < K; c += P) part[c] = plan_tiles(rows + cut[c], cut[c + 1] - cut[c], T);
+            });
+        for (auto &t : th) t.join();
+    }
+    TilePlan p;
+    size_t nt = 0, nh = 0;
+    for (const TilePlan &q : part) {
+        nt += q.tiles.size();
+        nh += q.heavy_rows.size();
+    }
+    p.tiles.reserve(nt);
+    p.heavy_rows.reserve(nh);
+    for (int c = 0; c < K; ++c) {
+        const uint32_t tbase = p.ntiles(), hbase = p.nheavy();
+        const TilePlan &q = part[c];
+        for (size_t t = 0; t < q.tiles.size(); t += 4) {
+            const int32_t h = q.tiles[t + 2];
+            p.tiles.insert(p.tiles.end(), {(int32_t)(q.tiles[t] + (int64_t)cut[c]), q.tiles[t + 1],
+                                           h >= 0 ? h + (int32_t)hbase : h, q.tiles[t + 3]});
+        }
+        for (size_t h = 0; h < q.heavy_rows.size(); h += 4)
+            p.heavy_rows.insert(p.heavy_rows.end(), {q.heavy_rows[h], q.heavy_rows[h + 1] + tbase,
+                                                     q.heavy_rows[h + 2], q.heavy_rows[h + 3]});
+    }
+    return p;
+}
+
 // counter-based uniform in [0,1): splitmix64 of (seed, mode, row, col)
 static inline double u01(uint64_t seed, uint64_t mode, uint64_t row, uint64_t col)
 {
