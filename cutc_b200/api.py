@@ -65,6 +65,12 @@ class Result(C.Structure):
                 ("nonspd_rows", C.c_uint64)]
 
 
+class FoParams(C.Structure):
+    _fields_ = [("rank", C.c_int), ("precision", C.c_int), ("lambda_", C.c_double), ("lr", C.c_double),
+                ("beta1", C.c_double), ("beta2", C.c_double), ("eps", C.c_double), ("batch", C.c_uint64),
+                ("epochs", C.c_int), ("seed", C.c_uint64), ("eval_every", C.c_int)]
+
+
 class TuneTrial(C.Structure):
     _fields_ = [("tile_len", C.c_int), ("threads_per_row", C.c_int), ("smem_budget", C.c_int),
                 ("ms_epoch", C.c_double), ("cached", C.c_int)]
@@ -137,6 +143,11 @@ def lib():
                                        C.POINTER(TuneTrial), C.c_int, C.POINTER(C.c_int)]),
             "ctc_tune_lookup": (C.c_int, [C.c_char_p, P, C.POINTER(Params), C.c_int, C.POINTER(Params)]),
             "ctc_tune_key": (C.c_int, [P, C.POINTER(Params), C.c_int, C.c_char_p, C.c_int]),
+            "ctc_fo_params_default": (C.c_int, [C.POINTER(FoParams)]),
+            "ctc_fo_create": (C.c_int, [P, P, P, C.POINTER(FoParams), C.POINTER(P)]),
+            "ctc_fo_free": (C.c_int, [P]),
+            "ctc_fo_dims": (C.c_int, [P, C.POINTER(C.c_int), _u64p]),
+            "ctc_fo_run": (C.c_int, [P, P, C.POINTER(FoParams), EPOCH_CB, P, C.POINTER(Result)]),
             "ctc_batch_info": (C.c_int, [P, C.POINTER(C.c_int), _u64p, _u64p]),
             "ctc_batch_run": (C.c_int, [P, C.POINTER(P), C.POINTER(Params), BATCH_CB, P, C.POINTER(Result)]),
         }
@@ -620,3 +631,59 @@ def tune_key(train: Tensor, p: Params, sm_count: int = 148) -> str:
     buf = C.create_string_buffer(512)
     _check(lib().ctc_tune_key(train.h, C.byref(p), sm_count, buf, 512))
     return buf.value.decode()
+
+
+def fo_params(**kw) -> FoParams:
+    """First-order (Adam) parameters: library defaults overridden by kw
+    ('lambda' is accepted for lambda_)."""
+    p = FoParams()
+    _check(lib().ctc_fo_params_default(C.byref(p)))
+    for k, v in kw.items():
+        if k == "lambda":
+            k = "lambda_"
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+class FirstOrder:
+    """Adjoint-driven full-gradient / minibatch Adam training (ctc_fo) of an
+    order-3 or order-4 tensor."""
+
+    def __init__(self, ctx: Context, train: Tensor, test: Tensor | None, p: FoParams):
+        h = C.c_void_p()
+        _check(lib().ctc_fo_create(ctx.h, train.h, test.h if test else None, C.byref(p), C.byref(h)))
+        self.h = h
+        self.ctx = ctx
+
+    def dims(self):
+        order = C.c_int()
+        d = (C.c_uint64 * 4)()
+        _check(lib().ctc_fo_dims(self.h, C.byref(order), d))
+        return [d[m] for m in range(order.value)]
+
+    def run(self, model: Model, p: FoParams, callback=None) -> RunOutput:
+        out = RunOutput(result={})
+
+        def _cb(_user, sp):
+            d = _stats_dict(sp.contents)
+            out.epochs.append(d)
+            return int(bool(callback(d))) if callback else 0
+
+        cb = EPOCH_CB(_cb)
+        res = Result()
+        _check(lib().ctc_fo_run(self.h, model.h, C.byref(p), cb, None, C.byref(res)))
+        out.result = _result_dict(res)
+        return out
+
+    def free(self):
+        if self.h:
+            lib().ctc_fo_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -101,7 +101,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // Gram + right-hand side of the heavy pieces listed in `pieces` (tile
 // indices of the mode's plan); slot[t] = {G (64 x 64 row-major), b (64)}.
 // err[0] is set when a bounded wait expires.
-__global__ void __launch_bounds__(kThreads, 2)
+static __global__ void __launch_bounds__(kThreads, 2)
     k_als_gram_tc(const int4 *__restrict__ tiles, const uint32_t *__restrict__ pieces, uint32_t npieces,
                   const uint4 *__restrict__ rec, int m, const __nv_bfloat16 *__restrict__ Ua,
                   const __nv_bfloat16 *__restrict__ Ub, float *__restrict__ slot, int *err)
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 }
 
 // FP32 factor rows -> BF16 copies (row-major, same shape)
-__global__ void k_to_bf16(const float *__restrict__ src, __nv_bfloat16 *__restrict__ dst, uint64_t n)
+static __global__ void k_to_bf16(const float *__restrict__ src, __nv_bfloat16 *__restrict__ dst, uint64_t n)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         dst[i] = __float2bfloat16_rn(src[i]);

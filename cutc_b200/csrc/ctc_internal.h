@@ -55,6 +55,10 @@ struct TilePlan {
 TilePlan plan_tiles(const uint32_t *rows, uint64_t n, uint32_t tile_len);
 TilePlan plan_tiles_chunked(const uint32_t *rows, uint64_t n, uint32_t tile_len);
 
+// FP64 gradient of the masked CP loss for order-3/4 tensors (fo.cu)
+void ctc_grad_fo(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double lambda, double *const *grads,
+                 double *obj);
+
 // Reference warp-kernel multiplicity of each nonzero (see ciss.cpp).
 void compat_weights(const ctc_ciss &c, int kernel, std::vector<double> &w);
 

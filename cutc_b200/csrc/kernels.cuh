@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(256) k_sse_chunks(const uint4 *__restrict__ re
 
 // out[i] = sum of partial[first[i] .. first[i+1]) in order (thread per
 // instance)
-__global__ void k_fold_segments(const double *__restrict__ partial, const uint32_t *__restrict__ first, int ninst,
+static __global__ void k_fold_segments(const double *__restrict__ partial, const uint32_t *__restrict__ first, int ninst,
                                 double *__restrict__ out)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ninst; i += gridDim.x * blockDim.x) {
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(256) k_sumsq(const T *__restrict__ x, uint64_t
 }
 
 // out[slot] = sum of partial[0..n) in a fixed order (one block).
-__global__ void __launch_bounds__(256) k_sum_partials(const double *__restrict__ partial, int n,
+static __global__ void __launch_bounds__(256) k_sum_partials(const double *__restrict__ partial, int n,
                                                       double *__restrict__ out)
 {
     double acc = 0;

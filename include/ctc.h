@@ -312,6 +312,40 @@ int ctc_tune_lookup(const char *cache_path, const ctc_tensor *train, const ctc_p
 /* The cache key of that shape (NUL-terminated, at most len bytes). */
 int ctc_tune_key(const ctc_tensor *train, const ctc_params *p, int sm_count, char *buf, int len);
 
+/* First-order training driven by the adjoint (no reference counterpart;
+ * the reference's first-order method is per-nonzero SGD, sgpu/sgd.cu:21-143,
+ * whose step is the negative gradient of 1/2 e^2 + 1/2 lambda ||a||^2, i.e.
+ * lambda twice the lambda below).  Loss of an order-3 or order-4 tensor:
+ *     f = 1/2 sum_Omega (x - [[U_1, ..., U_d]])^2 + lambda sum_m ||U_m||^2.
+ * Each step takes the gradient of a minibatch of `batch` nonzeros (scaled by
+ * nonzeros / batch; batch 0 = full gradient) in one pass, residuals
+ * recomputed, and applies Adam to FP32 master factors; with precision
+ * CTC_PREC_MIXED the pass gathers BF16 copies of the factors (refreshed by
+ * the Adam step) and accumulates in FP32.  The training nonzeros are
+ * shuffled once on the device (seeded); each epoch visits the minibatches
+ * in a seeded random order. */
+typedef struct {
+    int rank;           /* 8, 16, 32 or 64 */
+    int precision;      /* CTC_PREC_F32 or CTC_PREC_MIXED (BF16 gathers)      */
+    double lambda;
+    double lr, beta1, beta2, eps;   /* Adam */
+    uint64_t batch;     /* nonzeros per step; 0 = the whole tensor            */
+    int epochs;
+    uint64_t seed;      /* shuffle and minibatch order                         */
+    int eval_every;     /* epochs between evaluations; 0 = only the last       */
+} ctc_fo_params;
+typedef struct ctc_fo ctc_fo;
+int ctc_fo_params_default(ctc_fo_params *p);
+int ctc_fo_create(ctc_ctx *ctx, const ctc_tensor *train, const ctc_tensor *test,
+                  const ctc_fo_params *p, ctc_fo **out);
+int ctc_fo_free(ctc_fo *f);
+int ctc_fo_dims(const ctc_fo *f, int *order, uint64_t *dims);
+/* model: order and rows of the tensors (ctc_fo_dims), rank p->rank; initial
+ * factors in, final factors out.  cb gets loss (training SSE), frob
+ * (lambda sum ||U||^2) and the train/test RMSE after evaluated epochs. */
+int ctc_fo_run(ctc_fo *f, ctc_model *model, const ctc_fo_params *p, ctc_epoch_cb cb, void *user,
+               ctc_result *res);
+
 /* Per-kernel device time: with profiling on, every launch of this library
  * on the context is bracketed by a CUDA event pair; kernel_time sums the
  * launches whose kernel name contains `name` (count, milliseconds).  No
@@ -341,11 +375,11 @@ int ctc_rmse(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double *
 int ctc_sse_noalloc(const void *rec, uint64_t n, const float *U0, const float *U1,
                     const float *U2, int rank, double *out_sse, void *stream);
 
-/* Adjoint of the masked CP loss 1/2 ||P_Omega(X - [[A,B,C]])||^2 +
- * lambda sum ||U_m||^2: every factor gradient from one pass over the
- * tensor, residuals recomputed, not stored.  grads[m]: dims[m] x rank
- * row-major doubles.  obj (may be NULL) receives the loss value.
- * No reference counterpart (the reference has no gradient path). */
+/* Adjoint of the masked CP loss 1/2 ||P_Omega(X - [[U_1,...,U_d]])||^2 +
+ * lambda sum ||U_m||^2 (order d = 3 or 4, FP64): every factor gradient from
+ * one pass over the tensor, residuals recomputed, not stored.  grads[m]:
+ * dims[m] x rank row-major doubles.  obj (may be NULL) receives the loss
+ * value.  No reference counterpart (the reference has no gradient path). */
 int ctc_grad(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double lambda,
              double *const *grads, double *obj);
 

@@ -317,3 +317,35 @@ def write_tns(path, T: Tensor, fmt="%.17g"):
         cols = [T.ind[m] for m in range(T.nmodes)]
         for n in range(T.nnz):
             f.write(" ".join(str(int(c[n])) for c in cols) + " " + (fmt % T.vals[n]) + "\n")
+
+
+# ---------------------------------------------------------------------------
+# Masked CP loss of any order in FP64 (numpy): the checker of the adjoint
+# kernel at order 4 (the C restatement, orc_grad / orc_objective, is order 3).
+# f = 1/2 sum_Omega (x - sum_r prod_m U_m(i_m, r))^2 + lam sum_m ||U_m||^2
+# ---------------------------------------------------------------------------
+def cp_objective(ind, vals, U, lam):
+    P = np.ones((ind.shape[1], U[0].shape[1]))
+    for m, u in enumerate(U):
+        P *= u[ind[m].astype(np.int64) - 1]
+    e = vals - P.sum(1)
+    return 0.5 * float(e @ e) + lam * sum(float((u * u).sum()) for u in U)
+
+
+def cp_grad(ind, vals, U, lam):
+    idx = [ind[m].astype(np.int64) - 1 for m in range(len(U))]
+    rows = [u[i] for u, i in zip(U, idx)]
+    P = np.ones_like(rows[0])
+    for r in rows:
+        P = P * r
+    e = vals - P.sum(1)
+    G = []
+    for m, u in enumerate(U):
+        others = np.ones_like(rows[0])
+        for n, r in enumerate(rows):
+            if n != m:
+                others = others * r
+        g = 2.0 * lam * u
+        np.add.at(g, idx[m], -e[:, None] * others)
+        G.append(g)
+    return G

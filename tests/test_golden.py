@@ -110,3 +110,24 @@ def test_live_reference_ciss_random():
             assert np.array_equal(a["directory"], b["directory"])
             assert np.array_equal(a["dcounter"], b["dcounter"])
             assert np.array_equal(a["entries"].view(np.uint64)[w], b["entries"].view(np.uint64)[w])
+
+
+def test_numpy_cp_grad_is_the_fd_gradient():
+    """The order-d FP64 restatement of the masked CP loss gradient (the
+    adjoint kernel's checker) against central finite differences."""
+    rng = np.random.default_rng(5)
+    dims = (5, 4, 3, 2)
+    ind = np.stack([rng.integers(1, d + 1, 40) for d in dims]).astype(np.uint64)
+    v = rng.uniform(1, 5, 40)
+    U = [rng.uniform(0, 1, (d, 3)) for d in dims]
+    G = po.cp_grad(ind, v, U, 0.2)
+    h = 1e-6
+    for m in range(4):
+        for r in range(dims[m]):
+            for c in range(3):
+                Up = [u.copy() for u in U]
+                Um = [u.copy() for u in U]
+                Up[m][r, c] += h
+                Um[m][r, c] -= h
+                fd = (po.cp_objective(ind, v, Up, 0.2) - po.cp_objective(ind, v, Um, 0.2)) / (2 * h)
+                assert abs(fd - G[m][r, c]) < 1e-6 * max(1.0, abs(fd))
