@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip e2e / time-to-RMSE / CPU legs")
     ap.add_argument("--ccdpp-tile", type=int, default=0, help="CCD++ tile length (0 = library default)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 256-instance leg")
+    ap.add_argument("--no-fo", action="store_true", help="skip the first-order (order-4 Adam) leg")
     ap.add_argument("--instances", type=int, default=0, help="batch workloads: a K-instance sample of the same distribution")
     ap.add_argument("--tune-cache", default="", help="autotuner cache file (default: a fresh temporary one)")
     ap.add_argument("--no-tune", action="store_true", help="library defaults instead of autotuned parameters")
@@ -356,6 +357,8 @@ def run_ours(args):
     del tr, te
     if rank == 0 and not args.no_extras and not args.no_batch:
         out["batched"] = batch_leg(ctc, ctx, args, device)
+    if rank == 0 and not args.no_extras and not args.no_fo:
+        out["first_order"] = fo_leg(ctc, ctx, argparse.Namespace(**{**vars(args), "nnz": 0}), device)
     if rank == 0:
         print(json.dumps(out))
     ctx.close()
@@ -421,6 +424,61 @@ def batch_leg(ctc, ctx, args, device):
         B.free()
         for m in models:
             m.free()
+    return out
+
+
+def fo_leg(ctc, ctx, args, device):
+    """Adjoint-driven minibatch Adam on the order-4 workload (1M x 200k x 1k
+    x 24, 250M Zipf(1.2) cells, CP rank 32 + N(0, 0.1^2), R = 64, minibatch
+    2^20 nonzeros, Adam lr 1e-3): epochs in FP32 and with BF16 gathers
+    (FP32 masters and accumulation).  Reports epoch time, nonzeros/s, the
+    adjoint kernel's share and throughput, and the test RMSE of both."""
+    import torch
+
+    from cutc_b200 import synth
+    w = synth.WORKLOADS["zipf4-250m"]
+    if args.nnz:
+        w = synth.scaled(w, args.nnz)
+    t0 = time.time()
+    data = synth.generate(w, seed=args.seed, device=device)
+    tr = ctc.Tensor.from_coo(*data["train"], dims=w.dims)
+    te = ctc.Tensor.from_coo(*data["test"], dims=w.dims)
+    ntr, nte = int(data["train"][1].size), int(data["test"][1].size)
+    del data
+    torch.cuda.empty_cache()
+    out = {"workload": w.name, "dims": list(w.dims), "nnz_train": ntr, "nnz_test": nte, "rank": w.rank,
+           "batch": 1 << 20, "lr": 1e-3, "lambda": 1e-4, "generate_s": time.time() - t0}
+    epochs = 2
+    for name, prec in (("fp32", ctc.PREC_F32), ("mixed_bf16", ctc.PREC_MIXED)):
+        p = ctc.fo_params(rank=w.rank, precision=prec, lr=1e-3, batch=1 << 20, epochs=epochs, eval_every=0,
+                          seed=args.seed + 1, **{"lambda": 1e-4})
+        t1 = time.time()
+        F = ctc.FirstOrder(ctx, tr, te, p)
+        stage_s = time.time() - t1
+        m = ctc.Model(w.dims, w.rank).init_uniform(args.seed + 1, 1.0 / np.sqrt(w.rank))
+        ctx.set_profiling(True)
+        ctx.reset_kernel_times()
+        run = F.run(m, p)
+        kn, kms = ctx.kernel_time("k_fo_grad")
+        an, ams = ctx.kernel_time("k_fo_adam")
+        ctx.set_profiling(False)
+        ep_ms = [run.result["total_ms"] / epochs] * epochs  # device time of the update epochs
+        steps = (ntr + (1 << 20) - 1) >> 20
+        grad_launches = steps * epochs
+        # adjoint kernel per launch: 16 B indices + 4 B value per nonzero and
+        # four gathered rows (R elements each) per nonzero
+        gbytes = 2 if prec == ctc.PREC_MIXED else 4
+        per_nz = 20 + 4 * w.rank * gbytes
+        grad_avg = kms / max(kn, 1)
+        out[name] = {"epoch_s": float(np.mean(ep_ms)) / 1000.0, "nnz_per_s": ntr / (float(np.mean(ep_ms)) / 1000.0),
+                     "stage_s": stage_s, "test_rmse": run.epochs[-1]["rmse_te"],
+                     "train_rmse": run.epochs[-1]["rmse_tr"], "initial_test_rmse": run.epochs[0]["rmse_te"],
+                     "adjoint": {"launches": kn, "avg_ms": grad_avg,
+                                 "share": kms / max(sum(ep_ms), 1e-9),
+                                 "gathered_GBps": (1 << 20) * per_nz / (grad_avg / 1000.0) / 1e9},
+                     "adam": {"launches": an, "avg_ms": ams / max(an, 1)}}
+        F.free()
+        m.free()
     return out
 
 
@@ -516,6 +574,26 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def run_fo_only(args):
+    """--workload zipf4-250m: the first-order leg alone, as its own JSON line."""
+    import torch
+
+    import cutc_b200 as ctc
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    ctx = ctc.Context(local)
+    f = fo_leg(ctc, ctx, args, f"cuda:{local}")
+    print(json.dumps({"metric": "first-order training nnz/s (minibatch Adam epoch, BF16 gathers)",
+                      "value": f["mixed_bf16"]["nnz_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 2, "warmup": 0,
+                      "ms_per_step": 1000.0 * f["mixed_bf16"]["epoch_s"], "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "bf16/f32",
+                      "data": "synthetic (seeded order-4 Zipf CP tensor)", "config": {"workload": f["workload"]},
+                      "first_order": f}))
+    ctx.close()
+
+
 def run_batch_only(args):
     """--workload batch-256: the batched leg alone, as its own JSON line."""
     import torch
@@ -543,5 +621,7 @@ if __name__ == "__main__":
         run_reference(a)
     elif a.workload.startswith("batch"):
         run_batch_only(a)
+    elif a.workload.startswith("zipf4"):
+        run_fo_only(a)
     else:
         run_ours(a)

@@ -150,7 +150,9 @@ static void fo_pass(ctc_fo *f, const uint4 *idx, const float *val, uint64_t b, u
     a.priv_elems = priv;
     a.scale = scale;
     const unsigned g = grid_for(e - b, 256, kMaxPartials);
-    LAUNCH(ctx, (fo::k_fo<float, GT, R, D, GRAD>), g, 256, priv * sizeof(float), a, ctx->partial.p);
+    // named apart so that per-kernel times separate the adjoint from evaluation
+    launch_named(ctx, GRAD ? "fo::k_fo_grad" : "fo::k_fo_eval", fo::k_fo<float, GT, R, D, GRAD>, g, 256,
+                 priv * sizeof(float), a, ctx->partial.p);
 }
 
 template <int R, int D>

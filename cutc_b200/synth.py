@@ -43,6 +43,9 @@ WORKLOADS = {
     # 400M Zipf(1.3) cells over 1M x 600k x 300, CP rank 24, R = 64
     "zipf-400m": Workload("zipf-400m", (1_000_000, 600_000, 300), 400_000_000, 24, 64, 0.2, False,
                           (1.3, 1.3, 1.3)),
+    # order 4: 250M Zipf(1.2) cells over 1M x 200k x 1k x 24, CP rank 32, R = 64
+    "zipf4-250m": Workload("zipf4-250m", (1_000_000, 200_000, 1_000, 24), 250_000_000, 32, 64, 0.1, False,
+                           (1.2, 1.2, 1.2, 1.2)),
 }
 
 
@@ -68,15 +71,15 @@ def _zipf_ranks(torch, n, dim, s, gen, device):
 
 
 def _draw_cells(torch, w: Workload, n, gen, device, perms):
-    cols = []
+    # mixed-radix cell keys (the product of the dimensions stays below 2^63)
+    key = None
     for m, d in enumerate(w.dims):
         if w.zipf is None:
             c = torch.randint(0, d, (n,), generator=gen, device=device, dtype=torch.int64)
         else:
             c = perms[m][_zipf_ranks(torch, n, d, w.zipf[m], gen, device)]
-        cols.append(c)
-    J, K = w.dims[1], w.dims[2]
-    return cols[0] * (J * K) + cols[1] * K + cols[2]
+        key = c if key is None else key * d + c
+    return key
 
 
 def generate(w: Workload, seed: int = 0, device: str = "cpu", train_frac: float = 0.9):
@@ -85,7 +88,6 @@ def generate(w: Workload, seed: int = 0, device: str = "cpu", train_frac: float 
     torch = _torch()
     gen = torch.Generator(device=device)
     gen.manual_seed(seed)
-    I, J, K = w.dims
     perms = [torch.randperm(d, generator=gen, device=device) for d in w.dims]
     keys = torch.unique(_draw_cells(torch, w, w.nnz, gen, device, perms))
     tries = 0
@@ -99,9 +101,11 @@ def generate(w: Workload, seed: int = 0, device: str = "cpu", train_frac: float 
     # a seeded random subset of exactly nnz distinct cells
     sel = torch.randperm(keys.numel(), generator=gen, device=device)[: w.nnz]
     keys = keys[sel]
-    i = keys // (J * K)
-    j = (keys // K) % J
-    k = keys % K
+    cols = []
+    for d in reversed(w.dims):
+        cols.append(keys % d)
+        keys = keys // d
+    cols = cols[::-1]
     del keys, sel
     # values: rank-k CP model with N(0,1) factors
     F = [torch.randn(d, w.cp_rank, generator=gen, device=device, dtype=torch.float32) for d in w.dims]
@@ -109,14 +113,19 @@ def generate(w: Workload, seed: int = 0, device: str = "cpu", train_frac: float 
     step = 1 << 24
     for s0 in range(0, w.nnz, step):
         sl = slice(s0, min(s0 + step, w.nnz))
-        v[sl] = (F[0][i[sl]] * F[1][j[sl]] * F[2][k[sl]]).sum(1)
+        pr = F[0][cols[0][sl]]
+        for m in range(1, len(w.dims)):
+            pr = pr * F[m][cols[m][sl]]
+        v[sl] = pr.sum(1)
+        del pr
     lo, hi = v.min(), v.max()
     v = 1.0 + 4.0 * (v - lo) / (hi - lo)
     v = v.double() + w.sigma * torch.randn(w.nnz, generator=gen, device=device, dtype=torch.float64)
     if w.clip:
         v.clamp_(1.0, 5.0)
     train_mask = torch.rand(w.nnz, generator=gen, device=device) < train_frac
-    ind = torch.stack([i, j, k]) + 1
+    ind = torch.stack(cols) + 1
+    del cols
 
     def pack(mask):
         return (ind[:, mask].cpu().numpy().astype(np.uint64), v[mask].cpu().numpy())
