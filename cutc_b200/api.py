@@ -108,6 +108,7 @@ def lib():
             "ctc_tensor_free": (C.c_int, [P]),
             "ctc_ciss_build": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(P)]),
             "ctc_ciss_build_ga": (C.c_int, [P, C.c_int, C.c_int, C.POINTER(P)]),
+            "ctc_ciss_build_gpu": (C.c_int, [P, P, C.c_int, C.c_int, C.c_int, C.POINTER(P)]),
             "ctc_dataset_dims": (C.c_int, [P, _u64p]),
             "ctc_dataset_set_model": (C.c_int, [P, P]),
             "ctc_dataset_epochs": (C.c_int, [P, C.c_int]),
@@ -291,6 +292,24 @@ def ciss_alloc(t: Tensor, mode: int, tile_len: int = 32, ga: bool = False):
     h = C.c_void_p()
     build = lib().ctc_ciss_build_ga if ga else lib().ctc_ciss_build
     _check(build(t.h, mode, tile_len, C.byref(h)))
+    return _ciss_export(h)
+
+
+CISS_GA, CISS_SORT = 1, 2
+
+
+def ciss_alloc_gpu(ctx: Context, t: Tensor, mode: int, tile_len: int = 32, ga: bool = False,
+                   sort: bool = False):
+    """The same CISS built on the device (ctc_ciss_build_gpu); sort=True
+    first sorts the nonzeros for `mode` on the device (stable by the mode
+    index, then the next mode's)."""
+    h = C.c_void_p()
+    flags = (CISS_GA if ga else 0) | (CISS_SORT if sort else 0)
+    _check(lib().ctc_ciss_build_gpu(ctx.h, t.h, mode, tile_len, flags, C.byref(h)))
+    return _ciss_export(h)
+
+
+def _ciss_export(h):
     try:
         nnz, dl, sz = C.c_uint64(), C.c_uint64(), C.c_uint64()
         tl = C.c_int()

@@ -104,6 +104,16 @@ int ctc_ciss_build(const ctc_tensor *t, int mode, int tile_len, ctc_ciss **out);
  * rows): identical tiles; its directory counters count the first nonzero
  * too (ga/ciss.c:101-120), so dcounter[k] = start of slice k. */
 int ctc_ciss_build_ga(const ctc_tensor *t, int mode, int tile_len, ctc_ciss **out);
+/* The same CISS built on the GPU of `ctx`, bit-exact with ctc_ciss_build
+ * (CTC_CISS_GA: with ctc_ciss_build_ga's counters).  With CTC_CISS_SORT
+ * the nonzeros are first sorted for `mode` on the device (stable by the
+ * mode index, then the next mode's index: the order of the reference's
+ * traina/b/c files); without it `t` must already be in that order, as for
+ * ciss_alloc.  Same ownership and export as ctc_ciss_build. */
+#define CTC_CISS_GA 1
+#define CTC_CISS_SORT 2
+int ctc_ciss_build_gpu(ctc_ctx *ctx, const ctc_tensor *t, int mode, int tile_len, int flags,
+                       ctc_ciss **out);
 int ctc_ciss_sizes(const ctc_ciss *c, uint64_t *nnz, uint64_t *dlength,
                    uint64_t *size_rows, int *tile_len);
 /* directory: dlength u64; dcounter: dlength+1 u64; entries: size_rows*3 f64;
