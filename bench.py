@@ -345,6 +345,7 @@ def run_ours(args):
     if rank == 0 and not args.no_extras:
         out["time_to_rmse"] = time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, args.seed)
         out["e2e"] = e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args)
+        out["ciss_build"] = ciss_build_times(ctc, ctx, tr[0])
         v, s, threads, nsamp = cpu_baseline(base0, dims, R, args.sample, args.seed)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                "sample": f"{nsamp} of {n_train} training nonzeros (seeded random), one "
@@ -517,6 +518,21 @@ def time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, seed):
     return res
 
 
+def ciss_build_times(ctc, ctx, t0):
+    """The reference's CISS layout (tile length 32, mode 1) of the mode-1
+    training copy: host builder against the device builder (host tensor in,
+    host CISS out, transfers and the export to numpy included in both)."""
+    res = {}
+    for name, fn in (("host_s", lambda: ctc.ciss_alloc(t0, 1, 32)),
+                     ("gpu_s", lambda: ctc.ciss_alloc_gpu(ctx, t0, 1, 32))):
+        t = time.perf_counter()
+        c = fn()
+        res[name] = time.perf_counter() - t
+        res["entries_bytes"] = int(c["entries"].nbytes)
+        del c
+    return res
+
+
 def e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args):
     """The same metric through the reference-facing call with host buffers:
     ctc_run (tensors staged from host memory, one epoch, evaluation, factors
@@ -574,6 +590,72 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def als_leg(ctc, ctx, args, device):
+    """ALS at rank 64 on the 400M-nonzero Zipf(1.3) tensor (1M x 600k x
+    300, CP rank 24 + N(0, 0.2^2), lambda 0.05): iterations in FP32 and in
+    mixed precision (BF16 factor copies into tcgen05 Gram blocks for the
+    pieces of long rows, FP64 row solves with one refinement step)."""
+    import torch
+
+    from cutc_b200 import synth
+    w = synth.WORKLOADS["zipf-400m"]
+    if args.nnz:
+        w = synth.scaled(w, args.nnz)
+    t0 = time.time()
+    data = synth.generate(w, seed=args.seed, device=device)
+    ti, tv = data["train"]
+    te = ctc.Tensor.from_coo(*data["test"], dims=w.dims)
+    ntr = int(tv.size)
+    del data
+    srt = sort_modes_torch(ti, tv, w.dims, device)
+    del ti, tv
+    torch.cuda.empty_cache()
+    tr = [ctc.Tensor.from_coo(i, v, dims=w.dims) for i, v in srt]
+    del srt
+    out = {"workload": w.name, "dims": list(w.dims), "nnz_train": ntr, "rank": w.rank, "lambda": 0.05,
+           "generate_s": time.time() - t0}
+    iters = 3
+    for name, prec in (("fp32", ctc.PREC_F32), ("mixed_tc", ctc.PREC_MIXED)):
+        p = ctc.params("als", rank=w.rank, precision=prec, iters=iters, early_stop=0, eval_every=0,
+                       **{"lambda": 0.05})
+        t1 = time.time()
+        ds = ctc.Dataset(ctx, tr, None, te, p)
+        stage_s = time.time() - t1
+        m = ctc.Model(ds.dims(), w.rank).init_uniform(args.seed + 1, 1.0 / np.sqrt(w.rank))
+        ctx.set_profiling(True)
+        ctx.reset_kernel_times()
+        run = ds.run(m, p)
+        kt = {k: ctx.kernel_time(k) for k in ("k_als_tile", "k_als_fix", "k_als_gram_tc")}
+        ctx.set_profiling(False)
+        it_s = run.result["total_ms"] / 1000.0 / iters
+        out[name] = {"iteration_s": it_s, "nnz_per_s": ntr / it_s, "stage_s": stage_s,
+                     "test_rmse": run.epochs[-1]["rmse_te"], "train_rmse": run.epochs[-1]["rmse_tr"],
+                     "kernels": {k: {"launches": v[0], "ms_per_iter": v[1] / iters} for k, v in kt.items() if v[0]}}
+        ds.free()
+        m.free()
+    return out
+
+
+def run_als_only(args):
+    """--workload zipf-400m: the rank-64 ALS leg alone, as its own JSON line."""
+    import torch
+
+    import cutc_b200 as ctc
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    ctx = ctc.Context(local)
+    a = als_leg(ctc, ctx, args, f"cuda:{local}")
+    print(json.dumps({"metric": "ALS training nnz/s (rank 64, mixed precision with tensor-core Gram blocks)",
+                      "value": a["mixed_tc"]["nnz_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 3, "warmup": 0,
+                      "ms_per_step": 1000.0 * a["mixed_tc"]["iteration_s"], "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "bf16/f32/f64",
+                      "data": "synthetic (seeded Zipf CP tensor)", "config": {"workload": a["workload"]},
+                      "als": a}))
+    ctx.close()
+
+
 def run_fo_only(args):
     """--workload zipf4-250m: the first-order leg alone, as its own JSON line."""
     import torch
@@ -623,5 +705,7 @@ if __name__ == "__main__":
         run_batch_only(a)
     elif a.workload.startswith("zipf4"):
         run_fo_only(a)
+    elif a.workload == "zipf-400m":
+        run_als_only(a)
     else:
         run_ours(a)

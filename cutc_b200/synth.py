@@ -32,6 +32,7 @@ class Workload:
     sigma: float
     clip: bool
     zipf: tuple | None  # per-mode exponent, or None for uniform
+    zipf_top: tuple | None = None  # per mode: expected nonzeros of the top row (Zipf-Mandelbrot offset), 0 = plain
 
 
 WORKLOADS = {
@@ -40,9 +41,14 @@ WORKLOADS = {
     # 500k x 20k x 2k, 100M Zipf(1.1) cells, CP rank 16, R = 32
     "zipf-100m": Workload("zipf-100m", (500_000, 20_000, 2_000), 100_000_000, 16, 32, 0.25, True,
                           (1.1, 1.1, 1.1)),
-    # 400M Zipf(1.3) cells over 1M x 600k x 300, CP rank 24, R = 64
+    # 400M Zipf(1.3) cells over 1M x 600k x 300, CP rank 24, R = 64.  I.i.d.
+    # Zipf(1.3) in every mode puts about a quarter of the nonzeros in one
+    # row of each large mode and cannot be deduplicated to 400M distinct
+    # cells; the two large modes use a Zipf-Mandelbrot offset q, p(r) ~
+    # (r + q)^-1.3, solved so that their top row holds 1e5 nonzeros (rows
+    # then span 1 to ~1e5); the 300-row mode stays plain Zipf(1.3)
     "zipf-400m": Workload("zipf-400m", (1_000_000, 600_000, 300), 400_000_000, 24, 64, 0.2, False,
-                          (1.3, 1.3, 1.3)),
+                          (1.3, 1.3, 1.3), (100_000, 100_000, 0)),
     # order 4: 250M Zipf(1.2) cells over 1M x 200k x 1k x 24, CP rank 32, R = 64
     "zipf4-250m": Workload("zipf4-250m", (1_000_000, 200_000, 1_000, 24), 250_000_000, 32, 64, 0.1, False,
                            (1.2, 1.2, 1.2, 1.2)),
@@ -50,9 +56,35 @@ WORKLOADS = {
 
 
 def scaled(w: Workload, nnz: int, dims=None) -> Workload:
-    """The same distribution with fewer nonzeros (and optionally other dims)."""
+    """The same distribution with fewer nonzeros (and optionally other dims;
+    the top-row targets scale with the nonzeros)."""
+    top = None if w.zipf_top is None else tuple(int(t * nnz / w.nnz) for t in w.zipf_top)
     return Workload(w.name + f"@{nnz}", tuple(dims or w.dims), nnz, w.cp_rank, w.rank, w.sigma,
-                    w.clip, w.zipf)
+                    w.clip, w.zipf, top)
+
+
+def zipf_offset(dim: int, s: float, n: int, top: float) -> float:
+    """Offset q of the Zipf-Mandelbrot law p(r) ~ (r + q)^-s over ranks
+    1..dim such that n * p(1) = top (bisection; 0 when plain Zipf already
+    puts at most `top` nonzeros in the first rank)."""
+    r = np.arange(1, dim + 1, dtype=np.float64)
+
+    def first(q):
+        w = (r + q) ** -s
+        return n * w[0] / w.sum()
+
+    if top <= 0 or first(0.0) <= top:
+        return 0.0
+    lo, hi = 0.0, float(dim)
+    while first(hi) > top:
+        hi *= 2.0
+    for _ in range(100):
+        mid = 0.5 * (lo + hi)
+        if first(mid) > top:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
 
 
 def _torch():
@@ -60,10 +92,11 @@ def _torch():
     return torch
 
 
-def _zipf_ranks(torch, n, dim, s, gen, device):
-    # inverse CDF of the truncated Zipf(s) over ranks 1..dim
+def _zipf_ranks(torch, n, dim, s, gen, device, q=0.0):
+    # inverse CDF of the truncated Zipf(s) (offset q: Zipf-Mandelbrot) over
+    # ranks 1..dim
     ranks = torch.arange(1, dim + 1, device=device, dtype=torch.float64)
-    pmf = ranks.pow(-s)
+    pmf = (ranks + q).pow(-s)
     cdf = torch.cumsum(pmf, 0)
     cdf = cdf / cdf[-1]
     u = torch.rand(n, generator=gen, device=device, dtype=torch.float64)
@@ -77,7 +110,8 @@ def _draw_cells(torch, w: Workload, n, gen, device, perms):
         if w.zipf is None:
             c = torch.randint(0, d, (n,), generator=gen, device=device, dtype=torch.int64)
         else:
-            c = perms[m][_zipf_ranks(torch, n, d, w.zipf[m], gen, device)]
+            q = zipf_offset(d, w.zipf[m], w.nnz, w.zipf_top[m]) if w.zipf_top else 0.0
+            c = perms[m][_zipf_ranks(torch, n, d, w.zipf[m], gen, device, q)]
         key = c if key is None else key * d + c
     return key
 
