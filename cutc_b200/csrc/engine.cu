@@ -626,9 +626,14 @@ struct Session : SessionBase {
                    (const T *)(c.has_w ? c.w.p : nullptr), m, U[m].p, (const T *)U[m1].p, (const T *)U[m2].p,
                    (T)p.lambda, slot.p, nonspd_dev.p, tc ? 1 : 0);
             if (tc && c.npieces) als_gram_tc(c, m);
-            if (c.nheavy)
+            if (c.nheavy) {
+                // pieces summed element-parallel first; the solve reads one slot per row
+                LAUNCH(ctx, k::k_als_sum_pieces<T, R>,
+                       grid_for((uint64_t)c.nheavy * (R * R + R), 256, kSMs * 16), 256, 0,
+                       (const uint4 *)c.heavy.p, c.nheavy, slot.p);
                 LAUNCH(ctx, k::k_als_fix<T, R>, grid_for(c.nheavy, 4, kSMs * 16), 128, smem,
-                       (const uint4 *)c.heavy.p, c.nheavy, (const T *)slot.p, U[m].p, (T)p.lambda, nonspd_dev.p);
+                       (const uint4 *)c.heavy.p, c.nheavy, (const T *)slot.p, U[m].p, (T)p.lambda, nonspd_dev.p, 1);
+            }
             if (tc) refresh_bf16(m);
         }
     }

@@ -870,7 +870,7 @@ __global__ void __launch_bounds__(128) k_ccdc_fix(const uint4 *__restrict__ heav
 // in registers.  The row's system is solved by its warp in FP64 in shared
 // memory: Cholesky, forward/back substitution, one refinement step against
 // the register copy of the Gram matrix.  Heavy-row pieces store their
-// partial Gram + right-hand side; k_als_fix sums them in piece order.
+// partial Gram + right-hand side; k_als_sum_pieces sums them in piece order.
 // ---------------------------------------------------------------------
 template <int R>
 struct AlsShape {
@@ -1232,10 +1232,33 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
     if (lane == 0 && bad) atomicAdd(nonspd, (unsigned long long)bad);
 }
 
+// Sum of each long row's piece partials, element-parallel: thread per
+// (row, slot entry), pieces added in piece order (the order k_als_fix used
+// when it summed them itself), the total written into the row's first
+// slot.  Coalesced across the threads of a row; every thread touches only
+// its own entry.
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_als_sum_pieces(const uint4 *__restrict__ heavy, uint32_t nheavy,
+                                                        T *__restrict__ slot)
+{
+    constexpr uint32_t S = R * R + R;
+    const uint64_t total = (uint64_t)nheavy * S;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t h = (uint32_t)(i / S), e = (uint32_t)(i % S);
+        const uint4 hr = heavy[h];
+        const T *src = slot + (size_t)hr.y * S + e;
+        T acc = 0;
+        for (uint32_t q = 0; q < hr.z; ++q) acc += src[(size_t)q * S];
+        slot[(size_t)hr.y * S + e] = acc;
+    }
+}
+
+// summed != 0: the pieces were already summed into each row's first slot
 template <typename T, int R>
 __global__ void __launch_bounds__(128) k_als_fix(const uint4 *__restrict__ heavy, uint32_t nheavy,
                                                  const T *__restrict__ slot, T *Um, T lambda,
-                                                 unsigned long long *nonspd)
+                                                 unsigned long long *nonspd, int summed)
 {
     using Sh = AlsShape<R>;
     constexpr int L = Sh::L, C = Sh::C;
@@ -1257,7 +1280,8 @@ __global__ void __launch_bounds__(128) k_als_fix(const uint4 *__restrict__ heavy
 #pragma unroll
             for (int a = 0; a < R; ++a) G[a][c] = 0;
         }
-        for (uint32_t q = 0; q < hr.z; ++q) {
+        const uint32_t np = summed ? 1u : hr.z;
+        for (uint32_t q = 0; q < np; ++q) {
             const T *src = slot + (size_t)(hr.y + q) * (R * R + R);
 #pragma unroll
             for (int c = 0; c < C; ++c) {
