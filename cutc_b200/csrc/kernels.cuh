@@ -981,7 +981,8 @@ struct AlsBatch {
     static constexpr int NS = 32 / GS;
     static constexpr int TRI = R * (R + 1) / 2;
     static constexpr int gram_doubles = (TRI * (int)sizeof(T) + 7) / 8;
-    static constexpr int sys_doubles = TRI + 3 * R + gram_doubles;
+    // + R doubles: reciprocals of the factor's diagonal
+    static constexpr int sys_doubles = TRI + 4 * R + gram_doubles;
     static constexpr int warp_doubles = NS * sys_doubles + (NS + 1) / 2;
 };
 
@@ -1003,6 +1004,7 @@ __device__ __forceinline__ int als_solve_parked(double *W, int k, T lambda, T *U
     double *yy = bb + R;
     double *uu = yy + R;
     const T *gram = reinterpret_cast<const T *>(uu + R);
+    double *dinv = uu + R + B::gram_doubles;
     const uint32_t *rows = reinterpret_cast<const uint32_t *>(W + (size_t)B::NS * B::sys_doubles);
     int bad = 0;
     for (int j = 0; j < R; ++j) {
@@ -1012,22 +1014,38 @@ __device__ __forceinline__ int als_solve_parked(double *W, int k, T lambda, T *U
             d = 1e-300 + fabs(d) + 1e-12 * (double)lambda + 1e-30;
         }
         const double ljj = sqrt(d);
+        const double inv = 1.0 / ljj;  // one division per column
         __syncwarp();
         if (act) {
-            if (sl == 0) fac[tri_idx(j, j)] = ljj;
-            for (int i = j + 1 + sl; i < R; i += GS) fac[tri_idx(i, j)] /= ljj;
+            if (sl == 0) {
+                fac[tri_idx(j, j)] = ljj;
+                dinv[j] = inv;
+            }
+            for (int i = j + 1 + sl; i < R; i += GS) fac[tri_idx(i, j)] *= inv;
         }
         __syncwarp();
+        // trailing update L(i, k) -= L(i, j) L(k, j), j < k <= i, by columns:
+        // lane sl of the group owns the columns k with k mod 2GS equal to sl
+        // or 2GS-1-sl, which gives every lane the same number of entries
         if (act)
-            for (int i = j + 1 + sl; i < R; i += GS) {
-                const double lij = fac[tri_idx(i, j)];
-                for (int k2 = j + 1; k2 <= i; ++k2) fac[tri_idx(i, k2)] -= lij * fac[tri_idx(k2, j)];
+            for (int c0 = 0; c0 < R; c0 += 2 * GS) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = h == 0 ? c0 + sl : c0 + 2 * GS - 1 - sl;
+                    if (k <= j || k >= R) continue;
+                    const double lkj = fac[tri_idx(k, j)];
+                    int base = k * (k + 1) / 2;  // tri_idx(i, 0) for i = k
+                    for (int i = k; i < R; ++i) {
+                        fac[base + k] -= fac[base + j] * lkj;
+                        base += i + 1;
+                    }
+                }
             }
         __syncwarp();
     }
     for (int it = 0; it < 2; ++it) {
         for (int i = 0; i < R; ++i) {  // L z = y
-            const double zi = act ? yy[i] / fac[tri_idx(i, i)] : 0.0;
+            const double zi = act ? yy[i] * dinv[i] : 0.0;
             __syncwarp();
             if (act) {
                 if (sl == 0) yy[i] = zi;
@@ -1036,7 +1054,7 @@ __device__ __forceinline__ int als_solve_parked(double *W, int k, T lambda, T *U
             __syncwarp();
         }
         for (int i = R - 1; i >= 0; --i) {  // L^T v = z
-            const double vi = act ? yy[i] / fac[tri_idx(i, i)] : 0.0;
+            const double vi = act ? yy[i] * dinv[i] : 0.0;
             __syncwarp();
             if (act) {
                 if (sl == 0) yy[i] = vi;
