@@ -128,6 +128,9 @@ def lib():
             "ctc_model_copy": (C.c_int, [P, P]),
             "ctc_model_info": (C.c_int, [P, C.POINTER(C.c_int), _u64p, C.POINTER(C.c_int)]),
             "ctc_model_free": (C.c_int, [P]),
+            "ctc_model_write_text": (C.c_int, [P, C.c_int, C.c_char_p]),
+            "ctc_model_save": (C.c_int, [P, C.c_char_p]),
+            "ctc_model_load": (C.c_int, [C.c_char_p, C.POINTER(P)]),
             "ctc_params_default": (C.c_int, [C.c_int, C.POINTER(Params)]),
             "ctc_run": (C.c_int, [P, C.POINTER(P), P, P, P, P, C.POINTER(Params), EPOCH_CB, P,
                                   C.POINTER(Result)]),
@@ -355,6 +358,27 @@ class Model:
 
     def factors(self):
         return [self.get(m) for m in range(len(self.dims))]
+
+    def write_text(self, mode: int, path: str):
+        """Factor `mode` in the reference's mat_write text form."""
+        _check(lib().ctc_model_write_text(self.h, mode, path.encode()))
+
+    def save(self, path: str):
+        """Exact binary checkpoint of all factors."""
+        _check(lib().ctc_model_save(self.h, path.encode()))
+
+    @classmethod
+    def load(cls, path: str) -> "Model":
+        h = C.c_void_p()
+        _check(lib().ctc_model_load(path.encode(), C.byref(h)))
+        nm, r = C.c_int(), C.c_int()
+        d = (C.c_uint64 * 4)()
+        _check(lib().ctc_model_info(h, C.byref(nm), d, C.byref(r)))
+        m = cls.__new__(cls)
+        m.h = h
+        m.dims = [d[k] for k in range(nm.value)]
+        m.rank = r.value
+        return m
 
     def set_factors(self, Us):
         for m, U in enumerate(Us):

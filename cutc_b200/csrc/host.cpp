@@ -697,6 +697,85 @@ extern "C" int ctc_model_get(const ctc_model *m, int mode, double *rowmajor)
     });
 }
 
+// Text form of one factor matrix, as the reference's mat_write_file
+// (sgpu/io.c:565-591, row-first case): one row per line, every value
+// printed "%+0.8le " (the format, with its trailing space, kept alike so
+// that files compare with the reference's own output).
+extern "C" int ctc_model_write_text(const ctc_model *m, int mode, const char *path)
+{
+    return guarded([&] {
+        if (!m || mode < 0 || mode >= m->nmodes || !path) fail(CTC_E_ARG, "bad argument");
+        FILE *f = fopen(path, "w");
+        if (!f) fail(CTC_E_IO, "cannot open %s for writing", path);
+        const double *v = m->U[mode].data();
+        const uint64_t I = m->dims[mode];
+        const int R = m->rank;
+        std::string line;
+        char buf[40];
+        for (uint64_t i = 0; i < I; ++i) {
+            line.clear();
+            for (int j = 0; j < R; ++j) {
+                snprintf(buf, sizeof buf, "%+0.8le ", v[i * (uint64_t)R + j]);
+                line += buf;
+            }
+            line += '\n';
+            if (fwrite(line.data(), 1, line.size(), f) != line.size()) {
+                fclose(f);
+                fail(CTC_E_IO, "write to %s failed", path);
+            }
+        }
+        if (fclose(f) != 0) fail(CTC_E_IO, "closing %s failed", path);
+    });
+}
+
+// Exact binary checkpoint of a model (factors in FP64, bit for bit):
+//   "CTCM" | u32 version 1 | u32 nmodes | u32 rank | u64 dims[nmodes] |
+//   f64 rows of mode 0 (row-major) | ... | f64 rows of the last mode
+static const char kModelMagic[4] = {'C', 'T', 'C', 'M'};
+
+extern "C" int ctc_model_save(const ctc_model *m, const char *path)
+{
+    return guarded([&] {
+        if (!m || !path || m->nmodes < 1) fail(CTC_E_ARG, "bad argument");
+        FILE *f = fopen(path, "wb");
+        if (!f) fail(CTC_E_IO, "cannot open %s for writing", path);
+        const uint32_t hdr[3] = {1u, (uint32_t)m->nmodes, (uint32_t)m->rank};
+        bool ok = fwrite(kModelMagic, 1, 4, f) == 4 && fwrite(hdr, 4, 3, f) == 3 &&
+                  fwrite(m->dims, 8, (size_t)m->nmodes, f) == (size_t)m->nmodes;
+        for (int k = 0; ok && k < m->nmodes; ++k)
+            ok = fwrite(m->U[k].data(), 8, m->U[k].size(), f) == m->U[k].size();
+        if (fclose(f) != 0) ok = false;
+        if (!ok) fail(CTC_E_IO, "write to %s failed", path);
+    });
+}
+
+extern "C" int ctc_model_load(const char *path, ctc_model **out)
+{
+    return guarded([&] {
+        if (!path || !out) fail(CTC_E_ARG, "null argument");
+        FILE *f = fopen(path, "rb");
+        if (!f) fail(CTC_E_IO, "cannot open %s", path);
+        std::unique_ptr<FILE, int (*)(FILE *)> guard(f, fclose);
+        char magic[4];
+        uint32_t hdr[3];
+        if (fread(magic, 1, 4, f) != 4 || memcmp(magic, kModelMagic, 4) != 0 || fread(hdr, 4, 3, f) != 3)
+            fail(CTC_E_IO, "%s is not a model checkpoint", path);
+        if (hdr[0] != 1u) fail(CTC_E_IO, "%s: checkpoint version %u", path, hdr[0]);
+        if (hdr[1] < 1 || hdr[1] > 4 || hdr[2] < 1 || hdr[2] > 4096) fail(CTC_E_IO, "%s: bad shape", path);
+        auto m = std::make_unique<ctc_model>();
+        m->nmodes = (int)hdr[1];
+        m->rank = (int)hdr[2];
+        if (fread(m->dims, 8, (size_t)m->nmodes, f) != (size_t)m->nmodes) fail(CTC_E_IO, "%s: truncated", path);
+        for (int k = 0; k < m->nmodes; ++k) {
+            if (m->dims[k] == 0 || m->dims[k] > ((uint64_t)1 << 40)) fail(CTC_E_IO, "%s: bad dimension", path);
+            m->U[k].resize(m->dims[k] * (uint64_t)m->rank);
+            if (fread(m->U[k].data(), 8, m->U[k].size(), f) != m->U[k].size())
+                fail(CTC_E_IO, "%s: truncated", path);
+        }
+        *out = m.release();
+    });
+}
+
 extern "C" int ctc_model_copy(const ctc_model *src, ctc_model *dst)
 {
     return guarded([&] {

@@ -31,7 +31,11 @@ static void usage()
             "  --compat                  reference kernel semantics\n"
             "  --no-early-stop           run all epochs\n"
             "  --seed S                  factor initialisation seed (default 0)\n"
-            "  --device D                CUDA device (default 0)\n");
+            "  --device D                CUDA device (default 0)\n"
+            "  --load-model F            start from the checkpoint F (ctc_model_save) instead of a seeded init\n"
+            "  --save-model F            write the final factors to checkpoint F\n"
+            "  --write-factors PREFIX    write the best-epoch factors as PREFIX1.txt .. PREFIX3.txt\n"
+            "                            (one row per line, the reference's mat_write format)\n");
 }
 
 static int check(int rc, const char *what)
@@ -61,6 +65,7 @@ int main(int argc, char **argv)
     int early = 1, device = 0;
     double lambda = NAN, lr = NAN, lr_scale = NAN, decay = NAN;
     unsigned long long seed = 0;
+    const char *load_path = nullptr, *save_path = nullptr, *factors_prefix = nullptr;
     for (int i = 6; i < argc; ++i) {
         std::string a = argv[i];
         auto next = [&]() -> const char * {
@@ -91,6 +96,9 @@ int main(int argc, char **argv)
         else if (a == "--no-early-stop") early = 0;
         else if (a == "--seed") seed = strtoull(next(), nullptr, 10);
         else if (a == "--device") device = atoi(next());
+        else if (a == "--load-model") load_path = next();
+        else if (a == "--save-model") save_path = next();
+        else if (a == "--write-factors") factors_prefix = next();
         else {
             usage();
             return 2;
@@ -128,14 +136,24 @@ int main(int argc, char **argv)
     ctc_ctx *ctx = nullptr;
     check(ctc_ctx_create(device, &ctx), "context");
     ctc_model *model = nullptr, *best = nullptr;
-    check(ctc_model_create(3, dims, rank, &model), "model");
+    if (load_path) {
+        check(ctc_model_load(load_path, &model), load_path);
+    } else {
+        check(ctc_model_create(3, dims, rank, &model), "model");
+        check(ctc_model_init_uniform(model, seed, 1.0 / std::sqrt((double)rank)), "init");
+    }
     check(ctc_model_create(3, dims, rank, &best), "model");
-    check(ctc_model_init_uniform(model, seed, 1.0 / std::sqrt((double)rank)), "init");
     const ctc_tensor *train[3] = {t[0], t[1], t[2]};
     ctc_result res;
     check(ctc_run(ctx, train, t[3], t[4], model, best, &p, print_epoch, nullptr, &res), "run");
     printf("best epoch %d  best RMSE-vl %0.5e  final RMSE-te %0.5e  update time %.3f ms\n", res.best_epoch,
            res.best_rmse, res.final_rmse_te, res.total_ms);
+    if (save_path) check(ctc_model_save(model, save_path), save_path);
+    if (factors_prefix)
+        for (int m = 0; m < 3; ++m) {
+            const std::string f = std::string(factors_prefix) + std::to_string(m + 1) + ".txt";
+            check(ctc_model_write_text(best, m, f.c_str()), f.c_str());
+        }
     ctc_model_free(model);
     ctc_model_free(best);
     for (int k = 0; k < 5; ++k) ctc_tensor_free(t[k]);

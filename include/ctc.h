@@ -134,6 +134,14 @@ int ctc_model_create(int nmodes, const uint64_t *dims, int rank, ctc_model **out
 int ctc_model_init_uniform(ctc_model *m, uint64_t seed, double scale);
 int ctc_model_set(ctc_model *m, int mode, const double *rowmajor);
 int ctc_model_get(const ctc_model *m, int mode, double *rowmajor);
+/* Factor output and checkpoints.  write_text: factor `mode` (0-based) as the
+ * reference's mat_write (sgpu/io.c:554-591, unused by its drivers): one row
+ * per line, each value "%+0.8le ".  save / load: an exact binary checkpoint
+ * of all factors (FP64 bits), to resume a run with ctc_run or a dataset;
+ * load allocates the model (free with ctc_model_free). */
+int ctc_model_write_text(const ctc_model *m, int mode, const char *path);
+int ctc_model_save(const ctc_model *m, const char *path);
+int ctc_model_load(const char *path, ctc_model **out);
 int ctc_model_copy(const ctc_model *src, ctc_model *dst);
 int ctc_model_info(const ctc_model *m, int *nmodes, uint64_t *dims, int *rank);
 int ctc_model_free(ctc_model *m);

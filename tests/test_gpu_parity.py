@@ -338,3 +338,19 @@ def test_rejects_bad_input(ctx):
     assert e.value.code == -1
     with pytest.raises(ctc.CtcError):
         ctc.run(ctx, [t], None, None, m, ctc.params("als", rank=12, iters=1))
+
+
+def test_checkpoint_resume_is_exact(ctx, tmp_path):
+    """Two ALS iterations straight equal one iteration, a checkpoint
+    (ctc_model_save / ctc_model_load) and one more iteration, bit for bit."""
+    P = Problem(20000, (200, 150, 100), 16, seed=71)
+    lam = {"lambda": 0.05}
+    G2, _ = engine_run(ctx, P, ctc.ALS, 2, precision=ctc.PREC_F32, **lam)
+    m = P.c_model()
+    ctc.run(ctx, P.c_sorted(), None, P.c_test(), m, ctc.params(ctc.ALS, rank=16, iters=1, early_stop=0, **lam))
+    path = str(tmp_path / "ck.ctcm")
+    m.save(path)
+    m2 = ctc.Model.load(path)
+    ctc.run(ctx, P.c_sorted(), None, P.c_test(), m2, ctc.params(ctc.ALS, rank=16, iters=1, early_stop=0, **lam))
+    for a, b in zip(m2.factors(), G2):
+        assert np.array_equal(a, b)

@@ -208,3 +208,58 @@ def test_compat_weights_rules():
     K = 9 + 21  # continuation lanes: 1..9 (row 2) and 11..31 (row 3)
     assert np.all(w[42:63] == 1)
     assert w[63] == 1 + (K - (31 - 10))
+
+
+# ------------------------------------------------------------------ factor files
+def _ref_mat_write(U, path):
+    """The reference's own mat_write (sgpu/io.c:554-591, built from its
+    sources into oracle/_ref) on a row-first ordi_matrix."""
+    import ctypes as C
+
+    class OrdiMatrix(C.Structure):
+        _fields_ = [("I", C.c_uint64), ("J", C.c_uint64), ("values", C.POINTER(C.c_double)),
+                    ("row_col_flag", C.c_int)]
+
+    lib = C.CDLL(os.path.join(po.REF_DIR, "libref_host.so"))
+    lib.mat_write.argtypes = [C.POINTER(OrdiMatrix), C.c_char_p]
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    m = OrdiMatrix(U.shape[0], U.shape[1], U.ctypes.data_as(C.POINTER(C.c_double)), 1)
+    lib.mat_write(C.byref(m), path.encode())
+
+
+@pytest.mark.skipif(not po.ref_host_available(), reason="reference host code not built")
+def test_factor_text_matches_reference_mat_write(tmp_path):
+    rng = np.random.default_rng(4)
+    m = ctc.Model([7, 5, 3], 8)
+    U = [rng.standard_normal((d, 8)) * 10.0 ** rng.integers(-5, 5, (d, 8)) for d in (7, 5, 3)]
+    U[0][0, 0] = 0.0
+    U[0][0, 1] = -0.0
+    m.set_factors(U)
+    for mode in range(3):
+        ours, ref = str(tmp_path / f"ours{mode}.txt"), str(tmp_path / f"ref{mode}.txt")
+        m.write_text(mode, ours)
+        _ref_mat_write(U[mode], ref)
+        assert open(ours, "rb").read() == open(ref, "rb").read()
+
+
+def test_model_checkpoint_round_trip_and_rejects_bad_files(tmp_path):
+    rng = np.random.default_rng(5)
+    for dims in ([11, 7, 5], [6, 5, 4, 3]):
+        m = ctc.Model(dims, 16)
+        U = [rng.standard_normal((d, 16)) for d in dims]
+        U[0][1, 2] = np.nextafter(1.0, 2.0)
+        m.set_factors(U)
+        p = str(tmp_path / "m.ctcm")
+        m.save(p)
+        q = ctc.Model.load(p)
+        assert q.dims == dims and q.rank == 16
+        for a, b in zip(q.factors(), U):
+            assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    bad = tmp_path / "bad.ctcm"
+    bad.write_bytes(b"NOPE" + b"\0" * 64)
+    with pytest.raises(ctc.CtcError):
+        ctc.Model.load(str(bad))
+    raw = open(p, "rb").read()
+    (tmp_path / "short.ctcm").write_bytes(raw[: len(raw) // 2])
+    with pytest.raises(ctc.CtcError):
+        ctc.Model.load(str(tmp_path / "short.ctcm"))
