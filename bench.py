@@ -520,16 +520,21 @@ def time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, seed):
 
 def ciss_build_times(ctc, ctx, t0):
     """The reference's CISS layout (tile length 32, mode 1) of the mode-1
-    training copy: host builder against the device builder (host tensor in,
-    host CISS out, transfers and the export to numpy included in both)."""
+    training copy, built by the host builder and by the device builder
+    through the C ABI (host tensor in, host CISS object out: the device
+    build includes its transfers); the export to numpy is not timed."""
+    import ctypes as C
+    L = ctc.lib()
     res = {}
-    for name, fn in (("host_s", lambda: ctc.ciss_alloc(t0, 1, 32)),
-                     ("gpu_s", lambda: ctc.ciss_alloc_gpu(ctx, t0, 1, 32))):
+    for name, build in (("host_s", lambda h: L.ctc_ciss_build(t0.h, 1, 32, C.byref(h))),
+                        ("gpu_s", lambda h: L.ctc_ciss_build_gpu(ctx.h, t0.h, 1, 32, 0, C.byref(h)))):
+        h = C.c_void_p()
         t = time.perf_counter()
-        c = fn()
+        rc = build(h)
         res[name] = time.perf_counter() - t
-        res["entries_bytes"] = int(c["entries"].nbytes)
-        del c
+        if rc != 0:
+            raise RuntimeError(f"CISS build failed ({rc})")
+        L.ctc_ciss_free(h)
     return res
 
 
