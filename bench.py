@@ -353,6 +353,7 @@ def run_ours(args):
                                          f"{s:.2f} s per step"}
     elif not args.no_extras:
         out["e2e"] = None
+    out["sse_kernel"] = sse_roofline(ctx, ds_sgd, n_train, n_test, mdims, R, peak)
     ds_ccd.free()
     ds_sgd.free()
     del tr, te
@@ -516,6 +517,26 @@ def time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, seed):
         res[name] = {"epochs": iters, "final_test_rmse": final, "final_train_rmse": hist[-1][2],
                      "target_test_rmse": target, "time_to_target_s": reach, "total_s": hist[-1][0]}
     return res
+
+
+def sse_roofline(ctx, ds, n_train, n_test, mdims, R, peak):
+    """The per-nonzero residual / squared-error kernel (k_sse) over the
+    training copy and the test tensor of the SGD dataset (one evaluation):
+    algorithmic bytes = 16 B per nonzero + one read of the three factors,
+    per launch, over its event-timed duration."""
+    ds.evaluate()  # warm
+    ctx.set_profiling(True)
+    ctx.reset_kernel_times()
+    for _ in range(3):
+        ds.evaluate()
+    n, ms = ctx.kernel_time("k_sse")
+    ctx.set_profiling(False)
+    fac = sum(mdims) * R * 4
+    nbytes = B_NZ * (n_train + n_test) + 2 * fac
+    per_eval_ms = ms / 3.0
+    gbps = nbytes / (per_eval_ms / 1000.0) / 1e9
+    return {"kernel": "k_sse", "launches_per_eval": n // 3, "ms_per_eval": per_eval_ms,
+            "algorithmic_bytes_per_eval": nbytes, "achieved_GBps": gbps, "frac_hbm": gbps / peak}
 
 
 def ciss_build_times(ctc, ctx, t0):
