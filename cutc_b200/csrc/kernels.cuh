@@ -100,35 +100,71 @@ __device__ __forceinline__ double block_sum(double v)
 }
 
 // ---------------------------------------------------------------------
-// Squared error (the residual/RMSE kernel).  Thread per nonzero, rows of
-// the row-major factors read with 16-byte vector loads.  Per-block double
-// partials; k_sum_partials folds them in a fixed order.
+// Squared error (the residual/RMSE kernel).  A warp takes 32 consecutive
+// nonzeros with one coalesced 512-byte load of their records, then walks
+// them GPW at a time: a group of GL = R / VN lanes per nonzero, lane gl
+// reading the 16-byte slice gl of each of the three factor rows, so one
+// warp load covers whole 64/128-byte rows instead of 32 scattered slices.
+// The group's partial products meet in a butterfly; lane 0 of the group
+// adds e^2 to its double accumulator.  Per-block double partials, folded
+// in a fixed order afterwards, keep the result deterministic.
 // ---------------------------------------------------------------------
+template <typename T, int R>
+__device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const double *__restrict__ v64,
+                                           uint64_t first, uint64_t end, uint64_t stride,
+                                           const T *__restrict__ U0, const T *__restrict__ U1,
+                                           const T *__restrict__ U2)
+{
+    using V = typename Vec<T>::type;
+    constexpr int VN = Vec<T>::n;
+    constexpr int GL = R / VN;
+    constexpr int GPW = 32 / GL;
+    static_assert(GL >= 1 && 32 % GL == 0, "lanes per nonzero");
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % GL, gw = lane / GL;
+    double acc = 0;
+    for (uint64_t base = first; base < end; base += stride) {
+        const uint64_t mine = base + lane;
+        uint4 r = make_uint4(0u, 0u, 0u, 0u);  // row 0 for the tail: in bounds, result unused
+        T x = 0;
+        if (mine < end) {
+            r = rec[mine];
+            x = value_of<T>(r, v64, mine);
+        }
+        const uint64_t cnt = end - base;
+#pragma unroll 4
+        for (int j = 0; j < GL; ++j) {
+            const int src = j * GPW + gw;
+            const uint32_t i0 = __shfl_sync(0xffffffffu, r.x, src);
+            const uint32_t i1 = __shfl_sync(0xffffffffu, r.y, src);
+            const uint32_t i2 = __shfl_sync(0xffffffffu, r.z, src);
+            const T xv = __shfl_sync(0xffffffffu, x, src);
+            const V va = reinterpret_cast<const V *>(U0 + (size_t)i0 * R)[gl];
+            const V vb = reinterpret_cast<const V *>(U1 + (size_t)i1 * R)[gl];
+            const V vc = reinterpret_cast<const V *>(U2 + (size_t)i2 * R)[gl];
+            T p = 0;
+#pragma unroll
+            for (int v = 0; v < VN; ++v) p += vget(va, v) * vget(vb, v) * vget(vc, v);
+#pragma unroll
+            for (int o = GL / 2; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+            if (gl == 0 && (uint64_t)src < cnt) {
+                const T e = xv - p;
+                acc += (double)e * (double)e;
+            }
+        }
+    }
+    return acc;
+}
+
 template <typename T, int R>
 __global__ void __launch_bounds__(256) k_sse(const uint4 *__restrict__ rec,
                                              const double *__restrict__ v64, uint32_t n,
                                              const T *__restrict__ U0, const T *__restrict__ U1,
                                              const T *__restrict__ U2, double *__restrict__ partial)
 {
-    using V = typename Vec<T>::type;
-    constexpr int VN = Vec<T>::n;
-    double acc = 0;
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
-        const uint4 r = rec[idx];
-        const T x = value_of<T>(r, v64, idx);
-        const V *a = reinterpret_cast<const V *>(U0 + (size_t)r.x * R);
-        const V *b = reinterpret_cast<const V *>(U1 + (size_t)r.y * R);
-        const V *c = reinterpret_cast<const V *>(U2 + (size_t)r.z * R);
-        T p = 0;
-#pragma unroll
-        for (int q = 0; q < R / VN; ++q) {
-            const V va = a[q], vb = b[q], vc = c[q];
-#pragma unroll
-            for (int v = 0; v < VN; ++v) p += vget(va, v) * vget(vb, v) * vget(vc, v);
-        }
-        const T e = x - p;
-        acc += (double)e * (double)e;
-    }
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    double acc = sse_span<T, R>(rec, v64, warp * 32, n, nwarps * 32, U0, U1, U2);
     acc = block_sum(acc);
     if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
@@ -142,27 +178,10 @@ __global__ void __launch_bounds__(256) k_sse_chunks(const uint4 *__restrict__ re
                                                     const T *__restrict__ U0, const T *__restrict__ U1,
                                                     const T *__restrict__ U2, double *__restrict__ partial)
 {
-    using V = typename Vec<T>::type;
-    constexpr int VN = Vec<T>::n;
+    const uint64_t w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (uint32_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
         const uint4 ch = chunks[c];
-        double acc = 0;
-        for (uint32_t idx = ch.x + threadIdx.x; idx < ch.y; idx += blockDim.x) {
-            const uint4 r = rec[idx];
-            const T x = value_of<T>(r, v64, idx);
-            const V *a = reinterpret_cast<const V *>(U0 + (size_t)r.x * R);
-            const V *b = reinterpret_cast<const V *>(U1 + (size_t)r.y * R);
-            const V *cc = reinterpret_cast<const V *>(U2 + (size_t)r.z * R);
-            T pr = 0;
-#pragma unroll
-            for (int q = 0; q < R / VN; ++q) {
-                const V va = a[q], vb = b[q], vc = cc[q];
-#pragma unroll
-                for (int v = 0; v < VN; ++v) pr += vget(va, v) * vget(vb, v) * vget(vc, v);
-            }
-            const T e = x - pr;
-            acc += (double)e * (double)e;
-        }
+        double acc = sse_span<T, R>(rec, v64, ch.x + w * 32, ch.y, nw * 32, U0, U1, U2);
         acc = block_sum(acc);
         if (threadIdx.x == 0) partial[c] = acc;
         __syncthreads();  // block_sum's shared slots are reused by the next chunk
