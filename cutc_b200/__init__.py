@@ -9,11 +9,12 @@ bindings (api.py).
 from .api import (ALS, CCD, CCDPP, SGD, PREC_F32, PREC_F64, PREC_MIXED, LR_BOLD_DRIVER,
                   LR_CONSTANT, LR_EXP_DECAY, SGD_HOGWILD, SGD_SEQUENTIAL, Batch, Context, CtcError,
                   Dataset, FirstOrder, Model, Params, Tensor, autotune, ciss_alloc, ciss_alloc_gpu, fo_params, grad, lib, params,
+                  plan_tiles,
                   rmse, run, tc_als,
                   tune_key, tune_lookup,
                   tc_ccd, tc_main_ciss, tc_sgd, tt_read)
 
 __all__ = ["ALS", "CCD", "CCDPP", "SGD", "PREC_F32", "PREC_F64", "PREC_MIXED", "LR_BOLD_DRIVER",
            "LR_CONSTANT", "LR_EXP_DECAY", "SGD_HOGWILD", "SGD_SEQUENTIAL", "Batch", "Context", "CtcError",
-           "Dataset", "FirstOrder", "Model", "Params", "Tensor", "autotune", "ciss_alloc", "ciss_alloc_gpu", "fo_params", "grad", "lib", "params", "rmse",
+           "Dataset", "FirstOrder", "Model", "Params", "Tensor", "autotune", "ciss_alloc", "ciss_alloc_gpu", "fo_params", "grad", "lib", "params", "plan_tiles", "rmse",
            "run", "tc_als", "tc_ccd", "tc_main_ciss", "tc_sgd", "tt_read", "tune_key", "tune_lookup"]

@@ -121,6 +121,8 @@ def lib():
             "ctc_ciss_sizes": (C.c_int, [P, _u64p, _u64p, _u64p, C.POINTER(C.c_int)]),
             "ctc_ciss_export": (C.c_int, [P, _u64p, _u64p, _f64p, C.POINTER(C.c_uint8)]),
             "ctc_ciss_free": (C.c_int, [P]),
+            "ctc_plan_tiles": (C.c_int, [_u64p, C.c_uint64, C.c_uint32, C.c_int, C.POINTER(C.c_int32), C.c_uint64,
+                                         _u64p, C.POINTER(C.c_uint32), C.c_uint64, _u64p]),
             "ctc_model_create": (C.c_int, [C.c_int, _u64p, C.c_int, C.POINTER(P)]),
             "ctc_model_init_uniform": (C.c_int, [P, C.c_uint64, C.c_double]),
             "ctc_model_set": (C.c_int, [P, C.c_int, _f64p]),
@@ -287,6 +289,22 @@ class Tensor:
             self.free()
         except Exception:
             pass
+
+
+def plan_tiles(ind, tile_len: int, from_runs: bool = False):
+    """Work tiles of a copy sorted for one mode (ind: that mode's 1-based
+    indices): (tiles n x 4 int32 {first, length, heavy or -1, piece},
+    heavy rows h x 4 uint32 {row, first tile, tiles, 0})."""
+    ind = np.ascontiguousarray(np.asarray(ind, dtype=np.uint64))
+    nt, nh = C.c_uint64(), C.c_uint64()
+    _check(lib().ctc_plan_tiles(ind.ctypes.data_as(_u64p), ind.size, tile_len, int(from_runs), None, 0,
+                                C.byref(nt), None, 0, C.byref(nh)))
+    tiles = np.zeros((nt.value, 4), dtype=np.int32)
+    heavy = np.zeros((nh.value, 4), dtype=np.uint32)
+    _check(lib().ctc_plan_tiles(ind.ctypes.data_as(_u64p), ind.size, tile_len, int(from_runs),
+                                tiles.ctypes.data_as(C.POINTER(C.c_int32)), nt.value, C.byref(nt),
+                                heavy.ctypes.data_as(C.POINTER(C.c_uint32)), nh.value, C.byref(nh)))
+    return tiles, heavy
 
 
 def ciss_alloc(t: Tensor, mode: int, tile_len: int = 32, ga: bool = False):

@@ -34,7 +34,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "--ex
            f"-I{INCLUDE}", f"-I{CSRC}", "-Xptxas", "-warn-spills"]
 
 HOST_SOURCES = ["host.cpp"]
-CUDA_SOURCES = ["engine.cu", "noalloc.cu", "fo.cu", "ciss_gpu.cu"]
+CUDA_SOURCES = ["engine.cu", "noalloc.cu", "fo.cu", "ciss_gpu.cu", "stage_gpu.cu"]
 HEADERS = ["ctc_internal.h", "kernels.cuh", "als_tc.cuh", "ptx.cuh", "runtime.cuh", "fo.cuh"]
 
 

@@ -6,6 +6,7 @@
 #include "runtime.cuh"
 #include "kernels.cuh"
 #include "als_tc.cuh"
+#include "stage_gpu.h"
 
 #include <cuda_runtime.h>
 
@@ -16,6 +17,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <type_traits>
@@ -23,6 +25,64 @@
 double ctc_value_through_idx(double v);
 
 namespace ctc {
+
+namespace {
+struct PoolSlot {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+};
+std::mutex g_pool_mu;
+PoolSlot g_pools[64];
+
+PoolSlot &pool_slot()
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) fail(CTC_E_UNSUP, "device %d: at most 64 devices", dev);
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    PoolSlot &s = g_pools[dev];
+    if (!s.pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        CK(cudaMemPoolCreate(&s.pool, &props));
+        uint64_t keep = ~0ull;
+        CK(cudaMemPoolSetAttribute(s.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        CK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+    }
+    return s;
+}
+}  // namespace
+
+void *dev_alloc(size_t bytes)
+{
+    PoolSlot &s = pool_slot();
+    void *p = nullptr;
+    CK(cudaMallocFromPoolAsync(&p, bytes, s.pool, s.stream));
+    CK(cudaStreamSynchronize(s.stream));
+    return p;
+}
+
+void dev_free(void *p) noexcept
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || !g_pools[dev].stream) {
+        cudaFree(p);
+        return;
+    }
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, g_pools[dev].stream);
+    cudaStreamSynchronize(g_pools[dev].stream);
+}
+
+void dev_pool_trim() noexcept
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    if (g_pools[dev].pool) cudaMemPoolTrimTo(g_pools[dev].pool, 0);
+}
 
 // One tensor staged on the device as 16-byte records (+ FP64 values in
 // FP64 runs), optionally with its row-aligned work tiles for one mode and
@@ -57,16 +117,16 @@ static int bits_for(uint64_t d)
     return b;
 }
 
-// CCD++ copy of mode m: 64-bit keys row | q1 | q2 (row = index in mode m,
-// q1/q2 = indices in modes m+1, m+2, each in just enough bits) and the
-// values; the residual is formed on the device.
-// CCD++ copy of mode m: packed keys (row | q1 | q2) and values in the
-// tile slots of `plan` (slot length S = 32 * E): entry p of tile t sits at
-// t*S + (p % E)*32 + p / E, so that lane p / E of the warp owning the tile
-// holds its E consecutive entries and every warp load is coalesced.
-// Unused slot entries hold kPadKey, value 0 and residual 0.
+// CCD++ copy of mode m: packed 64-bit keys row | q1 | q2 (row = index in
+// mode m, q1/q2 = indices in modes m+1, m+2, each in just enough bits) and
+// values in the tile slots of `plan` (slot length S = 32 * E): entry p of
+// tile t sits at t*S + (p % E)*32 + p / E, so that lane p / E of the warp
+// owning the tile holds its E consecutive entries and every warp load is
+// coalesced.  Unused slot entries hold kPadKey, value 0 and residual 0.
+// The slots are gathered on the device from records in mode-m order
+// (rec, or rec through perm); the residual is formed on the device.
 template <typename T>
-static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t *dims, bool trunc,
+static void stage_keys(ctc_ctx *ctx, const DevTensor<T> &src, const uint32_t *perm, int m, const uint64_t *dims,
                        const TilePlan &plan, int E, DevTensor<T> &d)
 {
     const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
@@ -76,35 +136,17 @@ static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t 
     d.ks.s_q1 = (uint32_t)b2;
     d.ks.m_q1 = (b1 == 64) ? ~0ull : ((1ull << b1) - 1);
     d.ks.m_q2 = (b2 == 64) ? ~0ull : ((1ull << b2) - 1);
+    int eshift = 0;
+    while ((1 << eshift) < E) ++eshift;
+    if ((1 << eshift) != E) fail(CTC_E_ARG, "CCD++ lanes per tile must be a power of two");
     const uint64_t S = 32ull * (uint64_t)E;
     const uint64_t ntiles = plan.ntiles();
     const uint64_t nslots = ntiles * S;
     if (nslots >= 0xfffffff0ull) fail(CTC_E_UNSUP, "CCD++: more than 2^32 slot entries");
-    const uint32_t s_row = d.ks.s_row, s_q1 = d.ks.s_q1;
-    const uint64_t *im = t->ind[m].data(), *im1 = t->ind[m1].data(), *im2 = t->ind[m2].data();
-    const double *vals = t->vals.data();
-    // slot s: tile s / S, lane (s % S) % 32, step (s % S) / 32, i.e. entry
-    // lane * E + step of the tile (or a pad past its length)
-    auto source = [&](uint64_t sidx) -> int64_t {
-        const uint64_t tt = sidx / S, o = sidx % S;
-        const uint64_t q = (o % 32) * (uint64_t)E + o / 32;
-        if (q >= (uint64_t)plan.tiles[4 * tt + 1]) return -1;
-        return (int64_t)((uint64_t)plan.tiles[4 * tt] + q);
-    };
     d.keys.alloc(nslots);
-    upload_filled(ctx, d.keys.p, nslots, [&](uint64_t b, uint64_t e, uint64_t *h) {
-        for (uint64_t sidx = b; sidx < e; ++sidx) {
-            const int64_t i = source(sidx);
-            h[sidx - b] = i < 0 ? k::kPadKey : ((im[i] - 1) << s_row) | ((im1[i] - 1) << s_q1) | (im2[i] - 1);
-        }
-    });
     d.x.alloc(nslots);
-    upload_filled(ctx, d.x.p, nslots, [&](uint64_t b, uint64_t e, T *h) {
-        for (uint64_t sidx = b; sidx < e; ++sidx) {
-            const int64_t i = source(sidx);
-            h[sidx - b] = i < 0 ? T(0) : (T)(trunc ? ctc_value_through_idx(vals[i]) : vals[i]);
-        }
-    });
+    dev_fill_slots<T>(ctx, src.rec.p, sizeof(T) == 8 ? src.v64.p : nullptr, perm, m, d.tiles.p, nslots, eshift,
+                      d.ks.s_row, d.ks.s_q1, d.keys.p, d.x.p);
     // warp tasks: a light tile, or up to kCcdppGroup consecutive pieces of a
     // long row; the long-row table becomes {row, first group, groups, 0}
     std::vector<int32_t> tasks;
@@ -130,7 +172,7 @@ static void stage_keys(ctc_ctx *ctx, const ctc_tensor *t, int m, const uint64_t 
     d.ntasks = (uint32_t)(tasks.size() / 4);
     d.tasks.upload(reinterpret_cast<const int4 *>(tasks.data()), d.ntasks, ctx->stream);
     d.heavy.upload(reinterpret_cast<const uint4 *>(hv.data()), hv.size() / 4, ctx->stream);
-    d.n = (uint32_t)t->nnz;
+    d.n = src.n;
     d.nslots = (uint32_t)nslots;
     d.res.alloc(nslots);
     CK(cudaMemsetAsync(d.res.p, 0, nslots * sizeof(T), ctx->stream));
@@ -143,7 +185,9 @@ static int ccdpp_lanes(int tile_len)
     return tile_len <= 128 ? 4 : (tile_len <= 256 ? 8 : 16);
 }
 
-static void validate_tensor(const ctc_tensor *t, const uint64_t *dims, const char *what)
+// Order, size and dimension checks; the staging pass that reads the
+// indices (stage_tensor with check dims) checks their range.
+static void check_shape(const ctc_tensor *t, const uint64_t *dims, const char *what)
 {
     if (!t) fail(CTC_E_ARG, "%s: null tensor", what);
     if (t->nmodes != 3) fail(CTC_E_UNSUP, "%s: only order-3 tensors are supported (got %d)", what, t->nmodes);
@@ -152,6 +196,11 @@ static void validate_tensor(const ctc_tensor *t, const uint64_t *dims, const cha
     for (int m = 0; m < 3; ++m)
         if (dims[m] == 0 || dims[m] >= 0xfffffff0ull)
             fail(CTC_E_UNSUP, "%s: bad dimension %llu", what, (unsigned long long)dims[m]);
+}
+
+static void validate_tensor(const ctc_tensor *t, const uint64_t *dims, const char *what)
+{
+    check_shape(t, dims, what);
     std::atomic<int> bad{0};
     par_for(t->nnz, [&](uint64_t b, uint64_t e) {
         for (int m = 0; m < 3; ++m) {
@@ -166,24 +215,38 @@ static void validate_tensor(const ctc_tensor *t, const uint64_t *dims, const cha
     if (bad) fail(CTC_E_ARG, "%s: indices must be 1-based and within the model dimensions", what);
 }
 
+// check: when given, every index is checked against these dimensions in
+// the same pass (failing with `what` in the message before any kernel
+// reads the records).
 template <typename T>
-static void stage_tensor(ctc_ctx *ctx, const ctc_tensor *t, bool trunc, DevTensor<T> &d)
+static void stage_tensor(ctc_ctx *ctx, const ctc_tensor *t, bool trunc, DevTensor<T> &d,
+                         const uint64_t *check = nullptr, const char *what = "tensor")
 {
     const uint64_t n = t->nnz;
     d.n = (uint32_t)n;
     d.rec.alloc(n);
     const uint64_t *i0 = t->ind[0].data(), *i1 = t->ind[1].data(), *i2 = t->ind[2].data();
     const double *vals = t->vals.data();
+    const uint64_t c0 = check ? check[0] : ~0ull, c1 = check ? check[1] : ~0ull, c2 = check ? check[2] : ~0ull;
+    std::atomic<int> bad{0};
     upload_filled(ctx, d.rec.p, n, [&](uint64_t b, uint64_t e, uint4 *h) {
+        bool oob = false;
         for (uint64_t i = b; i < e; ++i) {
             double v = vals[i];
             if (trunc) v = ctc_value_through_idx(v);
             const float vf = (float)v;
             uint32_t bits;
             memcpy(&bits, &vf, 4);
-            h[i - b] = make_uint4((uint32_t)(i0[i] - 1), (uint32_t)(i1[i] - 1), (uint32_t)(i2[i] - 1), bits);
+            const uint64_t a0 = i0[i] - 1, a1 = i1[i] - 1, a2 = i2[i] - 1;
+            oob |= (a0 >= c0) | (a1 >= c1) | (a2 >= c2);
+            h[i - b] = make_uint4((uint32_t)a0, (uint32_t)a1, (uint32_t)a2, bits);
         }
+        if (oob) bad = 1;
     });
+    if (check) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (bad) fail(CTC_E_ARG, "%s: indices must be 1-based and within the model dimensions", what);
+    }
     if (std::is_same<T, double>::value) {
         d.v64.alloc(n);
         upload_filled(ctx, d.v64.p, n, [&](uint64_t b, uint64_t e, double *h) {
@@ -194,24 +257,25 @@ static void stage_tensor(ctc_ctx *ctx, const ctc_tensor *t, bool trunc, DevTenso
 }
 
 template <typename T>
+static void upload_plan(ctc_ctx *ctx, const TilePlan &p, int mode, DevTensor<T> &d);
+
+// host planner over the copy's index array (the compat ALS / CCD path)
+template <typename T>
 static TilePlan stage_plan(ctc_ctx *ctx, const ctc_tensor *t, int mode, uint32_t tile_len, DevTensor<T> &d)
 {
     const uint64_t n = t->nnz;
-    std::unique_ptr<uint32_t[]> rows(new uint32_t[std::max<uint64_t>(n, 1)]);  // filled in parallel
-    par_for(n, [&](uint64_t b, uint64_t e) {
-        for (uint64_t i = b; i < e; ++i) rows[i] = (uint32_t)(t->ind[mode][i] - 1);
-    });
-    std::atomic<int> unsorted{0};
-    par_for(n > 0 ? n - 1 : 0, [&](uint64_t b, uint64_t e) {
-        for (uint64_t i = b + 1; i <= e; ++i)
-            if (rows[i] < rows[i - 1]) {
-                unsorted = 1;
-                return;
-            }
-    });
-    if (unsorted) fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", mode + 1, mode + 1);
     if (n >= 0x7fffffffull) fail(CTC_E_UNSUP, "tile plans index at most 2^31 - 1 nonzeros");
-    TilePlan p = plan_tiles_chunked(rows.get(), n, tile_len);
+    bool unsorted = false;
+    TilePlan p = plan_tiles_chunked(t->ind[mode].data(), n, tile_len, &unsorted);
+    if (unsorted) fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", mode + 1, mode + 1);
+    upload_plan(ctx, p, mode, d);
+    return p;
+}
+
+// the plan's tiles, long rows and piece list on the device
+template <typename T>
+static void upload_plan(ctc_ctx *ctx, const TilePlan &p, int mode, DevTensor<T> &d)
+{
     d.mode = mode;
     d.ntiles = p.ntiles();
     d.nheavy = p.nheavy();
@@ -223,7 +287,6 @@ static TilePlan stage_plan(ctc_ctx *ctx, const ctc_tensor *t, int mode, uint32_t
     d.npieces = (uint32_t)pieces.size();
     d.pieces.upload(pieces.data(), pieces.size(), ctx->stream);
     CK(cudaStreamSynchronize(ctx->stream));
-    return p;
 }
 
 template <typename T>
@@ -296,6 +359,73 @@ static int default_tile(int alg)
     }
 }
 
+// The three mode copies of ALS / CCD / CCD++ staged through the device:
+// the records of train[0] (mode-1 order) are uploaded once; copy m is the
+// caller's train[m] uploaded as records when given, else the stable
+// (mode m, mode m+1) order of train[0] sorted on the device (the order
+// ctc_tensor_sort gives).  The rows' run lengths come back to the host for
+// the tile plan (plan_tiles_runs: the plan of the host planner), and the
+// CCD++ slots or the record copy are gathered on the device.
+template <typename T>
+static void stage_copies_dev(ctc_ctx *ctx, const ctc_params &p, uint32_t tl, const ctc_tensor *const train[3],
+                             const uint64_t *dims, bool trunc, DatasetImpl<T> &impl)
+{
+    const uint64_t n = train[0]->nnz;
+    if (n >= 0x7fffffffull) fail(CTC_E_UNSUP, "tile plans index at most 2^31 - 1 nonzeros");
+    const bool ccdpp = p.alg == CTC_ALG_CCDPP;
+    DevTensor<T> base;
+    {
+        TracePhase tp("records + upload");
+        stage_tensor<T>(ctx, train[0], trunc, base, dims, "training tensor");
+    }
+    // copy 1 last: it can take over the base records (ALS / CCD)
+    for (int m : {1, 2, 0}) {
+        DevTensor<T> given;
+        const DevTensor<T> *src = &base;
+        DevBuf<uint32_t> perm;
+        if (m > 0 && train[m]) {
+            TracePhase tp("records + upload");
+            stage_tensor<T>(ctx, train[m], trunc, given, dims, "training tensor");
+            src = &given;
+        } else if (m > 0) {
+            TracePhase tp("device sort");
+            const int m1 = (m + 1) % 3;
+            perm.alloc(n);
+            dev_sort_order(ctx, base.rec.p, (uint32_t)n, m, bits_for(dims[m1]), bits_for(dims[m]) + bits_for(dims[m1]),
+                           perm.p);
+        }
+        const uint32_t *pp = perm.p;
+        DevTensor<T> &d = impl.copy[m];
+        TilePlan plan;
+        {
+            TracePhase tp("row runs + tile plan");
+            std::vector<uint32_t> rows, counts;
+            if (dev_row_runs(ctx, src->rec.p, pp, (uint32_t)n, m, rows, counts))
+                fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", m + 1, m + 1);
+            plan = plan_tiles_runs(rows.data(), counts.data(), rows.size(), tl);
+            upload_plan(ctx, plan, m, d);
+        }
+        if (ccdpp) {
+            TracePhase tp("CCD++ slots");
+            stage_keys<T>(ctx, *src, pp, m, dims, plan, (int)(tl / 32), d);
+            continue;
+        }
+        TracePhase tp("record copy");
+        d.n = (uint32_t)n;
+        if (pp) {
+            d.rec.alloc(n);
+            if (sizeof(T) == 8) d.v64.alloc(n);
+            dev_gather_records(ctx, base.rec.p, sizeof(T) == 8 ? base.v64.p : nullptr, pp, (uint32_t)n, d.rec.p,
+                               d.v64.p);
+            CK(cudaStreamSynchronize(ctx->stream));
+        } else {
+            DevTensor<T> &from = (m == 0) ? base : given;
+            d.rec.swap(from.rec);
+            d.v64.swap(from.v64);
+        }
+    }
+}
+
 template <typename T>
 static void build_dataset(ctc_dataset *ds, const ctc_tensor *const train[3], const ctc_tensor *val,
                           const ctc_tensor *test)
@@ -307,74 +437,49 @@ static void build_dataset(ctc_dataset *ds, const ctc_tensor *const train[3], con
     uint32_t tl = (uint32_t)(p.tile_len > 0 ? p.tile_len : default_tile(p.alg));
     // CCD++: tiles fill slots of 32*E entries
     if (p.alg == CTC_ALG_CCDPP) tl = 32u * (uint32_t)ccdpp_lanes((int)tl);
-    std::unique_ptr<ctc_tensor> own[3];
-    const ctc_tensor *srt[3] = {train[0], train[1], train[2]};
-    const int ncopies = (p.alg == CTC_ALG_SGD) ? 1 : 3;
-    for (int m = 0; m < ncopies; ++m) {
-        if (!srt[m]) {
-            own[m].reset(new ctc_tensor(*train[0]));
-            if (ctc_tensor_sort(own[m].get(), m) != CTC_OK) fail(CTC_E_ARG, "%s", ctc_last_error());
-            srt[m] = own[m].get();
+    for (int m = 0; m < 3; ++m)
+        if (train[m]) {
+            check_shape(train[m], ds->dims, "training tensor");
+            if (train[m]->nnz != train[0]->nnz) fail(CTC_E_ARG, "training copies differ in size");
         }
-        if (srt[m]->nnz != train[0]->nnz) fail(CTC_E_ARG, "training copies differ in size");
-        {
-            TracePhase tp("validate training copy");
-            validate_tensor(srt[m], ds->dims, "training tensor");
-        }
-        if (p.alg == CTC_ALG_CCDPP) {
-            TilePlan plan;
-            {
-                TracePhase tp("tile plan");
-                plan = stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
-            }
-            TracePhase tp("CCD++ slots + upload");
-            stage_keys<T>(ctx, srt[m], m, ds->dims, trunc, plan, (int)(tl / 32), impl->copy[m]);
-        } else {
-            {
-                TracePhase tp("records + upload");
-                stage_tensor<T>(ctx, srt[m], trunc, impl->copy[m]);
-            }
-            TracePhase tp("tile plan");
-            if (p.alg != CTC_ALG_SGD) stage_plan<T>(ctx, srt[m], m, tl, impl->copy[m]);
-        }
-        if (trunc && (p.alg == CTC_ALG_ALS || p.alg == CTC_ALG_CCD))
-            stage_weights<T>(ctx, srt[m], m, p.alg == CTC_ALG_CCD ? 1 : 0, impl->copy[m]);
-    }
     if (p.alg == CTC_ALG_SGD) {
+        {
+            TracePhase tp("records + upload");
+            stage_tensor<T>(ctx, train[0], trunc, impl->copy[0], ds->dims, "training tensor");
+        }
         // SGD tiles are plain chunks of the mode-1 order (sgpu/sgd.cu:32-34)
         impl->copy[0].mode = 0;
         impl->copy[0].ntiles = (uint32_t)((impl->copy[0].n + tl - 1) / tl);
         TracePhase tp("SGD row counts");
+        for (int m = 0; m < 3; ++m)
+            dev_row_counts(ctx, impl->copy[0].rec.p, impl->copy[0].n, m, (uint32_t)ds->dims[m], impl->rowcnt[m]);
+    } else if (trunc && (p.alg == CTC_ALG_ALS || p.alg == CTC_ALG_CCD)) {
+        // the reference's lane multiplicities come from the host CISS of
+        // every sorted copy, so these copies are sorted and planned on the host
+        std::unique_ptr<ctc_tensor> own[3];
         for (int m = 0; m < 3; ++m) {
-            // per-thread histograms, summed
-            const uint64_t d = ds->dims[m];
-            const uint64_t *ind = srt[0]->ind[m].data();
-            const int P = std::max(1, std::min(host_threads(), 64));
-            std::vector<std::vector<uint32_t>> part(P);
-            std::vector<std::thread> th;
-            for (int q = 0; q < P; ++q)
-                th.emplace_back([&, q] {
-                    part[q].assign(d, 0);
-                    const uint64_t b = srt[0]->nnz * q / P, e = srt[0]->nnz * (q + 1) / P;
-                    for (uint64_t i = b; i < e; ++i) part[q][ind[i] - 1]++;
-                });
-            for (auto &t : th) t.join();
-            impl->rowcnt[m].assign(d, 0);
-            par_for(d, [&](uint64_t b, uint64_t e) {
-                for (int q = 0; q < P; ++q)
-                    for (uint64_t r = b; r < e; ++r) impl->rowcnt[m][r] += part[q][r];
-            });
+            const ctc_tensor *t = train[m];
+            if (!t) {
+                own[m].reset(new ctc_tensor(*train[0]));
+                if (ctc_tensor_sort(own[m].get(), m) != CTC_OK) fail(CTC_E_ARG, "%s", ctc_last_error());
+                t = own[m].get();
+            }
+            stage_tensor<T>(ctx, t, trunc, impl->copy[m], ds->dims, "training tensor");
+            stage_plan<T>(ctx, t, m, tl, impl->copy[m]);
+            stage_weights<T>(ctx, t, m, p.alg == CTC_ALG_CCD ? 1 : 0, impl->copy[m]);
         }
+    } else {
+        stage_copies_dev<T>(ctx, p, tl, train, ds->dims, trunc, *impl);
     }
     if (val) {
         TracePhase tp("validation tensor");
-        validate_tensor(val, ds->dims, "validation tensor");
-        stage_tensor<T>(ctx, val, false, impl->val);
+        check_shape(val, ds->dims, "validation tensor");
+        stage_tensor<T>(ctx, val, false, impl->val, ds->dims, "validation tensor");
     }
     if (test) {
         TracePhase tp("test tensor");
-        validate_tensor(test, ds->dims, "test tensor");
-        stage_tensor<T>(ctx, test, false, impl->test);
+        check_shape(test, ds->dims, "test tensor");
+        stage_tensor<T>(ctx, test, false, impl->test, ds->dims, "test tensor");
     }
     ds->impl = std::move(impl);
 }
@@ -941,7 +1046,11 @@ static void run_loop(ctc_dataset *ds, SessionBase *S, ctc_model *model, ctc_mode
                      ctc_epoch_cb cb, void *user, ctc_result *res)
 {
     ctc_ctx *ctx = ds->ctx;
-    S->set_model(model);
+    {
+        TracePhase tp("set model");
+        S->set_model(model);
+    }
+    TracePhase tp_loop("epochs + evaluation");
     double lr_base = p.lr;
     const double scale = p.lr_scale > 0 ? p.lr_scale : 1.0;
     double best_rmse = 10000000.0;  // BEST_RMSE, sgpu/base.h:35
@@ -1002,6 +1111,7 @@ static void run_loop(ctc_dataset *ds, SessionBase *S, ctc_model *model, ctc_mode
         res->total_ms = total_ms;
         res->nonspd_rows = S->nonspd();
     }
+    TracePhase tp("get model");
     S->get_model(model, false);
     if (best) {
         if (best->nmodes != 3 || best->rank != model->rank) *best = *model;
@@ -1083,6 +1193,7 @@ extern "C" int ctc_ctx_destroy(ctc_ctx *ctx)
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+    dev_pool_trim();
     return CTC_OK;
 }
 
@@ -1215,8 +1326,12 @@ extern "C" int ctc_dataset_run(ctc_dataset *d, ctc_model *model, ctc_model *best
         check_model(d, model, p->rank);
         CK(cudaSetDevice(d->ctx->device));
         d->p = *p;
-        SessionBase *S = session_for(d, p->rank);
-        S->set_params(*p);
+        SessionBase *S;
+        {
+            TracePhase tp("session");
+            S = session_for(d, p->rank);
+            S->set_params(*p);
+        }
         run_loop(d, S, model, best, *p, cb, user, res);
     });
 }
@@ -1289,6 +1404,7 @@ extern "C" int ctc_run(ctc_ctx *ctx, const ctc_tensor *const train[3], const ctc
         }
     });
     if (rc == CTC_OK) rc = ctc_dataset_run(ds, model, best, p, cb, user, res);
+    TracePhase tp("free dataset");
     ctc_dataset_free(ds);
     return rc;
 }

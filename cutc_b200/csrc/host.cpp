@@ -369,14 +369,32 @@ void compat_weights(const ctc_ciss &c, int kernel, std::vector<double> &w)
 // ------------------------------------------------------------------
 // work tiles
 // ------------------------------------------------------------------
-TilePlan plan_tiles(const uint32_t *rows, uint64_t n, uint32_t T)
+// Rows of a mode-sorted copy read straight from its 1-based index array.
+// A row that is smaller than the one before it marks the copy unsorted.
+struct SortedRows {
+    const uint64_t *ind;
+    uint64_t n;
+    bool bad = false;
+    uint32_t operator()(uint64_t i) const { return (uint32_t)(ind[i] - 1); }
+    // end of the run of equal rows that starts at i
+    uint64_t run_end(uint64_t i)
+    {
+        const uint64_t r = ind[i];
+        uint64_t e = i + 1;
+        while (e < n && ind[e] == r) ++e;
+        if (e < n && ind[e] < r) bad = true;
+        return e;
+    }
+};
+
+static TilePlan plan_span(SortedRows rows, uint32_t T, bool *unsorted)
 {
+    const uint64_t n = rows.n;
     TilePlan p;
     p.tiles.reserve((size_t)(n / std::max<uint32_t>(T / 2, 1) + 16) * 4);
     uint64_t i = 0;
     while (i < n) {
-        uint64_t e = i + 1;
-        while (e < n && rows[e] == rows[i]) ++e;
+        uint64_t e = rows.run_end(i);
         uint64_t len = e - i;
         if (len > T) {
             uint32_t h = p.nheavy();
@@ -387,49 +405,63 @@ TilePlan plan_tiles(const uint32_t *rows, uint64_t n, uint32_t T)
                 p.tiles.insert(p.tiles.end(),
                                {(int32_t)s, (int32_t)std::min<uint64_t>(T, e - s), (int32_t)h, (int32_t)q});
             }
-            p.heavy_rows.insert(p.heavy_rows.end(), {rows[i], first, np, 0u});
+            p.heavy_rows.insert(p.heavy_rows.end(), {rows(i), first, np, 0u});
             i = e;
             continue;
         }
-        // pack whole light rows
+        // pack whole light rows (the run found above is the first of them)
         uint64_t s = i, size = 0;
         while (i < n) {
-            uint64_t ee = i + 1;
-            while (ee < n && rows[ee] == rows[i]) ++ee;
-            uint64_t l = ee - i;
+            const uint64_t ee = (i == s) ? e : rows.run_end(i);
+            const uint64_t l = ee - i;
             if (l > T || size + l > T) break;
             size += l;
             i = ee;
         }
         p.tiles.insert(p.tiles.end(), {(int32_t)s, (int32_t)size, -1, 0});
     }
+    if (rows.bad) *unsorted = true;
     return p;
 }
 
-// The same plan built over 64 row-aligned chunks in parallel (the chunk
-// count is fixed, so the plan does not depend on the host's core count);
-// light tiles do not straddle a chunk boundary.
-TilePlan plan_tiles_chunked(const uint32_t *rows, uint64_t n, uint32_t T)
+// Tiles of at most T nonzeros over a copy sorted by one mode (ind: that
+// mode's 1-based indices): whole light rows packed greedily, rows longer
+// than T split into pieces of T.  Built over 64 row-aligned chunks in
+// parallel (the chunk count is fixed, so the plan does not depend on the
+// host's core count); light tiles do not straddle a chunk boundary.
+// *unsorted is set when the indices decrease anywhere.
+TilePlan plan_tiles_chunked(const uint64_t *ind, uint64_t n, uint32_t T, bool *unsorted)
 {
     constexpr int K = 64;
-    if (n < ((uint64_t)1 << 20)) return plan_tiles(rows, n, T);
-    std::vector<uint64_t> cut(K + 1, 0);
-    cut[K] = n;
-    for (int c = 1; c < K; ++c) {
-        uint64_t x = std::max<uint64_t>(n * (uint64_t)c / K, cut[c - 1]);
-        while (x > 0 && x < n && rows[x] == rows[x - 1]) ++x;
+    *unsorted = false;
+    const int chunks = n < ((uint64_t)1 << 20) ? 1 : K;
+    std::vector<uint64_t> cut(chunks + 1, 0);
+    cut[chunks] = n;
+    for (int c = 1; c < chunks; ++c) {
+        uint64_t x = std::max<uint64_t>(n * (uint64_t)c / chunks, cut[c - 1]);
+        while (x > 0 && x < n && ind[x] == ind[x - 1]) ++x;
         cut[c] = x;
     }
-    std::vector<TilePlan> part(K);
+    for (int c = 1; c < chunks; ++c)
+        if (cut[c] > 0 && cut[c] < n && ind[cut[c]] < ind[cut[c] - 1]) *unsorted = true;
+    std::vector<TilePlan> part(chunks);
+    std::vector<char> bad(chunks, 0);
     {
-        const int P = std::max(1, std::min(host_threads(), K));
+        const int P = std::max(1, std::min(host_threads(), chunks));
         std::vector<std::thread> th;
         for (int q = 0; q < P; ++q)
             th.emplace_back([&, q] {
-                for (int c = q; c < K; c += P) part[c] = plan_tiles(rows + cut[c], cut[c + 1] - cut[c], T);
+                for (int c = q; c < chunks; c += P) {
+                    bool b = false;
+                    part[c] = plan_span(SortedRows{ind + cut[c], cut[c + 1] - cut[c]}, T, &b);
+                    bad[c] = b;
+                }
             });
         for (auto &t : th) t.join();
     }
+    for (char b : bad)
+        if (b) *unsorted = true;
+    if (chunks == 1) return std::move(part[0]);
     TilePlan p;
     size_t nt = 0, nh = 0;
     for (const TilePlan &q : part) {
@@ -438,7 +470,7 @@ TilePlan plan_tiles_chunked(const uint32_t *rows, uint64_t n, uint32_t T)
     }
     p.tiles.reserve(nt);
     p.heavy_rows.reserve(nh);
-    for (int c = 0; c < K; ++c) {
+    for (int c = 0; c < chunks; ++c) {
         const uint32_t tbase = p.ntiles(), hbase = p.nheavy();
         const TilePlan &q = part[c];
         for (size_t t = 0; t < q.tiles.size(); t += 4) {
@@ -449,6 +481,58 @@ TilePlan plan_tiles_chunked(const uint32_t *rows, uint64_t n, uint32_t T)
         for (size_t h = 0; h < q.heavy_rows.size(); h += 4)
             p.heavy_rows.insert(p.heavy_rows.end(), {q.heavy_rows[h], q.heavy_rows[h + 1] + tbase,
                                                      q.heavy_rows[h + 2], q.heavy_rows[h + 3]});
+    }
+    return p;
+}
+
+// The plan of plan_tiles_chunked from the copy's row runs (run r: row
+// rows[r] repeated counts[r] times, in order): the chunk cut c is the first
+// run start at or after n*c/64 (a cut never precedes the one before it),
+// light tiles end at a cut, and tiles / heavy rows are numbered in order,
+// so the two builders give the same plan.  O(runs + tiles).
+TilePlan plan_tiles_runs(const uint32_t *rows, const uint32_t *counts, uint64_t nruns, uint32_t T)
+{
+    std::vector<uint64_t> start(nruns + 1, 0);
+    for (uint64_t r = 0; r < nruns; ++r) start[r + 1] = start[r] + counts[r];
+    const uint64_t n = start[nruns];
+    constexpr int K = 64;
+    const int chunks = n < ((uint64_t)1 << 20) ? 1 : K;
+    std::vector<uint64_t> cut(chunks + 1, 0);  // in runs
+    cut[chunks] = nruns;
+    for (int c = 1; c < chunks; ++c) {
+        const uint64_t x = std::max<uint64_t>(n * (uint64_t)c / chunks, start[cut[c - 1]]);
+        cut[c] = (uint64_t)(std::lower_bound(start.begin(), start.end(), x) - start.begin());
+    }
+    TilePlan p;
+    p.tiles.reserve((size_t)(n / std::max<uint32_t>(T / 2, 1) + 16) * 4);
+    for (int c = 0; c < chunks; ++c) {
+        uint64_t r = cut[c];
+        const uint64_t rend = cut[c + 1];
+        while (r < rend) {
+            const uint64_t len = counts[r];
+            if (len > T) {
+                const uint32_t h = p.nheavy(), first = p.ntiles();
+                const uint32_t np = (uint32_t)((len + T - 1) / T);
+                const uint64_t s0 = start[r], e = s0 + len;
+                for (uint32_t q = 0; q < np; ++q) {
+                    const uint64_t s = s0 + (uint64_t)q * T;
+                    p.tiles.insert(p.tiles.end(),
+                                   {(int32_t)s, (int32_t)std::min<uint64_t>(T, e - s), (int32_t)h, (int32_t)q});
+                }
+                p.heavy_rows.insert(p.heavy_rows.end(), {rows[r], first, np, 0u});
+                ++r;
+                continue;
+            }
+            const uint64_t s = start[r];
+            uint64_t size = 0;
+            while (r < rend) {
+                const uint64_t l = counts[r];
+                if (l > T || size + l > T) break;
+                size += l;
+                ++r;
+            }
+            p.tiles.insert(p.tiles.end(), {(int32_t)s, (int32_t)size, -1, 0});
+        }
     }
     return p;
 }
@@ -582,6 +666,37 @@ extern "C" int ctc_tensor_sort(ctc_tensor *t, int mode)
             for (uint64_t i = b; i < e; ++i) tv[i] = t->vals[perm[i]];
         });
         t->vals.swap(tv);
+    });
+}
+
+extern "C" int ctc_plan_tiles(const uint64_t *ind, uint64_t n, uint32_t tile_len, int from_runs, int32_t *tiles,
+                              uint64_t tiles_cap, uint64_t *ntiles, uint32_t *heavy, uint64_t heavy_cap,
+                              uint64_t *nheavy)
+{
+    return guarded([&] {
+        if ((!ind && n) || !ntiles || !nheavy || tile_len == 0) fail(CTC_E_ARG, "bad arguments");
+        if (n >= 0x7fffffffull) fail(CTC_E_UNSUP, "tile plans index at most 2^31 - 1 nonzeros");
+        TilePlan p;
+        if (from_runs) {
+            std::vector<uint32_t> rows, counts;
+            for (uint64_t i = 0; i < n;) {
+                if (i > 0 && ind[i] < ind[i - 1]) fail(CTC_E_ARG, "indices are not sorted");
+                uint64_t e = i + 1;
+                while (e < n && ind[e] == ind[i]) ++e;
+                rows.push_back((uint32_t)(ind[i] - 1));
+                counts.push_back((uint32_t)(e - i));
+                i = e;
+            }
+            p = plan_tiles_runs(rows.data(), counts.data(), rows.size(), tile_len);
+        } else {
+            bool unsorted = false;
+            p = plan_tiles_chunked(ind, n, tile_len, &unsorted);
+            if (unsorted) fail(CTC_E_ARG, "indices are not sorted");
+        }
+        *ntiles = p.ntiles();
+        *nheavy = p.nheavy();
+        if (tiles && tiles_cap >= p.ntiles()) std::copy(p.tiles.begin(), p.tiles.end(), tiles);
+        if (heavy && heavy_cap >= p.nheavy()) std::copy(p.heavy_rows.begin(), p.heavy_rows.end(), heavy);
     });
 }
 

@@ -33,6 +33,18 @@ static void check_cuda(cudaError_t e, const char *what)
 }
 #define CK(x) check_cuda((x), #x)
 
+// Device memory of the library comes from one stream-ordered pool per
+// device that keeps freed blocks (release threshold: unlimited), so that
+// datasets, sessions and staging scratch that come and go reuse mapped
+// memory instead of mapping and unmapping gigabytes on every call.
+// dev_alloc returns a block ready for use on any stream; dev_free first
+// waits for the device, as cudaFree does, so that a block is idle before
+// the pool hands it out again.  (Defined once, in engine.cu.)
+void *dev_alloc(size_t bytes);
+void dev_free(void *p) noexcept;
+// unused pool memory back to the driver
+void dev_pool_trim() noexcept;
+
 template <typename T>
 struct DevBuf {
     T *p = nullptr;
@@ -43,7 +55,7 @@ struct DevBuf {
     ~DevBuf() { release(); }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         n = 0;
     }
@@ -51,12 +63,17 @@ struct DevBuf {
     {
         release();
         if (count == 0) count = 1;
-        CK(cudaMalloc(&p, count * sizeof(T)));
+        p = static_cast<T *>(dev_alloc(count * sizeof(T)));
         n = count;
     }
     void ensure(size_t count)
     {
         if (n < count) alloc(count);
+    }
+    void swap(DevBuf &o)
+    {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
     }
     void upload(const T *h, size_t count, cudaStream_t s)
     {

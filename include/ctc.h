@@ -122,6 +122,19 @@ int ctc_ciss_export(const ctc_ciss *c, uint64_t *directory, uint64_t *dcounter,
                     double *entries, uint8_t *written);
 int ctc_ciss_free(ctc_ciss *c);
 
+/* Work-tile plan of a copy sorted for one mode (ind: that mode's 1-based
+ * indices, n of them): at most tile_len nonzeros per tile, whole rows
+ * packed, longer rows split into pieces.  tiles: 4 int32 per tile {first
+ * nonzero, length, heavy-row index or -1, piece}; heavy: 4 uint32 per long
+ * row {row (0-based), first tile, tiles, 0}.  from_runs = 1 builds it from
+ * the rows' run lengths (the planner of the device staging), 0 from the
+ * index array (the host staging's planner); the two give the same plan.
+ * The counts are always written, each array only when its capacity holds
+ * it.  CTC_E_ARG when ind is not sorted. */
+int ctc_plan_tiles(const uint64_t *ind, uint64_t n, uint32_t tile_len, int from_runs, int32_t *tiles,
+                   uint64_t tiles_cap, uint64_t *ntiles, uint32_t *heavy, uint64_t heavy_cap,
+                   uint64_t *nheavy);
+
 /* ---------------------------------------------------------------- */
 /* factor model                                                      */
 /* ---------------------------------------------------------------- */

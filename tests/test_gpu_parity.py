@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import cutc_b200 as ctc
+from cutc_b200 import synth
 from oracle import pyoracle as po
 from tests.helpers import Problem, max_factor_rel, rel
 
@@ -338,6 +339,75 @@ def test_rejects_bad_input(ctx):
     assert e.value.code == -1
     with pytest.raises(ctc.CtcError):
         ctc.run(ctx, [t], None, None, m, ctc.params("als", rank=12, iters=1))
+
+
+@pytest.mark.parametrize("alg", ["als", "ccd", "ccdpp", "sgd"])
+def test_rejects_out_of_range_indices_on_every_staging_path(ctx, alg):
+    """Indices are range-checked in the staging pass that reads them (the
+    record upload of every copy and of the test tensor): a bad index is an
+    argument error before any kernel runs."""
+    P = Problem(3000, (40, 30, 20), 8, seed=17)
+    p = ctc.params(alg, rank=8, iters=1, lr=1e-3, lr_scale=1.0)
+    ncopies = 1 if alg == "sgd" else 3
+
+    def copies(bad_copy=None, mode=0, at=0, value=0):
+        out = []
+        for m in range(ncopies):
+            ind, vals = P.sorted[m]
+            ind = ind.copy()
+            if m == bad_copy:
+                ind[mode, at] = value
+            out.append(ctc.Tensor.from_coo(ind, vals, dims=P.dims))
+        return out
+
+    ctc.run(ctx, copies(), None, P.c_test(), P.c_model(), p)  # well formed
+    n = P.sorted[0][0].shape[1]
+    cases = [copies(0, 1, n // 2, P.dims[1] + 1)]          # past mode 2's rows, middle of copy 1
+    if ncopies == 3:
+        cases.append(copies(2, 2, n - 1, P.dims[2] + 1))  # the last (largest) row of copy 3
+        cases.append(copies(1, 0, 0, 0))                  # a 0 index (indices are 1-based)
+    for train in cases:
+        with pytest.raises(ctc.CtcError) as e:
+            ctc.run(ctx, train, None, P.c_test(), P.c_model(), p)
+        assert e.value.code == -1 and "1-based" in str(e.value)
+    tind, tvals = P.test
+    tind = tind.copy()
+    tind[1, 0] = 0
+    with pytest.raises(ctc.CtcError) as e:
+        ctc.run(ctx, copies(), None, ctc.Tensor.from_coo(tind, tvals, dims=P.dims), P.c_model(), p)
+    assert e.value.code == -1 and "test tensor" in str(e.value)
+
+
+@pytest.mark.parametrize("alg,prec", [("ccdpp", ctc.PREC_F32), ("ccdpp", ctc.PREC_F64), ("als", ctc.PREC_F32),
+                                      ("ccd", ctc.PREC_F64)])
+def test_device_sorted_copies_match_host_sorted_copies(ctx, alg, prec):
+    """train[0] alone: copies 2 and 3 are sorted on the device (stable by
+    (mode, next mode), the order ctc_tensor_sort gives).  The training is
+    the same, bit for bit, as with the three copies sorted on the host
+    from train[0] and passed in."""
+    P = Problem(60000, (300, 200, 100), 16, seed=19, heavy_row=3000)
+    c0 = P.sorted[0]
+    host = [c0] + [synth.sort_for_mode(*c0, m) for m in (1, 2)]
+    p = ctc.params(alg, rank=16, iters=2, precision=prec, early_stop=0, eval_every=1, inner=2, **{"lambda": 0.1})
+    m3, m1 = P.c_model(), P.c_model()
+    o3 = ctc.run(ctx, [ctc.Tensor.from_coo(*h, dims=P.dims) for h in host], None, P.c_test(), m3, p)
+    o1 = ctc.run(ctx, [ctc.Tensor.from_coo(*c0, dims=P.dims)], None, P.c_test(), m1, p)
+    for a, b in zip(m3.factors(), m1.factors()):
+        assert np.array_equal(a, b)
+    assert [e["rmse_te"] for e in o3.epochs] == [e["rmse_te"] for e in o1.epochs]
+
+
+def test_rejects_unsorted_copy(ctx):
+    P = Problem(3000, (40, 30, 20), 8, seed=18)
+    tr = P.sorted
+    ind, vals = tr[1]
+    ind, vals = ind[:, ::-1].copy(), vals[::-1].copy()  # mode-2 order reversed
+    train = [ctc.Tensor.from_coo(*tr[0], dims=P.dims), ctc.Tensor.from_coo(ind, vals, dims=P.dims),
+             ctc.Tensor.from_coo(*tr[2], dims=P.dims)]
+    for alg in ("ccdpp", "als"):
+        with pytest.raises(ctc.CtcError) as e:
+            ctc.run(ctx, train, None, None, P.c_model(), ctc.params(alg, rank=8, iters=1))
+        assert e.value.code == -1 and "not sorted" in str(e.value)
 
 
 def test_checkpoint_resume_is_exact(ctx, tmp_path):

@@ -263,3 +263,43 @@ def test_model_checkpoint_round_trip_and_rejects_bad_files(tmp_path):
     (tmp_path / "short.ctcm").write_bytes(raw[: len(raw) // 2])
     with pytest.raises(ctc.CtcError):
         ctc.Model.load(str(tmp_path / "short.ctcm"))
+
+
+# ------------------------------------------------------------------ tile plans
+def _zipf_rows(n, nrows, seed):
+    rng = np.random.default_rng(seed)
+    w = 1.0 / np.arange(1, nrows + 1) ** 1.1
+    return np.sort(rng.choice(nrows, size=n, p=w / w.sum()) + 1).astype(np.uint64)
+
+
+@pytest.mark.parametrize("n,nrows,T", [(1, 5, 256), (5000, 40, 128), (70000, 3000, 256),
+                                       ((1 << 20) + 17, 20000, 512), (3 << 20, 500000, 256)])
+def test_plan_from_runs_is_the_plan_from_indices(n, nrows, T):
+    """The device staging plans from the rows' run lengths; the host staging
+    from the index array.  Same tiles, same long rows, chunk cuts included
+    (n above 2^20 takes the 64-chunk form)."""
+    ind = _zipf_rows(n, nrows, seed=n + T)
+    ta, ha = ctc.plan_tiles(ind, T, from_runs=False)
+    tb, hb = ctc.plan_tiles(ind, T, from_runs=True)
+    assert np.array_equal(ta, tb) and np.array_equal(ha, hb)
+    # the tiles cover [0, n) in order; light tiles hold whole rows
+    assert ta[0, 0] == 0 and int(ta[-1, 0]) + int(ta[-1, 1]) == n
+    assert np.all(ta[1:, 0] == ta[:-1, 0] + ta[:-1, 1]) and np.all((ta[:, 1] >= 1) & (ta[:, 1] <= T))
+    light = ta[ta[:, 2] < 0]
+    starts, ends = light[:, 0], light[:, 0] + light[:, 1]
+    assert np.all((starts == 0) | (ind[np.maximum(starts - 1, 0)] != ind[starts]))
+    assert np.all((ends == n) | (ind[np.minimum(ends, n - 1)] != ind[ends - 1]))
+    # long rows: pieces of T, numbered in order, one entry per row longer than T
+    runs = np.diff(np.flatnonzero(np.r_[True, ind[1:] != ind[:-1], True]))
+    assert len(ha) == int(np.sum(runs > T))
+    for h, (row, first, np_, _) in enumerate(ha):
+        pieces = ta[first:first + np_]
+        assert np.all(pieces[:, 2] == h) and np.array_equal(pieces[:, 3], np.arange(np_))
+        assert np.all(ind[pieces[:, 0]] == row + 1)
+
+
+def test_plan_rejects_unsorted_indices():
+    ind = np.array([1, 1, 3, 2, 4], dtype=np.uint64)
+    for runs in (False, True):
+        with pytest.raises(ctc.CtcError):
+            ctc.plan_tiles(ind, 32, from_runs=runs)
