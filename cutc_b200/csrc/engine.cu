@@ -637,19 +637,32 @@ struct Session : SessionBase {
         CK(cudaStreamSynchronize(ctx->stream));
     }
 
+    // rows x cols row-major -> cols x rows row-major on the device
+    void transpose(const T *in, uint64_t rows, uint64_t cols, T *out)
+    {
+        const dim3 grid((unsigned)((rows + 31) / 32), (unsigned)std::min<uint64_t>((cols + 31) / 32, 65535));
+        LAUNCH(ctx, k::k_transpose<T>, grid, dim3(32, 8), 0, in, rows, cols, out);
+    }
+
+    // The factors stream through the pinned buffer as rows of T (converted
+    // on the host threads); CCD++'s column-major factors are transposed on
+    // the device.
     void set_model(const ctc_model *mdl) override
     {
+        DevBuf<T> rowmajor;
         for (int m = 0; m < 3; ++m) {
-            const uint64_t d = dims[m];
-            std::vector<T> h(d * R);
+            const uint64_t d = dims[m], n = d * R;
             const double *src = mdl->U[m].data();
-            par_for(d, [&](uint64_t b, uint64_t e) {
-                for (uint64_t r = b; r < e; ++r)
-                    for (int f = 0; f < R; ++f)
-                        h[colmajor ? (uint64_t)f * d + r : r * R + f] = (T)src[r * R + f];
+            T *dst = U[m].p;
+            if (colmajor) {
+                rowmajor.ensure(n);
+                dst = rowmajor.p;
+            }
+            upload_filled(ctx, dst, n, [&](uint64_t b, uint64_t e, T *h) {
+                for (uint64_t i = b; i < e; ++i) h[i - b] = (T)src[i];
             });
-            U[m].upload(h.data(), h.size(), ctx->stream);
-            CK(cudaMemcpyAsync(Ubest[m].p, U[m].p, h.size() * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+            if (colmajor) transpose(rowmajor.p, d, R, U[m].p);
+            CK(cudaMemcpyAsync(Ubest[m].p, U[m].p, n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
         }
         CK(cudaMemsetAsync(nonspd_dev.p, 0, sizeof(unsigned long long), ctx->stream));
@@ -664,16 +677,18 @@ struct Session : SessionBase {
     void get_model(ctc_model *mdl, bool best) override
     {
         DevBuf<T> *src = best ? Ubest : U;
+        DevBuf<T> rowmajor;
         for (int m = 0; m < 3; ++m) {
-            const uint64_t d = dims[m];
-            std::vector<T> h(d * R);
-            CK(cudaMemcpyAsync(h.data(), src[m].p, h.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
+            const uint64_t d = dims[m], n = d * R;
+            const T *from = src[m].p;
+            if (colmajor) {
+                rowmajor.ensure(n);
+                transpose(src[m].p, R, d, rowmajor.p);
+                from = rowmajor.p;
+            }
             double *dst = mdl->U[m].data();
-            par_for(d, [&](uint64_t b, uint64_t e) {
-                for (uint64_t r = b; r < e; ++r)
-                    for (int f = 0; f < R; ++f)
-                        dst[r * R + f] = (double)h[colmajor ? (uint64_t)f * d + r : r * R + f];
+            download_drained(ctx, from, n, [&](uint64_t b, uint64_t e, const T *h) {
+                for (uint64_t i = b; i < e; ++i) dst[i] = (double)h[i - b];
             });
         }
     }

@@ -188,6 +188,30 @@ __global__ void __launch_bounds__(256) k_sse_chunks(const uint4 *__restrict__ re
     }
 }
 
+// out = transpose of in: in is rows x cols row-major, out[c * rows + r] =
+// in[r * cols + c].  32 x 32 tiles through shared memory (padded rows), so
+// both the reads and the writes are coalesced; 32 x 8 threads per block,
+// blocks over row tiles in x and (looping) column tiles in y.
+template <typename T>
+__global__ void __launch_bounds__(256) k_transpose(const T *__restrict__ in, uint64_t rows, uint64_t cols,
+                                                   T *__restrict__ out)
+{
+    __shared__ T tile[32][33];
+    const uint64_t r0 = (uint64_t)blockIdx.x * 32;
+    for (uint64_t c0 = (uint64_t)blockIdx.y * 32; c0 < cols; c0 += (uint64_t)gridDim.y * 32) {
+        for (int i = threadIdx.y; i < 32; i += 8) {
+            const uint64_t r = r0 + i, c = c0 + threadIdx.x;
+            if (r < rows && c < cols) tile[i][threadIdx.x] = in[r * cols + c];
+        }
+        __syncthreads();
+        for (int i = threadIdx.y; i < 32; i += 8) {
+            const uint64_t c = c0 + i, r = r0 + threadIdx.x;
+            if (r < rows && c < cols) out[c * rows + r] = tile[threadIdx.x][i];
+        }
+        __syncthreads();
+    }
+}
+
 // out[i] = sum of partial[first[i] .. first[i+1]) in order (thread per
 // instance)
 static __global__ void k_fold_segments(const double *__restrict__ partial, const uint32_t *__restrict__ first, int ninst,

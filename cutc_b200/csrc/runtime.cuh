@@ -180,14 +180,19 @@ namespace ctc {
 // next one is filled on the host threads.
 constexpr size_t kPinBytes = (size_t)32 << 20;
 
-template <typename E, typename F>
-static void upload_filled(ctc_ctx *ctx, E *dev, uint64_t n, F &&fill)
+static void ensure_pinned(ctc_ctx *ctx)
 {
     if (!ctx->pin[0])
         for (int q = 0; q < 2; ++q) {
             CK(cudaMallocHost(&ctx->pin[q], kPinBytes));
             CK(cudaEventCreateWithFlags(&ctx->pin_ev[q], cudaEventDisableTiming));
         }
+}
+
+template <typename E, typename F>
+static void upload_filled(ctc_ctx *ctx, E *dev, uint64_t n, F &&fill)
+{
+    ensure_pinned(ctx);
     const uint64_t per = kPinBytes / sizeof(E);
     int q = 0;
     for (uint64_t b = 0; b < n; b += per, q ^= 1) {
@@ -197,6 +202,33 @@ static void upload_filled(ctc_ctx *ctx, E *dev, uint64_t n, F &&fill)
         par_for(e - b, [&](uint64_t i0, uint64_t i1) { fill(b + i0, b + i1, h + i0); });
         CK(cudaMemcpyAsync(dev + b, h, (e - b) * sizeof(E), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaEventRecord(ctx->pin_ev[q], ctx->stream));
+    }
+}
+
+// Device-to-host through the same pinned double buffer: consume(b, e, h)
+// reads elements [b, e) of the device array from h (element b at h[0]) on
+// the host threads while the copy of the next chunk runs.
+template <typename E, typename F>
+static void download_drained(ctc_ctx *ctx, const E *dev, uint64_t n, F &&consume)
+{
+    ensure_pinned(ctx);
+    const uint64_t per = kPinBytes / sizeof(E);
+    const uint64_t nch = (n + per - 1) / per;
+    auto issue = [&](uint64_t c) {
+        const int q = (int)(c & 1);
+        const uint64_t b = c * per, e = std::min(n, b + per);
+        CK(cudaEventSynchronize(ctx->pin_ev[q]));  // an earlier copy through this buffer is done
+        CK(cudaMemcpyAsync(ctx->pin[q], dev + b, (e - b) * sizeof(E), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaEventRecord(ctx->pin_ev[q], ctx->stream));
+    };
+    if (nch) issue(0);
+    for (uint64_t c = 0; c < nch; ++c) {
+        if (c + 1 < nch) issue(c + 1);
+        const int q = (int)(c & 1);
+        const uint64_t b = c * per, e = std::min(n, b + per);
+        CK(cudaEventSynchronize(ctx->pin_ev[q]));
+        const E *h = reinterpret_cast<const E *>(ctx->pin[q]);
+        par_for(e - b, [&](uint64_t i0, uint64_t i1) { consume(b + i0, b + i1, h + i0); });
     }
 }
 
@@ -217,8 +249,8 @@ static void kt_flush(ctc_ctx *ctx)
 }
 
 template <typename Kern, typename... Args>
-static void launch_named(ctc_ctx *ctx, const char *name, Kern kern, unsigned grid, unsigned block,
-                         size_t smem, Args... args)
+static void launch_named(ctc_ctx *ctx, const char *name, Kern kern, dim3 grid, dim3 block, size_t smem,
+                         Args... args)
 {
     KernelTimes &k = ctx->kt;
     const bool timed = k.on && !ctx->capturing;
