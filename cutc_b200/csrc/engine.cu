@@ -363,9 +363,11 @@ static int default_tile(int alg)
 // the records of train[0] (mode-1 order) are uploaded once; copy m is the
 // caller's train[m] uploaded as records when given, else the stable
 // (mode m, mode m+1) order of train[0] sorted on the device (the order
-// ctc_tensor_sort gives).  The rows' run lengths come back to the host for
-// the tile plan (plan_tiles_runs: the plan of the host planner), and the
-// CCD++ slots or the record copy are gathered on the device.
+// ctc_tensor_sort gives).  CCD++ copies are further sorted by the full key
+// (row, larger other mode, smaller other mode).  The rows' run lengths
+// come back to the host for the tile plan (plan_tiles_runs: the plan of the
+// host planner), and the CCD++ slots or the record copy are gathered on
+// the device.
 template <typename T>
 static void stage_copies_dev(ctc_ctx *ctx, const ctc_params &p, uint32_t tl, const ctc_tensor *const train[3],
                              const uint64_t *dims, bool trunc, DatasetImpl<T> &impl)
@@ -380,19 +382,39 @@ static void stage_copies_dev(ctc_ctx *ctx, const ctc_params &p, uint32_t tl, con
     }
     // copy 1 last: it can take over the base records (ALS / CCD)
     for (int m : {1, 2, 0}) {
+        const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
         DevTensor<T> given;
         const DevTensor<T> *src = &base;
         DevBuf<uint32_t> perm;
+        bool in_order = m == 0;  // src already sorted for mode m (copy 1, or the caller's copy)
         if (m > 0 && train[m]) {
             TracePhase tp("records + upload");
             stage_tensor<T>(ctx, train[m], trunc, given, dims, "training tensor");
             src = &given;
-        } else if (m > 0) {
+            in_order = true;
+        }
+        if (in_order && dev_unsorted(ctx, src->rec.p, (uint32_t)n, m))
+            fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", m + 1, m + 1);
+        if (ccdpp) {
+            // CCD++ slots: within each row, the larger of the other two modes
+            // in increasing order (then the smaller), so that the gathers from
+            // the column that cannot be staged in shared memory sweep it
+            // instead of jumping; the full key makes the order unique for
+            // distinct coordinates, whichever copy it starts from
             TracePhase tp("device sort");
-            const int m1 = (m + 1) % 3;
+            const int kb = bits_for(dims[0]) + bits_for(dims[1]) + bits_for(dims[2]);
+            if (kb > 64) fail(CTC_E_UNSUP, "CCD++ keys need %d bits (> 64) for these dimensions", kb);
+            const int big = dims[m2] > dims[m1] ? m2 : m1, small = big == m1 ? m2 : m1;
+            const int k[3] = {m, big, small};
+            const int b[3] = {bits_for(dims[m]), bits_for(dims[big]), bits_for(dims[small])};
             perm.alloc(n);
-            dev_sort_order(ctx, base.rec.p, (uint32_t)n, m, bits_for(dims[m1]), bits_for(dims[m]) + bits_for(dims[m1]),
-                           perm.p);
+            dev_sort_order(ctx, src->rec.p, (uint32_t)n, k, b, perm.p);
+        } else if (!in_order) {
+            TracePhase tp("device sort");
+            const int k[3] = {m, m1, m1};
+            const int b[3] = {bits_for(dims[m]), bits_for(dims[m1]), 0};
+            perm.alloc(n);
+            dev_sort_order(ctx, base.rec.p, (uint32_t)n, k, b, perm.p);
         }
         const uint32_t *pp = perm.p;
         DevTensor<T> &d = impl.copy[m];

@@ -20,15 +20,22 @@ constexpr uint64_t kPadKey = ~0ull;
 
 __device__ __forceinline__ uint32_t field(const uint4 &r, int m) { return m == 0 ? r.x : (m == 1 ? r.y : r.z); }
 
-static __global__ void k_order_keys(const uint4 *__restrict__ rec, uint32_t n, int m, int b1,
-                                    uint64_t *__restrict__ keys, uint32_t *__restrict__ ids)
+static __global__ void k_order_keys(const uint4 *__restrict__ rec, uint32_t n, int k0, int k1, int k2, int b1,
+                                    int b2, uint64_t *__restrict__ keys, uint32_t *__restrict__ ids)
 {
-    const int m1 = (m + 1) % 3;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint4 r = rec[i];
-        keys[i] = ((uint64_t)field(r, m) << b1) | field(r, m1);
+        uint64_t key = ((uint64_t)field(r, k0) << (b1 + b2)) | ((uint64_t)field(r, k1) << b2);
+        if (b2) key |= field(r, k2);
+        keys[i] = key;
         ids[i] = i;
     }
+}
+
+static __global__ void k_check_sorted(const uint4 *__restrict__ rec, uint32_t n, int m, int *__restrict__ unsorted)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += gridDim.x * blockDim.x)
+        if (field(rec[i], m) < field(rec[i - 1], m)) *unsorted = 1;
 }
 
 static __global__ void k_rows_in_order(const uint4 *__restrict__ rec, const uint32_t *__restrict__ perm, uint32_t n,
@@ -115,14 +122,17 @@ static __global__ void k_row_hist_global(const uint4 *__restrict__ rec, uint32_t
 
 }  // namespace sg
 
-void dev_sort_order(ctc_ctx *ctx, const uint4 *rec, uint32_t n, int m, int b1, int end_bit, uint32_t *perm)
+void dev_sort_order(ctc_ctx *ctx, const uint4 *rec, uint32_t n, const int k[3], const int b[3], uint32_t *perm)
 {
+    const int end_bit = b[0] + b[1] + b[2];
+    if (end_bit > 64) fail(CTC_E_UNSUP, "sort keys need %d bits (> 64) for these dimensions", end_bit);
     DevBuf<uint64_t> k_in, k_out;
     DevBuf<uint32_t> ids;
     k_in.alloc(n);
     k_out.alloc(n);
     ids.alloc(n);
-    LAUNCH(ctx, sg::k_order_keys, grid_for(n, 256, kSMs * 16), 256, 0, rec, n, m, b1, k_in.p, ids.p);
+    LAUNCH(ctx, sg::k_order_keys, grid_for(n, 256, kSMs * 16), 256, 0, rec, n, k[0], k[1], k[2], b[1], b[2], k_in.p,
+           ids.p);
     size_t tmp = 0;
     CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k_in.p, k_out.p, ids.p, perm, (int)n, 0, end_bit,
                                        ctx->stream));
@@ -131,6 +141,18 @@ void dev_sort_order(ctc_ctx *ctx, const uint4 *rec, uint32_t n, int m, int b1, i
     CK(cub::DeviceRadixSort::SortPairs(scratch.p, tmp, k_in.p, k_out.p, ids.p, perm, (int)n, 0, end_bit,
                                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+}
+
+bool dev_unsorted(ctc_ctx *ctx, const uint4 *rec, uint32_t n, int m)
+{
+    DevBuf<int> flag;
+    flag.alloc(1);
+    CK(cudaMemsetAsync(flag.p, 0, sizeof(int), ctx->stream));
+    LAUNCH(ctx, sg::k_check_sorted, grid_for(n, 256, kSMs * 16), 256, 0, rec, n, m, flag.p);
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return h != 0;
 }
 
 bool dev_row_runs(ctc_ctx *ctx, const uint4 *rec, const uint32_t *perm, uint32_t n, int m,

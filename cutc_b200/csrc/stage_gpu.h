@@ -13,10 +13,14 @@ struct ctc_ctx;
 
 namespace ctc {
 
-// perm[i] = the record at position i of the stable (mode m, mode m+1)
-// order, the order ctc_tensor_sort gives (rows of mode m+1 in b1 bits,
-// end_bit = bits of mode m + b1).
-void dev_sort_order(ctc_ctx *ctx, const uint4 *rec, uint32_t n, int m, int b1, int end_bit, uint32_t *perm);
+// perm[i] = the record at position i of the stable order by the key
+// (mode k[0], mode k[1], mode k[2]) with those indices in b[0], b[1], b[2]
+// bits (b[2] = 0: two keys).  k = {m, m+1}, b = {bits(m), bits(m+1), 0} is
+// the order ctc_tensor_sort gives.
+void dev_sort_order(ctc_ctx *ctx, const uint4 *rec, uint32_t n, const int k[3], const int b[3], uint32_t *perm);
+
+// true when the mode-m indices of the records decrease somewhere
+bool dev_unsorted(ctc_ctx *ctx, const uint4 *rec, uint32_t n, int m);
 
 // Runs of equal mode-m rows in the order `perm` (null: as stored): run r
 // is row rows[r] repeated counts[r] times.  Returns true when the rows

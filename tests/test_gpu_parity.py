@@ -382,9 +382,10 @@ def test_rejects_out_of_range_indices_on_every_staging_path(ctx, alg):
                                       ("ccd", ctc.PREC_F64)])
 def test_device_sorted_copies_match_host_sorted_copies(ctx, alg, prec):
     """train[0] alone: copies 2 and 3 are sorted on the device (stable by
-    (mode, next mode), the order ctc_tensor_sort gives).  The training is
-    the same, bit for bit, as with the three copies sorted on the host
-    from train[0] and passed in."""
+    (mode, next mode), the order ctc_tensor_sort gives; CCD++ slots by the
+    full key, the larger other mode first).  The training is the same, bit
+    for bit, as with the three copies sorted on the host from train[0] and
+    passed in."""
     P = Problem(60000, (300, 200, 100), 16, seed=19, heavy_row=3000)
     c0 = P.sorted[0]
     host = [c0] + [synth.sort_for_mode(*c0, m) for m in (1, 2)]
