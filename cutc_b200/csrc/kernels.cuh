@@ -1230,6 +1230,144 @@ __device__ __forceinline__ void als_accumulate(const uint4 *__restrict__ rec,
     }
 }
 
+// Short rows: a row with k <= KW = R / 2 nonzeros (and no reference
+// multiplicities) has a Gram H^T H of rank k, and its system
+//     (H^T H + lambda I) u = H^T x            (R x R)
+// is solved through the k x k dual (the Woodbury identity)
+//     (H H^T + lambda I) y = x,   u = H^T y
+// in FP64: H (the row's Khatri-Rao rows, h_i = U_a(q1_i) o U_b(q2_i)
+// formed in T as the R x R path forms them) in the warp's free
+// parked-system slot, K = H H^T + lambda I by lane per entry, its Cholesky
+// factor with lane j owning row j, substitutions with y in registers (lane
+// i holds y_i), and one refinement step on the dual residual
+// x - H u - lambda y.  Costs k^2 R + k^3 / 6 instead of k R^2 + R^3 / 6.
+// Returns 1 when a pivot was not positive (diagonal shifted).
+template <typename T, int R>
+struct AlsShort {
+    static constexpr int KW = R / 2;        // longest row solved this way
+    static constexpr int HS = R + 1;        // H row stride (doubles): 2-way banks at most
+    static constexpr int KS = KW + 1;       // K row stride
+    static constexpr int doubles = KW * HS + KW * KS + KW + R;
+    static_assert(doubles <= AlsBatch<T, R>::sys_doubles, "short-row scratch fits one parked-system slot");
+    static_assert(KW <= 32, "one lane per dual row");
+};
+
+template <typename T, int R>
+__device__ __forceinline__ int als_solve_short(const uint4 *__restrict__ rec, const double *__restrict__ v64, int m,
+                                               const T *__restrict__ Ua, const T *__restrict__ Ub, uint32_t s,
+                                               int k, T lambda, double *scr, T *Um, uint32_t row)
+{
+    using Sw = AlsShort<T, R>;
+    constexpr int HS = Sw::HS, KS = Sw::KS, KW = Sw::KW;
+    constexpr int FL = R < 32 ? R : 32;  // lanes per h row
+    constexpr int IPS = 32 / FL;         // h rows per step
+    const int lane = threadIdx.x & 31;
+    const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+    double *H = scr;                 // k x R
+    double *K = H + KW * HS;         // k x k, lower triangle
+    double *dinv = K + KW * KS;      // 1 / L(j, j)
+    double *u = dinv + KW;           // R
+    const double lam = (double)lambda;
+    // lane i < k: the record of nonzero i
+    uint32_t qa = 0, qb = 0;
+    double xi = 0.0;
+    if (lane < k) {
+        const uint4 r = rec[s + lane];
+        qa = key_of(r, m1);
+        qb = key_of(r, m2);
+        xi = (double)value_of<T>(r, v64, s + lane);
+    }
+    for (int i0 = 0; i0 < k; i0 += IPS) {
+        const int i = i0 + lane / FL;
+        const int src = min(i, k - 1);
+        const uint32_t a = __shfl_sync(0xffffffffu, qa, src), b = __shfl_sync(0xffffffffu, qb, src);
+        if (i < k)
+            for (int f = lane % FL; f < R; f += FL) H[i * HS + f] = (double)(Ua[(size_t)a * R + f] * Ub[(size_t)b * R + f]);
+    }
+    __syncwarp();
+    // K = H H^T + lambda I, lower triangle, one lane per entry
+    const int npairs = k * (k + 1) / 2;
+    for (int p = lane; p < npairs; p += 32) {
+        int i = (int)((sqrtf(8.0f * (float)p + 1.0f) - 1.0f) * 0.5f);
+        while (i * (i + 1) / 2 > p) --i;
+        while ((i + 1) * (i + 2) / 2 <= p) ++i;
+        const int j = p - i * (i + 1) / 2;
+        double acc = (i == j) ? lam : 0.0;
+#pragma unroll 8
+        for (int f = 0; f < R; ++f) acc += H[i * HS + f] * H[j * HS + f];
+        K[i * KS + j] = acc;
+    }
+    __syncwarp();
+    // Cholesky K = L L^T, right-looking; lane i updates row i
+    int bad = 0;
+    for (int j = 0; j < k; ++j) {
+        if (lane == j) {
+            double d = K[j * KS + j];
+            if (!(d > 0.0)) {
+                bad = 1;
+                d = 1e-300 + fabs(d) + 1e-12 * lam + 1e-30;
+            }
+            const double l = sqrt(d);
+            K[j * KS + j] = l;
+            dinv[j] = 1.0 / l;
+        }
+        __syncwarp();
+        if (lane > j && lane < k) K[lane * KS + j] *= dinv[j];  // column j of L
+        __syncwarp();
+        if (lane > j && lane < k) {  // trailing update of row `lane`
+            const double lij = K[lane * KS + j];
+            for (int c = j + 1; c <= lane; ++c) K[lane * KS + c] -= lij * K[c * KS + j];
+        }
+        __syncwarp();
+    }
+    // y = K^-1 x (lane i holds y_i), u = H^T y, then one refinement step
+    auto solve = [&](double rhs) -> double {
+        double yi = rhs;
+        for (int j = 0; j < k; ++j) {  // L z = rhs
+            const double yj = __shfl_sync(0xffffffffu, yi, j) * dinv[j];
+            if (lane == j) yi = yj;
+            else if (lane > j && lane < k) yi -= K[lane * KS + j] * yj;
+        }
+        for (int j = k - 1; j >= 0; --j) {  // L^T y = z
+            const double yj = __shfl_sync(0xffffffffu, yi, j) * dinv[j];
+            if (lane == j) yi = yj;
+            else if (lane < j) yi -= K[j * KS + lane] * yj;
+        }
+        return lane < k ? yi : 0.0;
+    };
+    auto primal = [&](double yi) {  // u = H^T y into shared memory
+        double uf[(R + 31) / 32];
+#pragma unroll
+        for (int t = 0; t < (R + 31) / 32; ++t) uf[t] = 0.0;
+        for (int i = 0; i < k; ++i) {
+            const double yv = __shfl_sync(0xffffffffu, yi, i);
+#pragma unroll
+            for (int t = 0; t < (R + 31) / 32; ++t)
+                if (lane + 32 * t < R) uf[t] += yv * H[i * HS + lane + 32 * t];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < (R + 31) / 32; ++t)
+            if (lane + 32 * t < R) u[lane + 32 * t] = uf[t];
+        __syncwarp();
+    };
+    double y = solve(xi);
+    primal(y);
+    // dual residual x_i - h_i . u - lambda y_i (lane i), corrected y
+    double res = 0.0;
+    if (lane < k) {
+        double hu = 0.0;
+        for (int f = 0; f < R; ++f) hu += H[lane * HS + f] * u[f];
+        res = xi - hu - lam * y;
+    }
+    y += solve(res);
+    primal(y);
+    for (int f = lane; f < R; f += 32) Um[(size_t)row * R + f] = (T)u[f];
+    const bool any_bad = __any_sync(0xffffffffu, bad != 0);
+    __syncwarp();
+    return (any_bad && lane == 0) ? 1 : 0;  // once per row, as the parked solves count
+}
+
 template <typename T, int R>
 __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles, uint32_t ntiles,
                                                   const uint4 *__restrict__ rec,
@@ -1251,6 +1389,7 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const int gl = lane % L;
     int bad = 0, parked = 0;
+    const bool short_rows = w == nullptr && lambda > T(0);
     T G[R][C];
     T b[C];
     for (uint64_t tile = warp; tile < ntiles; tile += nwarps) {
@@ -1284,6 +1423,13 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
                     break;
                 }
                 e += 32;
+            }
+            if (short_rows && e - s <= (uint32_t)AlsShort<T, R>::KW) {
+                // the free slot (parked < NS here) holds the short row's scratch
+                bad += als_solve_short<T, R>(rec, v64, m, Ua, Ub, s, (int)(e - s), lambda,
+                                             W + (size_t)parked * Bt::sys_doubles, Um, key);
+                s = e;
+                continue;
             }
             als_accumulate<T, R>(rec, v64, w, m, Ua, Ub, s, e, G, b);
             als_park<T, R>(W, parked, key, G, b, lambda);

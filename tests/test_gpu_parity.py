@@ -69,6 +69,25 @@ def test_als_f64(ctx, R):
         assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-9
 
 
+@pytest.mark.parametrize("R", [8, 16, 32, 64])
+def test_als_short_rows_dual_solve(ctx, R):
+    """Mode 1 has 3000 rows for 9000 nonzeros, so most of its rows hold at
+    most R / 2 nonzeros and take the k x k dual solve (u = H^T (H H^T +
+    lambda I)^-1 x); modes 2 and 3 have long rows and take the R x R
+    solves.  Both match the FP64 oracle to 1e-9 in FP64 and to the FP32
+    bars in FP32."""
+    P = Problem(10000, (3000, 40, 30), R, seed=41)
+    U, hist = oracle_als(P, 2, 0.1)
+    G, out = engine_run(ctx, P, ctc.ALS, 2, precision=ctc.PREC_F64, **{"lambda": 0.1})
+    assert max_factor_rel(G, U) < 1e-9
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-9
+    U1, hist1 = oracle_als(P, 1, 0.1)
+    G1, out1 = engine_run(ctx, P, ctc.ALS, 1, precision=ctc.PREC_F32, **{"lambda": 0.1})
+    assert max_factor_rel(G1, U1) < 1e-4
+    assert abs(out1.epochs[1]["rmse_te"] - hist1[1][1]) / hist1[1][1] < 1e-5
+
+
 def test_als_f32_config(ctx):
     """Plain FP32 ALS at R=16, lambda=0.05 (the small uniform workload's
     settings), 10 iterations."""
