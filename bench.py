@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--instances", type=int, default=0, help="batch workloads: a K-instance sample of the same distribution")
     ap.add_argument("--tune-cache", default="", help="autotuner cache file (default: a fresh temporary one)")
     ap.add_argument("--no-tune", action="store_true", help="library defaults instead of autotuned parameters")
+    ap.add_argument("--als", action="store_true",
+                    help="the ALS leg alone on --workload (zipf-400m runs it by default)")
     return ap.parse_args()
 
 
@@ -630,14 +632,15 @@ def run_reference(args):
 
 
 def als_leg(ctc, ctx, args, device):
-    """ALS at rank 64 on the 400M-nonzero Zipf(1.3) tensor (1M x 600k x
-    300, CP rank 24 + N(0, 0.2^2), lambda 0.05): iterations in FP32 and in
-    mixed precision (BF16 factor copies into tcgen05 Gram blocks for the
-    pieces of long rows, FP64 row solves with one refinement step)."""
+    """ALS on --workload: at rank 64 (the 400M-nonzero Zipf(1.3) tensor,
+    1M x 600k x 300, CP rank 24 + N(0, 0.2^2), lambda 0.05) iterations in
+    FP32 and in mixed precision (BF16 factor copies into tcgen05 Gram blocks
+    for the pieces of long rows, FP64 row solves with one refinement step);
+    at other ranks (the 100M-nonzero rank-32 tensor, lambda 0.1) FP32."""
     import torch
 
     from cutc_b200 import synth
-    w = synth.WORKLOADS["zipf-400m"]
+    w = synth.WORKLOADS[args.workload]
     if args.nnz:
         w = synth.scaled(w, args.nnz)
     t0 = time.time()
@@ -651,12 +654,14 @@ def als_leg(ctc, ctx, args, device):
     torch.cuda.empty_cache()
     tr = [ctc.Tensor.from_coo(i, v, dims=w.dims) for i, v in srt]
     del srt
-    out = {"workload": w.name, "dims": list(w.dims), "nnz_train": ntr, "rank": w.rank, "lambda": 0.05,
+    lam = 0.05 if w.rank == 64 else 0.1
+    out = {"workload": w.name, "dims": list(w.dims), "nnz_train": ntr, "rank": w.rank, "lambda": lam,
            "generate_s": time.time() - t0}
     iters = 3
-    for name, prec in (("fp32", ctc.PREC_F32), ("mixed_tc", ctc.PREC_MIXED)):
+    forms = [("fp32", ctc.PREC_F32)] + ([("mixed_tc", ctc.PREC_MIXED)] if w.rank == 64 else [])
+    for name, prec in forms:
         p = ctc.params("als", rank=w.rank, precision=prec, iters=iters, early_stop=0, eval_every=0,
-                       **{"lambda": 0.05})
+                       **{"lambda": lam})
         t1 = time.time()
         ds = ctc.Dataset(ctx, tr, None, te, p)
         stage_s = time.time() - t1
@@ -664,7 +669,7 @@ def als_leg(ctc, ctx, args, device):
         ctx.set_profiling(True)
         ctx.reset_kernel_times()
         run = ds.run(m, p)
-        kt = {k: ctx.kernel_time(k) for k in ("k_als_tile", "k_als_fix", "k_als_gram_tc")}
+        kt = {k: ctx.kernel_time(k) for k in ("k_als_tile", "k_als_sum_pieces", "k_als_fix", "k_als_gram_tc")}
         ctx.set_profiling(False)
         it_s = run.result["total_ms"] / 1000.0 / iters
         out[name] = {"iteration_s": it_s, "nnz_per_s": ntr / it_s, "stage_s": stage_s,
@@ -686,10 +691,14 @@ def run_als_only(args):
     torch.cuda.set_device(local)
     ctx = ctc.Context(local)
     a = als_leg(ctc, ctx, args, f"cuda:{local}")
-    print(json.dumps({"metric": "ALS training nnz/s (rank 64, mixed precision with tensor-core Gram blocks)",
-                      "value": a["mixed_tc"]["nnz_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 3, "warmup": 0,
-                      "ms_per_step": 1000.0 * a["mixed_tc"]["iteration_s"], "higher_is_better": True,
-                      "scaling": "weak", "vs_baseline": None, "dtype": "bf16/f32/f64",
+    form = "mixed_tc" if "mixed_tc" in a else "fp32"
+    metric = ("ALS training nnz/s (rank 64, mixed precision with tensor-core Gram blocks)" if form == "mixed_tc"
+              else f"ALS training nnz/s (rank {a['rank']}, FP32)")
+    print(json.dumps({"metric": metric,
+                      "value": a[form]["nnz_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 3, "warmup": 0,
+                      "ms_per_step": 1000.0 * a[form]["iteration_s"], "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None,
+                      "dtype": "bf16/f32/f64" if form == "mixed_tc" else "f32/f64",
                       "data": "synthetic (seeded Zipf CP tensor)", "config": {"workload": a["workload"]},
                       "als": a}))
     ctx.close()
@@ -744,7 +753,7 @@ if __name__ == "__main__":
         run_batch_only(a)
     elif a.workload.startswith("zipf4"):
         run_fo_only(a)
-    elif a.workload == "zipf-400m":
+    elif a.workload == "zipf-400m" or a.als:
         run_als_only(a)
     else:
         run_ours(a)
