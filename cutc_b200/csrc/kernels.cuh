@@ -1018,15 +1018,15 @@ __device__ __forceinline__ int als_solve_warp(const T (&G)[R][AlsShape<R>::C], c
 // triangle, forward/back substitution, one refinement step against the
 // FP32/FP64 Gram as accumulated).  Per system: factor (TRI doubles), b, y,
 // u (R doubles each), the Gram (TRI of T); per warp also NS row ids.
-// GS = R / 2 (32 at R = 64): two trailing-update columns per lane, and few
-// enough parked systems that the shared memory of a 4-warp block does not
-// hold the SM below what its registers allow (at R = 32, FP32: 2 systems,
-// 59 KB per block, 3 blocks = 12 warps per SM; 4 systems held it to 1).
-// Each factor element sees the same operations in the same order for any
-// GS, so the choice does not change results.
+// GS = R / 2 below rank 32, 32 from rank 32: few enough parked systems
+// that the shared memory of a 4-warp block does not hold the SM below what
+// its registers allow (at R = 32, FP32: one 7.4 KB system per warp, 4
+// blocks = 16 warps per SM; four systems per warp held it to 1 block, two
+// to 3).  Each factor element sees the same operations in the same order
+// for any GS, so the choice does not change results.
 template <typename T, int R>
 struct AlsBatch {
-    static constexpr int GS = R >= 64 ? 32 : (R >= 8 ? R / 2 : 2);
+    static constexpr int GS = R >= 32 ? 32 : (R >= 8 ? R / 2 : 2);
     static constexpr int NS = 32 / GS;
     static constexpr int TRI = R * (R + 1) / 2;
     static constexpr int gram_doubles = (TRI * (int)sizeof(T) + 7) / 8;
