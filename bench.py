@@ -249,7 +249,8 @@ def run_ours(args):
         p_sgd, tr_sgd = ctc.autotune(ctx, [tr[0]], p_sgd, cache_path=cache)
         tuned = {"search_s": time.time() - t0, "cache_hit": bool(tr_ccd and tr_ccd[0]["cached"]),
                  "ccdpp": {"tile_len": p_ccd.tile_len, "smem_budget": p_ccd.smem_budget, "trials": tr_ccd},
-                 "sgd": {"tile_len": p_sgd.tile_len, "threads_per_row": p_sgd.threads_per_row, "trials": tr_sgd}}
+                 "sgd": {"tile_len": p_sgd.tile_len, "threads_per_row": p_sgd.threads_per_row,
+                         "sgd_atomic": p_sgd.sgd_atomic, "trials": tr_sgd}}
     ds_ccd = ctc.Dataset(ctx, tr, None, te, p_ccd)
     ds_sgd = ctc.Dataset(ctx, [tr[0]], None, te, p_sgd)
     mdims = ds_ccd.dims()
@@ -351,7 +352,7 @@ def run_ours(args):
                                                                 **{"lambda": 0.1}))
         out["time_to_rmse"] = time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, args.seed, ds_als)
         ds_als.free()
-        out["e2e"] = e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args)
+        out["e2e"] = e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args, p_ccd, p_sgd)
         out["ciss_build"] = ciss_build_times(ctc, ctx, tr[0])
         v, s, threads, nsamp = cpu_baseline(base0, dims, R, args.sample, args.seed)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
@@ -570,13 +571,18 @@ def ciss_build_times(ctc, ctx, t0):
     return res
 
 
-def e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args):
+def e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args, p_ccd=None, p_sgd=None):
     """The same metric through the reference-facing call with host buffers:
     ctc_run on the mode-1 training tensor alone, as the reference's tc_ccd /
     tc_sgd take one training tensor and build their own copies (the
     records go to the device once; the other mode orders, tile plans and
     CCD++ slots are made there), then one epoch, evaluation and the factors
-    copied back, for CCD++ and for SGD."""
+    copied back, for CCD++ and for SGD, with the tuned tile length, lanes,
+    column staging and reduction mode when given (a tuning cache hit)."""
+
+    def knobs(p):
+        return {} if p is None else dict(tile_len=p.tile_len, threads_per_row=p.threads_per_row,
+                                         smem_budget=p.smem_budget, sgd_atomic=p.sgd_atomic)
     h2d = 2 * (n_train + n_test) * 16 + 2 * sum(mdims) * R * 4
     d2h = 2 * 2 * sum(mdims) * R * 4
     times = []
@@ -585,10 +591,10 @@ def e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args):
         m2 = ctc.Model(mdims, R).init_uniform(args.seed + 1, 1.0 / np.sqrt(R))
         t0 = time.perf_counter()
         ctc.run(ctx, [tr[0]], None, te, m1, ctc.params("ccdpp", rank=R, inner=3, iters=1, early_stop=0,
-                                                  eval_every=0, **{"lambda": 0.1}))
+                                                  eval_every=0, **knobs(p_ccd), **{"lambda": 0.1}))
         ctc.run(ctx, [tr[0]], None, te, m2, ctc.params("sgd", rank=R, lr=1e-3, lr_scale=1.0, iters=1,
                                                        lr_schedule=ctc.LR_CONSTANT, early_stop=0,
-                                                       eval_every=0, **{"lambda": 0.01}))
+                                                       eval_every=0, **knobs(p_sgd), **{"lambda": 0.01}))
         times.append(time.perf_counter() - t0)
     s = min(times)
     return {"value": 2 * n_train / s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),

@@ -16,6 +16,7 @@ library must have been built (python -m cutc_b200.build).
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import os
 from dataclasses import dataclass, field
 
@@ -73,7 +74,7 @@ class FoParams(C.Structure):
 
 class TuneTrial(C.Structure):
     _fields_ = [("tile_len", C.c_int), ("threads_per_row", C.c_int), ("smem_budget", C.c_int),
-                ("ms_epoch", C.c_double), ("cached", C.c_int)]
+                ("ms_epoch", C.c_double), ("cached", C.c_int), ("sgd_atomic", C.c_int)]
 
 
 TUNE_FORCE, TUNE_NO_WRITE = 1, 2
@@ -192,6 +193,10 @@ class Context:
         _check(lib().ctc_ctx_create(device, C.byref(h)))
         self.h = h
         self.device = device
+        self._deps = weakref.WeakSet()  # datasets, batches, first-order states on this context
+
+    def _track(self, obj):
+        self._deps.add(obj)
 
     def launches(self) -> int:
         n = C.c_uint64()
@@ -215,7 +220,13 @@ class Context:
         _check(lib().ctc_ctx_reset_kernel_times(self.h))
 
     def close(self):
+        """Frees every object still living on this context, then the context."""
         if self.h:
+            for d in list(self._deps):
+                try:
+                    d.free()
+                except Exception:
+                    pass
             lib().ctc_ctx_destroy(self.h)
             self.h = None
 
@@ -479,6 +490,7 @@ class Dataset:
                                         test.h if test else None, C.byref(p), C.byref(h)))
         self.h = h
         self.ctx = ctx
+        ctx._track(self)
 
     def run(self, model: Model, p: Params, best: Model | None = None, callback=None) -> RunOutput:
         out = RunOutput(result={})
@@ -627,6 +639,7 @@ class Batch:
         _check(lib().ctc_batch_create(ctx.h, n, tr, te, C.byref(p), C.byref(h)))
         self.h = h
         self.ctx = ctx
+        ctx._track(self)
         self.ninst = n
 
     def info(self):
@@ -717,6 +730,7 @@ class FirstOrder:
         _check(lib().ctc_fo_create(ctx.h, train.h, test.h if test else None, C.byref(p), C.byref(h)))
         self.h = h
         self.ctx = ctx
+        ctx._track(self)
 
     def dims(self):
         order = C.c_int()

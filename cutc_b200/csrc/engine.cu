@@ -572,6 +572,12 @@ struct Session : SessionBase {
             for (int m = 0; m < 3; ++m) Ubf[m].alloc((size_t)dims[m] * R);
             CK(cudaFuncSetAttribute(tc::k_als_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
         }
+        if (p.alg == CTC_ALG_SGD && std::is_same<T, float>::value) {
+            // bulk row reductions stage 2 x 3 rows per group in shared memory
+            set_sgd_smem<1>();
+            set_sgd_smem<2>();
+            set_sgd_smem<4>();
+        }
         if (p.alg == CTC_ALG_ALS) {
             using Sh = k::AlsShape<R>;
             const int smem = (int)(4 * Sh::smem_doubles * sizeof(double));
@@ -841,6 +847,16 @@ struct Session : SessionBase {
         return 1;
     }
     int sgd_groups_per_block() const { return 8 * (32 / (R / k::Vec<T>::n / sgd_vectors())); }
+    template <int C>
+    void set_sgd_smem()
+    {
+        if constexpr ((R / k::Vec<T>::n) % C == 0 && R / k::Vec<T>::n / C <= 32) {
+            const int gpb = 8 * (32 / (R / k::Vec<T>::n / C));
+            const int smem = gpb * 2 * 3 * R * (int)sizeof(T);
+            if (smem > 48 * 1024)
+                CK(cudaFuncSetAttribute(k::k_sgd<T, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        }
+    }
 
     void sgd_epoch()
     {
@@ -870,8 +886,11 @@ struct Session : SessionBase {
                     break;
                 }
         }
+        // bulk row reductions: two staged deltas of three rows per group
+        const bool bulk = !seq && p.sgd_atomic == 2 && std::is_same<T, float>::value;
+        const size_t smem = bulk ? (size_t)gpb * 2 * 3 * R * sizeof(T) : 0;
         if constexpr ((R / k::Vec<T>::n) % C == 0)
-            LAUNCH(ctx, k::k_sgd<T, R, C>, g, seq ? 32 : 256, 0, (const uint4 *)c.rec.p, (const double *)c.v64.p,
+            LAUNCH(ctx, k::k_sgd<T, R, C>, g, seq ? 32 : 256, smem, (const uint4 *)c.rec.p, (const double *)c.v64.p,
                    c.n, tile_len, c.ntiles, U[0].p, U[1].p, U[2].p, (const T *)lr_dev.p, (T)p.lambda, p.sgd_atomic,
                    seq ? 1 : 0, stride, d0, d1, d2);
     }
@@ -1298,7 +1317,7 @@ extern "C" int ctc_params_default(int alg, ctc_params *p)
         p->tolerance = 1e-4;          // TOLERANCE, base.h:36
         p->max_bad_epochs = 3;        // MAX_BADEPOCHS, base.h:32
         p->sgd_order = CTC_SGD_HOGWILD;
-        p->sgd_atomic = 1;
+        p->sgd_atomic = 2;
         p->eval_every = 1;
     });
 }
@@ -1842,7 +1861,7 @@ extern "C" int ctc_batch_run(ctc_batch *B, ctc_model *const *models, const ctc_p
 namespace ctc {
 
 struct TuneCand {
-    int tile_len = 0, threads_per_row = 0, smem_budget = 0;
+    int tile_len = 0, threads_per_row = 0, smem_budget = 0, sgd_atomic = 0;
 };
 
 // shape key: algorithm, precision, rank, compat, SGD order, dimensions and
@@ -1869,8 +1888,8 @@ static bool tune_read(const char *path, const std::string &key, TuneCand &c, dou
         char k[300];
         TuneCand t;
         double x = 0;
-        if (sscanf(line, "%299s tile_len=%d threads_per_row=%d smem_budget=%d ms=%lf", k, &t.tile_len,
-                   &t.threads_per_row, &t.smem_budget, &x) == 5 &&
+        if (sscanf(line, "%299s tile_len=%d threads_per_row=%d smem_budget=%d sgd_atomic=%d ms=%lf", k,
+                   &t.tile_len, &t.threads_per_row, &t.smem_budget, &t.sgd_atomic, &x) == 6 &&
             key == k) {
             c = t;  // the last entry for a key wins
             ms = x;
@@ -1897,19 +1916,20 @@ static void tune_write(const char *path, const std::string &key, const TuneCand 
     FILE *f = fopen(path, "w");
     if (!f) fail(CTC_E_IO, "cannot write the tuning cache %s", path);
     for (const std::string &l : keep) fputs(l.c_str(), f);
-    fprintf(f, "%s tile_len=%d threads_per_row=%d smem_budget=%d ms=%.6f\n", key.c_str(), c.tile_len,
-            c.threads_per_row, c.smem_budget, ms);
+    fprintf(f, "%s tile_len=%d threads_per_row=%d smem_budget=%d sgd_atomic=%d ms=%.6f\n", key.c_str(),
+            c.tile_len, c.threads_per_row, c.smem_budget, c.sgd_atomic, ms);
     fclose(f);
 }
 
 static std::vector<TuneCand> tune_space(const ctc_params &p)
 {
     std::vector<TuneCand> v;
-    auto add = [&](int t, int c, int s) {
+    auto add = [&](int t, int c, int s, int a = -1) {
         TuneCand x;
         x.tile_len = t;
         x.threads_per_row = c;
         x.smem_budget = s;
+        x.sgd_atomic = a < 0 ? p.sgd_atomic : a;
         v.push_back(x);
     };
     switch (p.alg) {
@@ -1931,9 +1951,19 @@ static std::vector<TuneCand> tune_space(const ctc_params &p)
             add(p.tile_len, 0, 0);
             break;
         }
+        // FP32: vector atomic adds or bulk row reductions (which one is
+        // faster depends on how hot the hottest rows are)
+        const bool f32 = p.precision != CTC_PREC_F64;
         for (int t : {128, 256, 512, 1024})
             for (int c : {base, base / 2, base / 4})
-                if (c >= 1) add(t, c, 0);
+                if (c >= 1) {
+                    if (f32 && p.sgd_atomic != 0) {
+                        add(t, c, 0, 1);
+                        add(t, c, 0, 2);
+                    } else {
+                        add(t, c, 0);
+                    }
+                }
         break;
     }
     }
@@ -1972,6 +2002,7 @@ extern "C" int ctc_tune_lookup(const char *cache_path, const ctc_tensor *train, 
         out->tile_len = c.tile_len;
         out->threads_per_row = c.threads_per_row;
         out->smem_budget = c.smem_budget;
+        out->sgd_atomic = c.sgd_atomic;
     });
 }
 
@@ -1991,7 +2022,8 @@ extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], cons
         double best_ms = 0;
         if (!(flags & CTC_TUNE_FORCE) && tune_read(cache_path, key, best, best_ms)) {
             if (trials && max_trials > 0) {
-                trials[0] = ctc_tune_trial{best.tile_len, best.threads_per_row, best.smem_budget, best_ms, 1};
+                trials[0] = ctc_tune_trial{best.tile_len, best.threads_per_row, best.smem_budget, best_ms, 1,
+                                           best.sgd_atomic};
                 nt = 1;
             }
         } else {
@@ -2027,6 +2059,7 @@ extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], cons
                     if (c.tile_len != tl) continue;
                     q.threads_per_row = c.threads_per_row;
                     q.smem_budget = c.smem_budget;
+                    q.sgd_atomic = c.sgd_atomic;
                     ds->p = q;
                     S->set_params(q);
                     S->set_model(&mdl);
@@ -2039,7 +2072,8 @@ extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], cons
                     CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
                     const double per = ms / 2.0;
                     if (trials && nt < max_trials)
-                        trials[nt] = ctc_tune_trial{c.tile_len, c.threads_per_row, c.smem_budget, per, 0};
+                        trials[nt] = ctc_tune_trial{c.tile_len, c.threads_per_row, c.smem_budget, per, 0,
+                                                    c.sgd_atomic};
                     ++nt;
                     if (per < best_ms) {
                         best_ms = per;
@@ -2053,6 +2087,7 @@ extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], cons
         out->tile_len = best.tile_len;
         out->threads_per_row = best.threads_per_row;
         out->smem_budget = best.smem_budget;
+        out->sgd_atomic = best.sgd_atomic;
         if (ntrials) *ntrials = nt;
     });
 }

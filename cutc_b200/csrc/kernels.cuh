@@ -289,6 +289,13 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
         ngroups = 1;
     }
     const T s = *lr_dev;
+    // atomic == 2 (FP32 Hogwild): a nonzero's three row deltas are staged in
+    // the group's shared buffer (two of them, alternating) and added by
+    // three bulk reductions of whole rows, issued by the group's lane 0
+    extern __shared__ __align__(16) unsigned char sgd_smem[];
+    const bool bulk = std::is_same<T, float>::value && atomic == 2 && !sequential;
+    T *gbuf = reinterpret_cast<T *>(sgd_smem) + (size_t)((threadIdx.x >> 5) * GPW + gw) * (2 * 3 * R);
+    uint32_t nstaged = 0;
     for (uint64_t t = group; t < ntiles; t += ngroups) {
         // Hogwild: tiles in flight together are spread over the tensor
         // (tile_stride is coprime to ntiles), so a long row of the sorted
@@ -309,7 +316,7 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
                 // by the updates in flight
                 arow = reinterpret_cast<V *>(U0 + (size_t)r.x * R) + gl * C;
 #pragma unroll
-                for (int q = 0; q < C; ++q) a0[q] = a[q] = arow[q];
+                for (int q = 0; q < C; ++q) a0[q] = a[q] = bulk ? __ldcg(arow + q) : arow[q];
             } else if (r.x != cur) {
                 if (arow)
 #pragma unroll
@@ -322,10 +329,12 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
             V *brow = reinterpret_cast<V *>(U1 + (size_t)r.y * R) + gl * C;
             V *crow = reinterpret_cast<V *>(U2 + (size_t)r.z * R) + gl * C;
             V b[C], c[C];
+            // bulk reductions are applied at L2 and leave stale lines in L1,
+            // so that mode reads the rows from L2
 #pragma unroll
             for (int q = 0; q < C; ++q) {
-                b[q] = brow[q];
-                c[q] = crow[q];
+                b[q] = bulk ? __ldcg(brow + q) : brow[q];
+                c[q] = bulk ? __ldcg(crow + q) : crow[q];
             }
             T part = 0;
 #pragma unroll
@@ -341,6 +350,12 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
                 sb *= (T)damp1[r.y];
                 sc *= (T)damp2[r.z];
             }
+            T *buf = gbuf + (nstaged & 1) * (3 * R);
+            if (bulk) {
+                // the buffer staged two nonzeros ago has been read by its reductions
+                if (gl == 0) px::bulk_wait_read<1>();
+                __syncwarp(gmask);
+            }
 #pragma unroll
             for (int q = 0; q < C; ++q) {
                 V an, db, dc;
@@ -355,9 +370,16 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
                     V da;
 #pragma unroll
                     for (int v = 0; v < VN; ++v) vset(da, v, vget(an, v) - vget(a0[q], v));
-                    vatomic_add(arow + q, da);
-                    vatomic_add(brow + q, db);
-                    vatomic_add(crow + q, dc);
+                    if (bulk) {
+                        V *sb3 = reinterpret_cast<V *>(buf) + gl * C + q;
+                        sb3[0] = da;
+                        sb3[R / VN] = db;
+                        sb3[2 * (R / VN)] = dc;
+                    } else {
+                        vatomic_add(arow + q, da);
+                        vatomic_add(brow + q, db);
+                        vatomic_add(crow + q, dc);
+                    }
                 } else {
                     V bn, cn;
 #pragma unroll
@@ -371,11 +393,25 @@ __global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
                 }
                 a[q] = an;
             }
+            if constexpr (std::is_same<T, float>::value) {
+                if (bulk) {
+                    px::fence_proxy_async_smem();
+                    __syncwarp(gmask);
+                    if (gl == 0) {
+                        px::bulk_reduce_add_f32(U0 + (size_t)r.x * R, buf, R * sizeof(float));
+                        px::bulk_reduce_add_f32(U1 + (size_t)r.y * R, buf + R, R * sizeof(float));
+                        px::bulk_reduce_add_f32(U2 + (size_t)r.z * R, buf + 2 * R, R * sizeof(float));
+                        px::bulk_commit();
+                    }
+                    ++nstaged;
+                }
+            }
         }
         if (sequential && arow)
 #pragma unroll
             for (int q = 0; q < C; ++q) arow[q] = a[q];
     }
+    if (bulk && gl == 0) px::bulk_wait_all();
 }
 
 // ---------------------------------------------------------------------

@@ -206,7 +206,10 @@ typedef struct {
     int mode_start;        /* first mode of the rotation (reference: rand()%3,
                               sgpu/als.cu:684-685; fixed here)                      */
     int sgd_order;         /* enum ctc_sgd_order                                    */
-    int sgd_atomic;        /* Hogwild: 1 = atomic adds, 0 = plain stores            */
+    int sgd_atomic;        /* Hogwild: 2 = each nonzero's three row deltas added by
+                              three bulk row reductions from shared memory (FP32;
+                              the default), 1 = vector atomic adds, 0 = plain
+                              stores                                                */
     int eval_every;        /* evaluate RMSE every n epochs (0 = only at the end)    */
     int use_graph;         /* capture the epoch in a CUDA graph when possible       */
     uint64_t seed;         /* reserved for stochastic modes                          */
@@ -320,7 +323,8 @@ int ctc_batch_run(ctc_batch *b, ctc_model *const *models, const ctc_params *p, c
  * half powers of two), the algorithm, precision and rank of `p` and this
  * device's SM count, it times update epochs over a candidate set: tile
  * length (ALS, CCD, CCD++, SGD), lanes per nonzero (SGD threads_per_row),
- * CCD++ column staging on/off (smem_budget), and writes the fastest into
+ * the FP32 Hogwild reduction mode (SGD sgd_atomic 1 or 2), CCD++ column
+ * staging on/off (smem_budget), and writes the fastest into
  * `out` (a copy of `p` with those fields replaced).  With cache_path, a
  * cached entry for the shape is returned without a search (unless
  * CTC_TUNE_FORCE), and a search stores its winner there (unless
@@ -332,6 +336,7 @@ typedef struct {
     int tile_len, threads_per_row, smem_budget;
     double ms_epoch;   /* device time of one update epoch */
     int cached;
+    int sgd_atomic;    /* SGD: the Hogwild reduction mode tried */
 } ctc_tune_trial;
 int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], const ctc_params *p,
                  const char *cache_path, int flags, ctc_params *out, ctc_tune_trial *trials,

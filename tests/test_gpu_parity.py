@@ -266,13 +266,15 @@ def test_sgd_sequential_f32_trajectory(ctx):
         assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-3, e
 
 
-def test_sgd_hogwild_final_rmse(ctx):
-    """Hogwild with atomic adds: final test RMSE within 0.5 % of the
+@pytest.mark.parametrize("atomic,R", [(1, 32), (2, 32), (2, 8), (2, 64)])
+def test_sgd_hogwild_final_rmse(ctx, atomic, R):
+    """Hogwild with vector atomic adds (1) or bulk row reductions from
+    shared memory (2, the default): final test RMSE within 0.5 % of the
     deterministic sequential order."""
-    P = Problem(200000, (2000, 1500, 200), 32, seed=13)
+    P = Problem(200000, (2000, 1500, 200), R, seed=13)
     U, hist = oracle_sgd(P, 10, 0.01, 0.01, decay=0.95)
     G, out = engine_run(ctx, P, ctc.SGD, 10, precision=ctc.PREC_F32, sgd_order=ctc.SGD_HOGWILD,
-                        sgd_atomic=1, lr=0.01, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY,
+                        sgd_atomic=atomic, lr=0.01, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY,
                         lr_decay=0.95, **{"lambda": 0.01})
     assert abs(out.epochs[-1]["rmse_te"] - hist[-1][1]) / hist[-1][1] < 0.005
 

@@ -16,13 +16,16 @@ def test_tune_sgd_searches_caches_and_hits(ctx, tmp_path):
     p = ctc.params(ctc.SGD, rank=16, lr=0.01, lr_scale=1.0, **{"lambda": 0.01})
     path = str(tmp_path / "tune.txt")
     q, trials = ctc.autotune(ctx, P.c_sorted(), p, cache_path=path)
-    assert len(trials) == 12 and all(t["cached"] == 0 and t["ms_epoch"] > 0 for t in trials)
-    assert q.tile_len in (128, 256, 512, 1024) and q.threads_per_row in (4, 2, 1)
+    # tile length x lanes per nonzero x reduction mode (vector atomics, bulk rows)
+    assert len(trials) == 24 and all(t["cached"] == 0 and t["ms_epoch"] > 0 for t in trials)
+    assert {t["sgd_atomic"] for t in trials} == {1, 2}
+    assert q.tile_len in (128, 256, 512, 1024) and q.threads_per_row in (4, 2, 1) and q.sgd_atomic in (1, 2)
     best = min(trials, key=lambda t: t["ms_epoch"])
-    assert (q.tile_len, q.threads_per_row) == (best["tile_len"], best["threads_per_row"])
+    assert (q.tile_len, q.threads_per_row, q.sgd_atomic) == (best["tile_len"], best["threads_per_row"],
+                                                             best["sgd_atomic"])
     q2, trials2 = ctc.autotune(ctx, P.c_sorted(), p, cache_path=path)
     assert len(trials2) == 1 and trials2[0]["cached"] == 1
-    assert (q2.tile_len, q2.threads_per_row) == (q.tile_len, q.threads_per_row)
+    assert (q2.tile_len, q2.threads_per_row, q2.sgd_atomic) == (q.tile_len, q.threads_per_row, q.sgd_atomic)
     assert ctc.tune_lookup(path, P.c_sorted()[0], p) is not None
 
 

@@ -33,11 +33,13 @@ def test_lookup_hit_miss_and_last_entry_wins(tmp_path):
     with open(path, "w") as f:
         f.write("garbage line\n")
         f.write("alg=9,other 1 2 3\n")
-        f.write(f"{key} tile_len=128 threads_per_row=0 smem_budget=-1 ms=1.5\n")
-        f.write(f"{key} tile_len=512 threads_per_row=0 smem_budget=0 ms=1.2\n")
+        f.write(f"{key} tile_len=128 threads_per_row=0 smem_budget=-1 sgd_atomic=1 ms=1.5\n")
+        f.write(f"{key} tile_len=512 threads_per_row=0 smem_budget=0 sgd_atomic=2 ms=1.2\n")
+        # a line without the reduction mode (an older cache) is not an entry
+        f.write(f"{key} tile_len=256 threads_per_row=0 smem_budget=0 ms=1.0\n")
     q = ctc.tune_lookup(path, t, p)
     assert q is not None
-    assert (q.tile_len, q.threads_per_row, q.smem_budget) == (512, 0, 0)
+    assert (q.tile_len, q.threads_per_row, q.smem_budget, q.sgd_atomic) == (512, 0, 0, 2)
     # everything else is the caller's
     assert q.rank == 32 and q.alg == ctc.CCDPP and abs(q.lambda_ - p.lambda_) == 0
     assert ctc.tune_lookup(path, t, ctc.params(ctc.CCDPP, rank=16)) is None
