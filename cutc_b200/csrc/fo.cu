@@ -149,10 +149,17 @@ static void fo_pass(ctc_fo *f, const uint4 *idx, const float *val, uint64_t b, u
     }
     a.priv_elems = priv;
     a.scale = scale;
+    // bulk row reductions: two staged slots of D rows per nonzero group
+    a.bulk = GRAD ? 1 : 0;
+    constexpr int kGroups = 8 * (32 / (R / fo::Gather<float, GT>::VE));
+    const size_t smem = (priv + (GRAD ? (size_t)kGroups * 2 * D * R : 0)) * sizeof(float);
+    if (smem > 48 * 1024)
+        CK(cudaFuncSetAttribute(fo::k_fo<float, GT, R, D, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
     const unsigned g = grid_for(e - b, 256, kMaxPartials);
     // named apart so that per-kernel times separate the adjoint from evaluation
-    launch_named(ctx, GRAD ? "fo::k_fo_grad" : "fo::k_fo_eval", fo::k_fo<float, GT, R, D, GRAD>, g, 256,
-                 priv * sizeof(float), a, ctx->partial.p);
+    launch_named(ctx, GRAD ? "fo::k_fo_grad" : "fo::k_fo_eval", fo::k_fo<float, GT, R, D, GRAD>, g, 256, smem, a,
+                 ctx->partial.p);
 }
 
 template <int R, int D>

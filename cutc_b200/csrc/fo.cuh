@@ -74,6 +74,7 @@ struct FoArgs {
     uint32_t priv_off[4];   // their offset in shared memory (elements)
     uint32_t priv_elems;    // total privatised elements
     double scale;           // data-term gradient scale (nonzeros / batch size)
+    int bulk;               // 1: gradient rows of the other modes added by bulk row reductions
 };
 
 __device__ __forceinline__ void red_add4(float *p, float a, float b, float c, float d)
@@ -94,7 +95,7 @@ __global__ void __launch_bounds__(256) k_fo(FoArgs a, double *__restrict__ parti
     constexpr int GPW = 32 / GL;
     static_assert(GL >= 1 && 32 % GL == 0, "lanes per nonzero");
     constexpr bool kPriv = GRAD && std::is_same<T, float>::value;
-    extern __shared__ float fo_smem[];
+    extern __shared__ __align__(16) float fo_smem[];
     const int lane = threadIdx.x & 31;
     const int gl = lane % GL, gw = lane / GL;
     const uint32_t gmask = (GL == 32) ? 0xffffffffu : (((1u << GL) - 1u) << (gw * GL));
@@ -105,6 +106,14 @@ __global__ void __launch_bounds__(256) k_fo(FoArgs a, double *__restrict__ parti
     const uint64_t group = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * GPW + gw;
     const uint64_t ngroups = (((uint64_t)gridDim.x * blockDim.x) >> 5) * GPW;
     const T *vals = static_cast<const T *>(a.val);
+    // bulk mode (FP32): a nonzero's gradient rows of the modes not kept in
+    // shared memory are staged in the group's slot (two, alternating) and
+    // added by one bulk reduction per mode, issued by the group's lane 0;
+    // nothing reads G during the pass, so the reductions can land late
+    const bool bulk = kPriv && a.bulk;
+    float *stage = fo_smem + a.priv_elems +
+                   (size_t)((threadIdx.x >> 5) * GPW + gw) * (2 * D * R);
+    uint32_t nstaged = 0;
     double obj = 0;
     for (uint64_t p = a.begin + group; p < a.end; p += ngroups) {
         const uint4 ix = a.idx[p];
@@ -128,6 +137,12 @@ __global__ void __launch_bounds__(256) k_fo(FoArgs a, double *__restrict__ parti
         if (gl == 0) obj += 0.5 * (double)e * (double)e;
         if constexpr (GRAD) {
             const T se = -e * (T)a.scale;
+            float *buf = stage + (nstaged & 1) * (D * R);
+            if (bulk) {
+                // the slot staged two nonzeros ago has been read by its reductions
+                if (gl == 0) px::bulk_wait_read<1>();
+                __syncwarp(gmask);
+            }
 #pragma unroll
             for (int m = 0; m < D; ++m) {
                 T g[VE];
@@ -150,6 +165,13 @@ __global__ void __launch_bounds__(256) k_fo(FoArgs a, double *__restrict__ parti
                 }
                 T *dst = static_cast<T *>(a.G[m]) + off;
                 if constexpr (std::is_same<T, float>::value) {
+                    if (bulk) {
+#pragma unroll
+                        for (int v = 0; v < VE; v += 4)
+                            *reinterpret_cast<float4 *>(buf + m * R + gl * VE + v) =
+                                make_float4(g[v], g[v + 1], g[v + 2], g[v + 3]);
+                        continue;
+                    }
 #pragma unroll
                     for (int v = 0; v < VE; v += 4) red_add4(dst + v, g[v], g[v + 1], g[v + 2], g[v + 3]);
                 } else {
@@ -157,8 +179,24 @@ __global__ void __launch_bounds__(256) k_fo(FoArgs a, double *__restrict__ parti
                     for (int v = 0; v < VE; ++v) atomicAdd(dst + v, g[v]);
                 }
             }
+            if constexpr (kPriv) {
+                if (bulk) {
+                    px::fence_proxy_async_smem();
+                    __syncwarp(gmask);
+                    if (gl == 0) {
+#pragma unroll
+                        for (int m = 0; m < D; ++m)
+                            if (!a.priv[m])
+                                px::bulk_reduce_add_f32(static_cast<float *>(a.G[m]) + (size_t)row[m] * R,
+                                                        buf + m * R, R * sizeof(float));
+                        px::bulk_commit();
+                    }
+                    ++nstaged;
+                }
+            }
         }
     }
+    if (bulk && gl == 0) px::bulk_wait_all();
     obj = k::block_sum(obj);
     if (threadIdx.x == 0) partial[blockIdx.x] = obj;
     if constexpr (kPriv) {
