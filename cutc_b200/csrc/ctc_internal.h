@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <functional>
 #include <vector>
 
 namespace ctc {
@@ -41,6 +42,8 @@ int guarded(F &&fn)
 
 // Number of host threads used by the parallel host passes.
 int host_threads();
+// task(0 .. ntasks-1) on the persistent host workers and the calling thread
+void host_run(int ntasks, const std::function<void(int)> &task);
 
 // Row-aligned work tiles over one mode-sorted copy of the nonzeros.
 //   light tile: whole rows packed up to `tile_len` nonzeros (heavy == -1)

@@ -3,6 +3,9 @@
 #include "ctc_internal.h"
 
 #include <algorithm>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -37,6 +40,87 @@ int host_threads()
     return n;
 }
 
+// Persistent host workers (host_threads() - 1 of them; the calling thread
+// works too): parallel loops over staging chunks no longer create and join
+// a thread set per call.  One job runs at a time; callers from several
+// threads queue on run_mu, and a loop started inside a task runs inline.
+namespace {
+thread_local bool tl_in_task = false;
+
+struct HostPool {
+    std::mutex run_mu, mu;
+    std::condition_variable cv_start, cv_done;
+    const std::function<void(int)> *job = nullptr;
+    int ntasks = 0, next = 0, pending = 0;
+    uint64_t gen = 0;
+    bool stop = false;
+    std::vector<std::thread> workers;
+
+    explicit HostPool(int nworkers)
+    {
+        for (int i = 0; i < nworkers; ++i) workers.emplace_back([this] { loop(); });
+    }
+    ~HostPool()
+    {
+        {
+            std::lock_guard<std::mutex> l(mu);
+            stop = true;
+        }
+        cv_start.notify_all();
+        for (auto &t : workers) t.join();
+    }
+    // take tasks of the current job until none is left (mu held on entry and exit)
+    void drain(std::unique_lock<std::mutex> &l)
+    {
+        while (next < ntasks) {
+            const int t = next++;
+            const std::function<void(int)> *f = job;
+            l.unlock();
+            tl_in_task = true;
+            (*f)(t);
+            tl_in_task = false;
+            l.lock();
+            if (--pending == 0) cv_done.notify_all();
+        }
+    }
+    void loop()
+    {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> l(mu);
+        for (;;) {
+            cv_start.wait(l, [&] { return stop || gen != seen; });
+            if (stop) return;
+            seen = gen;
+            drain(l);
+        }
+    }
+    void run(int n, const std::function<void(int)> &f)
+    {
+        std::lock_guard<std::mutex> g(run_mu);
+        std::unique_lock<std::mutex> l(mu);
+        job = &f;
+        ntasks = n;
+        next = 0;
+        pending = n;
+        ++gen;
+        cv_start.notify_all();
+        drain(l);
+        cv_done.wait(l, [&] { return pending == 0; });
+        job = nullptr;
+    }
+};
+}  // namespace
+
+void host_run(int ntasks, const std::function<void(int)> &task)
+{
+    static HostPool pool(host_threads() - 1);
+    if (ntasks <= 1 || host_threads() == 1 || tl_in_task) {
+        for (int t = 0; t < ntasks; ++t) task(t);
+        return;
+    }
+    pool.run(ntasks, task);
+}
+
 template <typename F>
 static void parallel_for(uint64_t n, F &&fn)
 {
@@ -45,12 +129,8 @@ static void parallel_for(uint64_t n, F &&fn)
         fn(0, 0, n);
         return;
     }
-    std::vector<std::thread> th;
-    for (int p = 0; p < P; ++p) {
-        uint64_t b = n * p / P, e = n * (p + 1) / P;
-        th.emplace_back([&, p, b, e] { fn(p, b, e); });
-    }
-    for (auto &t : th) t.join();
+    const std::function<void(int)> task = [&](int p) { fn(p, n * p / P, n * (p + 1) / P); };
+    host_run(P, task);
 }
 
 // ------------------------------------------------------------------

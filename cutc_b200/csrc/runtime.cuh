@@ -90,12 +90,8 @@ static void par_for(uint64_t n, F &&fn)
         fn((uint64_t)0, n);
         return;
     }
-    std::vector<std::thread> th;
-    for (int p = 0; p < P; ++p) {
-        uint64_t b = n * p / P, e = n * (p + 1) / P;
-        th.emplace_back([&, b, e] { fn(b, e); });
-    }
-    for (auto &t : th) t.join();
+    const std::function<void(int)> task = [&](int p) { fn(n * p / P, n * (p + 1) / P); };
+    host_run(P, task);
 }
 
 template <typename F>
