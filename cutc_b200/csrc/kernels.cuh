@@ -779,7 +779,11 @@ __device__ __forceinline__ void key_modes(uint64_t k, const KeyShape &ks, int m,
     idx[(m + 2) % 3] = q2;
 }
 
-// res = x - sum_f U0(i0,f) U1(i1,f) U2(i2,f), row-major factors
+// res = x - sum_f U0(i0,f) U1(i1,f) U2(i2,f), row-major factors.  A warp
+// reads 32 consecutive slots (keys and values) with coalesced loads, then
+// walks them with groups of R / VN lanes per slot, lane gl reading the
+// 16-byte slice gl of each row (whole rows per warp load), and a butterfly
+// sum; unused slot entries (kPadKey) keep their zero residual.
 template <typename T, int R>
 __global__ void __launch_bounds__(256) k_ccdpp_init(const uint64_t *__restrict__ keys, const T *__restrict__ x,
                                                     T *__restrict__ res, uint32_t n, KeyShape ks, int m,
@@ -788,22 +792,39 @@ __global__ void __launch_bounds__(256) k_ccdpp_init(const uint64_t *__restrict__
 {
     using V = typename Vec<T>::type;
     constexpr int VN = Vec<T>::n;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        const uint64_t key = keys[p];
-        if (key == kPadKey) continue;  // unused slot entry: residual stays 0
-        uint32_t idx[3];
-        key_modes(key, ks, m, idx);
-        const V *a = reinterpret_cast<const V *>(U0 + (size_t)idx[0] * R);
-        const V *b = reinterpret_cast<const V *>(U1 + (size_t)idx[1] * R);
-        const V *c = reinterpret_cast<const V *>(U2 + (size_t)idx[2] * R);
-        T s = 0;
-#pragma unroll
-        for (int q = 0; q < R / VN; ++q) {
-            const V va = a[q], vb = b[q], vc = c[q];
-#pragma unroll
-            for (int v = 0; v < VN; ++v) s += vget(va, v) * vget(vb, v) * vget(vc, v);
+    constexpr int GL = R / VN;
+    constexpr int GPW = 32 / GL;
+    static_assert(GL >= 1 && 32 % GL == 0, "lanes per slot");
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % GL, gw = lane / GL;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t base = warp * 32; base < n; base += nwarps * 32) {
+        const uint64_t mine = base + lane;
+        uint64_t key = kPadKey;  // past the end: treated as a pad
+        T xv = 0;
+        if (mine < n) {
+            key = keys[mine];
+            xv = x[mine];
         }
-        res[p] = x[p] - s;
+#pragma unroll 4
+        for (int j = 0; j < GL; ++j) {
+            const int src = j * GPW + gw;
+            const uint64_t k = __shfl_sync(0xffffffffu, key, src);
+            const T xs = __shfl_sync(0xffffffffu, xv, src);
+            const bool real = k != kPadKey;
+            uint32_t idx[3] = {0u, 0u, 0u};  // row 0 for pads: in bounds, result unused
+            if (real) key_modes(k, ks, m, idx);
+            const V va = reinterpret_cast<const V *>(U0 + (size_t)idx[0] * R)[gl];
+            const V vb = reinterpret_cast<const V *>(U1 + (size_t)idx[1] * R)[gl];
+            const V vc = reinterpret_cast<const V *>(U2 + (size_t)idx[2] * R)[gl];
+            T p = 0;
+#pragma unroll
+            for (int v = 0; v < VN; ++v) p += vget(va, v) * vget(vb, v) * vget(vc, v);
+#pragma unroll
+            for (int o = GL / 2; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+            if (real && gl == 0) res[base + src] = xs - p;
+        }
     }
 }
 
