@@ -303,3 +303,19 @@ def test_plan_rejects_unsorted_indices():
     for runs in (False, True):
         with pytest.raises(ctc.CtcError):
             ctc.plan_tiles(ind, 32, from_runs=runs)
+
+
+def test_sort_through_the_host_worker_pool_is_numpys_stable_sort():
+    """ctc_tensor_sort on 300k nonzeros (large enough that its copies run on
+    the persistent host workers), three modes in a row: numpy's stable
+    (mode, next mode) order, values included."""
+    rng = np.random.default_rng(7)
+    n, dims = 300_000, (5000, 4000, 300)
+    ind = np.stack([rng.integers(1, d + 1, n) for d in dims]).astype(np.uint64)
+    vals = rng.random(n)
+    for m in range(3):
+        t = ctc.Tensor.from_coo(ind, vals, dims=dims)
+        api._check(api.lib().ctc_tensor_sort(t.h, m))
+        gi, gv = t.export()
+        o = np.lexsort((ind[(m + 1) % 3], ind[m]))
+        assert np.array_equal(gi, ind[:, o]) and np.array_equal(gv, vals[o]), m
