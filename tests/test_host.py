@@ -319,3 +319,28 @@ def test_sort_through_the_host_worker_pool_is_numpys_stable_sort():
         gi, gv = t.export()
         o = np.lexsort((ind[(m + 1) % 3], ind[m]))
         assert np.array_equal(gi, ind[:, o]) and np.array_equal(gv, vals[o]), m
+
+
+@pytest.mark.parametrize("case", ["tile_1", "rows_of_exactly_T", "one_row", "n_at_chunk_threshold"])
+def test_plan_edge_cases_agree(case):
+    """Edge cases of the two planners: tile length 1 (every row of more than
+    one nonzero becomes pieces), rows exactly one tile long, a single row
+    (all pieces), and n = 2^20 (the smallest chunked plan)."""
+    rng = np.random.default_rng(11)
+    if case == "tile_1":
+        ind, T = np.sort(rng.integers(1, 50, 3000)).astype(np.uint64), 1
+    elif case == "rows_of_exactly_T":
+        T = 64
+        ind = np.repeat(np.arange(1, 201, dtype=np.uint64), T)
+    elif case == "one_row":
+        ind, T = np.full(10000, 7, dtype=np.uint64), 256
+    else:
+        ind, T = _zipf_rows(1 << 20, 30000, seed=5), 256
+    ta, ha = ctc.plan_tiles(ind, T, from_runs=False)
+    tb, hb = ctc.plan_tiles(ind, T, from_runs=True)
+    assert np.array_equal(ta, tb) and np.array_equal(ha, hb)
+    assert int(ta[:, 1].sum()) == ind.size and np.all(ta[:, 1] <= T)
+    if case == "rows_of_exactly_T":
+        assert len(ha) == 0 and np.all(ta[:, 1] == T)  # a row of exactly T is one light tile
+    if case == "one_row":
+        assert len(ha) == 1 and ha[0][0] == 6 and ha[0][2] == len(ta)
