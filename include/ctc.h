@@ -256,8 +256,13 @@ typedef struct {
 /* Replaces tc_als / tc_sgd / tc_ccd (sgpu/als.cuh:20-33, sgd.cuh:18-32,
  * ccd.cuh:20-33) and tc_main_ciss (sgpu/completion.c:422-497):
  * train[m] is the training tensor sorted for mode m (the reference's
- * traina/b/c); train[1], train[2] may be NULL (sorted copies are then made
- * internally).  val/test may be NULL.  `model` holds the initial factors
+ * traina/b/c); train[1], train[2] may be NULL: those copies are then sorted
+ * on the device from train[0] in ctc_tensor_sort's order (stable by the
+ * mode index, then the next mode's), so a run with only train[0] equals
+ * one with the three host-sorted copies.  CCD++ orders the nonzeros of
+ * each row further by the other two indices (the larger mode first),
+ * whichever copies are given.  Only train[0] crosses PCIe when the others
+ * are NULL.  val/test may be NULL.  `model` holds the initial factors
  * and receives the final ones; `best` (may be NULL) receives the factors of
  * the best validation epoch (tc_converge's best_mats).  Everything is
  * staged to the device inside the call and released before it returns. */
