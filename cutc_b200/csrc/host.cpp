@@ -3,6 +3,7 @@
 #include "ctc_internal.h"
 
 #include <algorithm>
+#include <charconv>
 #include <condition_variable>
 #include <functional>
 #include <mutex>
@@ -137,6 +138,46 @@ static void parallel_for(uint64_t n, F &&fn)
 // .tns text reader
 // ------------------------------------------------------------------
 
+// Token parsers with strtoul / strtod semantics.  The common form
+// (optional blanks, plain decimal digits, a separator or the line end after
+// the token) goes through std::from_chars, which is correctly rounded like
+// glibc's strtod and several times faster; anything else (a sign, a hex
+// float, a token glued to other text) is handed to strtoul / strtod
+// unchanged, so every input parses as the reference's reader parses it.
+static inline bool token_end(const char *p, const char *end)
+{
+    return p >= end || *p == ' ' || *p == '\t' || *p == '\r' || *p == '\0';
+}
+
+static inline uint64_t parse_index(char *&ptr, const char *end)
+{
+    const char *q = ptr;
+    while (q < end && (*q == ' ' || *q == '\t')) ++q;
+    uint64_t v = 0;
+    const auto r = std::from_chars(q, end, v, 10);
+    if (r.ec == std::errc() && token_end(r.ptr, end)) {
+        ptr = const_cast<char *>(r.ptr);
+        return v;
+    }
+    return strtoul(ptr, &ptr, 10);
+}
+
+static inline double parse_value(char *&ptr, const char *end)
+{
+    const char *q = ptr;
+    while (q < end && (*q == ' ' || *q == '\t')) ++q;
+    // digits only (inf / nan spellings and their NaN payloads stay strtod's)
+    const char *d = (q < end && *q == '-') ? q + 1 : q;
+    if (d >= end || !((*d >= '0' && *d <= '9') || *d == '.')) return strtod(ptr, &ptr);
+    double v = 0;
+    const auto r = std::from_chars(q, end, v);
+    if (r.ec == std::errc() && token_end(r.ptr, end)) {
+        ptr = const_cast<char *>(r.ptr);
+        return v;
+    }
+    return strtod(ptr, &ptr);
+}
+
 // Restates sgpu/io.c:234-308 (tt_get_dims) + io.c:58-106 (p_tt_read_file):
 // the mode count comes from the first data line split on " \t" (the value
 // token and the trailing newline token excluded), a data line is one whose
@@ -194,14 +235,12 @@ static void read_tns(const char *path, ctc_tensor &t)
         while (c < N && data[c - 1] != '\n') ++c;
         cut[p] = std::max(c, cut[p - 1]);
     }
-    // NUL-terminate lines so a short line cannot run into the next one
-    for (size_t i = 0; i < N; ++i)
-        if (data[i] == '\n') data[i] = '\0';
-
     auto is_data = [&](size_t p, size_t e) {
         size_t len = e - p + (e < N ? 1 : 0);
         return len > 1 && data[p] != '#';
     };
+    // count the data lines of each chunk, NUL-terminating its lines on the
+    // way so a short line cannot run into the next one
     std::vector<uint64_t> count(P, 0);
     std::vector<std::thread> th;
     for (int p = 0; p < P; ++p)
@@ -210,7 +249,8 @@ static void read_tns(const char *path, ctc_tensor &t)
             size_t q = cut[p];
             while (q < cut[p + 1]) {
                 size_t e = q;
-                while (e < N && data[e] != '\0') ++e;
+                while (e < N && data[e] != '\n' && data[e] != '\0') ++e;
+                if (e < N) data[e] = '\0';
                 if (is_data(q, e)) ++c;
                 q = e + 1;
             }
@@ -236,13 +276,14 @@ static void read_tns(const char *path, ctc_tensor &t)
                 while (e < N && data[e] != '\0') ++e;
                 if (is_data(q, e)) {
                     char *ptr = data + q;
+                    const char *end = data + e;
                     for (int m = 0; m < nmodes; ++m) {
-                        uint64_t v = strtoul(ptr, &ptr, 10);
+                        uint64_t v = parse_index(ptr, end);
                         t.ind[m][n] = v;
                         if (v > mx[p * 4 + m]) mx[p * 4 + m] = v;
                         if (v < mn[p * 4 + m]) mn[p * 4 + m] = v;
                     }
-                    t.vals[n] = strtod(ptr, &ptr);
+                    t.vals[n] = parse_value(ptr, end);
                     ++n;
                 }
                 q = e + 1;

@@ -92,6 +92,54 @@ def test_tns_reader_large_parallel_matches_oracle(tmp_path):
     assert a.dims == b.dims
 
 
+_TOKEN_LINES = [
+    "1 2 3 4.5", "# a comment", "", "  7\t8 9 1e5", "+3 4 5 +2.5", "10 11 12 0x1p3", "2 3 4 -0.0",
+    "5 6 7 .25\r", "18446744073709551615 1 1 3", "4 5 6 1.7976931348623157e308", "4 5 6 4.9e-324",
+    "6 6 6 1e-400", "7 7 7 inf", "7 7 8 -nan", "8 9 10 12abc", "3 4 5 1.5e", "9 9 9 0.1000000000000000055511151231257827",
+    "1 1 1 123456789012345678901234567890", "2 2 2 -3.25E-2",
+]
+
+
+def _reference_parse(lines, nmodes):
+    """Each data line through libc's strtoul / strtod, chained as the
+    reference's reader chains them (sgpu/io.c:58-106)."""
+    import ctypes as C
+    libc = C.CDLL(None)
+    libc.strtoul.restype, libc.strtod.restype = C.c_ulong, C.c_double
+    libc.strtoul.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int]
+    libc.strtod.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    ind, vals = [], []
+    for line in lines:
+        if len(line) + 1 <= 1 or line.startswith("#"):
+            continue
+        buf = C.create_string_buffer(line.encode())
+        ptr = C.c_void_p(C.addressof(buf))
+        row = []
+        for _ in range(nmodes):
+            end = C.c_void_p()
+            row.append(libc.strtoul(ptr, C.byref(end), 10))
+            ptr = end
+        end = C.c_void_p()
+        vals.append(libc.strtod(ptr, C.byref(end)))
+        ind.append(row)
+    return np.array(ind, dtype=np.uint64).T, np.array(vals, dtype=np.float64)
+
+
+@pytest.mark.parametrize("repeat", [1, 40000])
+def test_tns_token_forms_parse_as_strtoul_strtod(tmp_path, repeat):
+    """Blanks, tabs, signs, hex floats, CRLF, overflow, subnormals,
+    underflow, inf / nan and tokens glued to text: the reader's values equal
+    libc's strtoul / strtod bit for bit (repeat = 40000 makes the file large
+    enough for the chunked parallel parse)."""
+    p = tmp_path / "forms.tns"
+    p.write_bytes(("\n".join(_TOKEN_LINES * repeat) + "\n").encode())
+    a = ctc.tt_read(str(p))
+    ia, va = a.export()
+    ib, vb = _reference_parse(_TOKEN_LINES * repeat, 3)
+    assert np.array_equal(ia, ib)
+    assert np.array_equal(va.view(np.uint64), vb.view(np.uint64))
+
+
 def test_tns_first_line_token_rule(tmp_path):
     """The mode count comes from strtok on the first data line, so trailing
     whitespace there adds a mode (sgpu/io.c:249-257) -- in both readers."""
