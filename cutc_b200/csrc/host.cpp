@@ -2,10 +2,15 @@
 // builder, reference lane multiplicities, work-tile planning, factor models.
 #include "ctc_internal.h"
 
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <charconv>
 #include <condition_variable>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <atomic>
 #include <cmath>
@@ -186,20 +191,37 @@ static inline double parse_value(char *&ptr, const char *end)
 // parallel over line-aligned chunks.
 static void read_tns(const char *path, ctc_tensor &t)
 {
-    FILE *f = fopen(path, "rb");
-    if (!f) fail(CTC_E_IO, "cannot open '%s'", path);
-    fseek(f, 0, SEEK_END);
-    long sz = ftell(f);
-    fseek(f, 0, SEEK_SET);
-    std::vector<char> buf((size_t)sz + 1);
-    if (sz > 0 && fread(buf.data(), 1, (size_t)sz, f) != (size_t)sz) {
-        fclose(f);
-        fail(CTC_E_IO, "short read on '%s'", path);
+    const int fd = open(path, O_RDONLY);
+    if (fd < 0) fail(CTC_E_IO, "cannot open '%s'", path);
+    struct stat st;
+    if (fstat(fd, &st) != 0) {
+        close(fd);
+        fail(CTC_E_IO, "cannot stat '%s'", path);
     }
-    fclose(f);
-    buf[(size_t)sz] = '\0';
-    char *data = buf.data();
-    const size_t N = (size_t)sz;
+    const size_t N = (size_t)st.st_size;
+    // an uninitialised buffer, read by byte ranges on the host threads
+    std::unique_ptr<char[]> buf(new char[N + 1]);
+    char *data = buf.get();
+    {
+        const int RP = N < ((size_t)8 << 20) ? 1 : host_threads();
+        std::atomic<int> short_read{0};
+        const std::function<void(int)> rd = [&](int p) {
+            size_t b = N * (size_t)p / RP;
+            const size_t e = N * (size_t)(p + 1) / RP;
+            while (b < e) {
+                const ssize_t r = pread(fd, data + b, e - b, (off_t)b);
+                if (r <= 0) {
+                    short_read = 1;
+                    return;
+                }
+                b += (size_t)r;
+            }
+        };
+        host_run(RP, rd);
+        close(fd);
+        if (short_read) fail(CTC_E_IO, "short read on '%s'", path);
+    }
+    data[N] = '\0';
 
     // mode count from the first data line (reference counts strtok tokens
     // on " \t", where the last token carries the newline, then subtracts 1)
