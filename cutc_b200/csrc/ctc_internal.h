@@ -8,6 +8,8 @@
 #include <stdexcept>
 #include <string>
 #include <functional>
+#include <memory>
+#include <utility>
 #include <vector>
 
 namespace ctc {
@@ -75,12 +77,40 @@ struct ctc_tensor {
     std::vector<double> vals;
 };
 
+namespace ctc {
+// An allocator whose value-less construct leaves the element uninitialised:
+// vectors that are filled right after resize (in parallel, or by a
+// device-to-host copy) skip a serial zero fill.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept
+    {
+    }
+    template <typename U>
+    void construct(U *p) noexcept
+    {
+        ::new ((void *)p) U;
+    }
+    template <typename U, typename... A>
+    void construct(U *p, A &&...a)
+    {
+        ::new ((void *)p) U(std::forward<A>(a)...);
+    }
+};
+}  // namespace ctc
+
 struct ctc_ciss {
     uint64_t nnz = 0, dlength = 0, size_rows = 0;
     int tile_len = 32;
     std::vector<uint64_t> directory, dcounter;
-    std::vector<double> entries;
-    std::vector<uint8_t> written;
+    std::vector<double, ctc::NoInitAlloc<double>> entries;  // every slot is written by the builders
+    std::vector<uint8_t, ctc::NoInitAlloc<uint8_t>> written;
 };
 
 struct ctc_model {

@@ -389,74 +389,117 @@ static void build_ciss(const ctc_tensor &t, int mode, int T, bool ga, ctc_ciss &
     const uint64_t *im = t.ind[mode].data();
     const uint64_t *ij = t.ind[(mode + 1) % 3].data();
     const uint64_t *ik = t.ind[(mode + 2) % 3].data();
-    // directory: distinct mode indices in order of appearance (ciss.c:89-115)
-    std::vector<uint64_t> dir;
-    dir.reserve(1024);
-    dir.push_back(im[0]);
-    for (uint64_t m = 1; m < nnz; ++m)
-        if (im[m] != dir.back()) dir.push_back(im[m]);
+    const double *vals = t.vals.data();
+    c.nnz = nnz;
+    c.tile_len = T;
+    const uint64_t ntiles = nnz / (uint64_t)T + 1;  // the last one holds the terminator
+    c.size_rows = ntiles + nnz + 1;
+    const uint64_t cap = c.size_rows * 3;
+    // The reference loop (ciss.c:89-195) is sequential, but a tile depends on
+    // the tiles before it only through the directory index of the row of the
+    // nonzero just before it.  Chunks of whole tiles therefore run that loop
+    // in parallel once a first pass has counted each chunk's row changes;
+    // with one chunk it is the reference loop itself.
+    int P = host_threads();
+    if (nnz < ((uint64_t)1 << 18)) P = 1;
+    if ((uint64_t)P > ntiles) P = (int)ntiles;
+    std::vector<uint64_t> tb(P + 1), mb(P + 1), changes(P, 0), base(P + 1, 0);
+    for (int q = 0; q <= P; ++q) {
+        tb[q] = ntiles * (uint64_t)q / (uint64_t)P;
+        mb[q] = q == P ? nnz : std::min<uint64_t>(tb[q] * (uint64_t)T, nnz);
+    }
+    const std::function<void(int)> count = [&](int q) {
+        uint64_t k = 0;
+        for (uint64_t m = std::max<uint64_t>(mb[q], 1); m < mb[q + 1]; ++m) k += im[m] != im[m - 1];
+        changes[q] = k;
+    };
+    host_run(P, count);
+    for (int q = 0; q < P; ++q) base[q + 1] = base[q] + changes[q];
+    // directory: distinct mode indices in order of appearance (ciss.c:89-115);
     // dcounter[0] = 0 and dcounter[k] = start(slice k) - 1, the inclusive end
     // of slice k-1, which is what the reference's running counter
     // (ciss.c:97-114) accumulates; the last slot is nnz-1 (ciss.c:110).
-    c.dlength = dir.size();
-    c.directory = dir;
+    // ga/ciss.c:101-120 starts its running count at the first nonzero, so
+    // there the counters are one larger: dcounter[k] = start(slice k).
+    c.dlength = 1 + base[P];
+    c.directory.assign(c.dlength, 0);
     c.dcounter.assign(c.dlength + 1, 0);
-    {
-        uint64_t k = 0;
-        for (uint64_t m = 1; m < nnz; ++m)
-            if (im[m] != im[m - 1]) c.dcounter[++k] = ga ? m : m - 1;
-        // ga/ciss.c:101-120 starts its running count at the first nonzero,
-        // so there the counters are one larger: dcounter[k] = start(slice k)
-        c.dcounter[c.dlength] = nnz - 1;
-    }
-    c.nnz = nnz;
-    c.tile_len = T;
-    const uint64_t tilesize = nnz / (uint64_t)T + 1;
-    c.size_rows = tilesize + nnz + 1;
-    const uint64_t cap = c.size_rows * 3;
-    c.entries.assign(cap, 0.0);
-    c.written.assign(cap, 0);
+    c.directory[0] = im[0];
+    const std::function<void(int)> fill_dir = [&](int q) {
+        uint64_t k = base[q];
+        for (uint64_t m = std::max<uint64_t>(mb[q], 1); m < mb[q + 1]; ++m)
+            if (im[m] != im[m - 1]) {
+                ++k;
+                c.directory[k] = im[m];
+                c.dcounter[k] = ga ? m : m - 1;
+            }
+    };
+    host_run(P, fill_dir);
+    c.dcounter[c.dlength] = nnz - 1;
+    const uint64_t *dir = c.directory.data();
+    c.entries.resize(cap);
+    c.written.resize(cap);
     double *E = c.entries.data();
     uint8_t *Wr = c.written.data();
-    uint64_t npos = 0, nl = 0, m = 0;
-    auto put = [&](uint64_t off, double v) {
-        uint64_t o = npos + off;
-        if (o >= cap) fail(CTC_E_ARG, "CISS layout overflow");
-        E[o] = v;
-        Wr[o] = 1;
-    };
-    while (m < nnz + 1) {
-        uint64_t bitmap = 1;
-        uint64_t ns = nl;
-        uint64_t niv = dir[ns];
-        uint64_t lc = 1;
-        put(0, -1.0 * (double)ns);
-        while (lc <= (uint64_t)T) {
-            if (m == nnz) {
-                put(lc * 3, -1.0);
-                put(lc * 3 + 1, -1.0);
-                put(lc * 3 + 2, -1.0);
+    std::atomic<int> overflow{0};
+    const uint64_t row3 = ((uint64_t)T + 1) * 3;
+    const std::function<void(int)> tiles = [&](int q) {
+        // this chunk's tile rows start zeroed (slots the loop leaves unwritten
+        // stay 0); the last chunk also clears the unused tail
+        const uint64_t z0 = std::min(tb[q] * row3, cap);
+        const uint64_t z1 = q == P - 1 ? cap : std::min(tb[q + 1] * row3, cap);
+        std::fill(E + z0, E + z1, 0.0);
+        std::fill(Wr + z0, Wr + z1, (uint8_t)0);
+        uint64_t m = mb[q];
+        uint64_t nl = m == 0 ? 0 : base[q];  // directory index of the row of nonzero m - 1
+        uint64_t npos = tb[q] * row3;
+        const uint64_t mend = q == P - 1 ? nnz + 1 : mb[q + 1];
+        bool bad = false;
+        auto put = [&](uint64_t off, double v) {
+            const uint64_t o = npos + off;
+            if (o >= cap) {
+                bad = true;
+                return;
+            }
+            E[o] = v;
+            Wr[o] = 1;
+        };
+        while (m < mend) {
+            uint64_t bitmap = 1;
+            uint64_t ns = nl;
+            uint64_t niv = dir[ns];
+            uint64_t lc = 1;
+            put(0, -1.0 * (double)ns);
+            while (lc <= (uint64_t)T) {
+                if (m == nnz) {
+                    put(lc * 3, -1.0);
+                    put(lc * 3 + 1, -1.0);
+                    put(lc * 3 + 2, -1.0);
+                    m++;
+                    break;
+                }
+                uint64_t ti = im[m];
+                if (ti == niv) {
+                    bitmap = (bitmap << 1) + 1;
+                } else {
+                    bitmap = bitmap << 1;
+                    niv = ti;
+                    nl++;
+                    put(1, -1.0 * (double)nl);
+                }
+                put(lc * 3, (double)ij[m]);
+                put(lc * 3 + 1, (double)ik[m]);
+                put(lc * 3 + 2, (double)value_through_idx(vals[m]));
+                put(2, (double)bitmap);
                 m++;
-                break;
+                lc++;
             }
-            uint64_t ti = im[m];
-            if (ti == niv) {
-                bitmap = (bitmap << 1) + 1;
-            } else {
-                bitmap = bitmap << 1;
-                niv = ti;
-                nl++;
-                put(1, -1.0 * (double)nl);
-            }
-            put(lc * 3, (double)ij[m]);
-            put(lc * 3 + 1, (double)ik[m]);
-            put(lc * 3 + 2, (double)value_through_idx(t.vals[m]));
-            put(2, (double)bitmap);
-            m++;
-            lc++;
+            npos += row3;
         }
-        npos += ((uint64_t)T + 1) * 3;
-    }
+        if (bad) overflow = 1;
+    };
+    host_run(P, tiles);
+    if (overflow) fail(CTC_E_ARG, "CISS layout overflow");
 }
 
 static uint64_t brev64(uint64_t x)

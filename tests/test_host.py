@@ -392,3 +392,59 @@ def test_plan_edge_cases_agree(case):
         assert len(ha) == 0 and np.all(ta[:, 1] == T)  # a row of exactly T is one light tile
     if case == "one_row":
         assert len(ha) == 1 and ha[0][0] == 6 and ha[0][2] == len(ta)
+
+
+def _sorted_random(n, dims, seed, mode):
+    rng = np.random.default_rng(seed)
+    ind = np.stack([rng.integers(1, d + 1, n) for d in dims]).astype(np.uint64)
+    vals = rng.uniform(-2, 6, n)
+    o = np.lexsort((ind[(mode + 1) % 3], ind[mode]))
+    return ind[:, o].copy(), vals[o].copy()
+
+
+@pytest.mark.skipif(not po.ref_host_available(), reason="reference host library not built")
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_parallel_ciss_equals_the_reference_builder_on_a_large_tensor(mode):
+    """1.5M nonzeros: the host builder runs in chunks of tiles in parallel;
+    every written slot equals the reference's own ciss_alloc bit for bit."""
+    dims = (40000, 3000, 200)
+    ind, vals = _sorted_random(1_500_000, dims, 21 + mode, mode)
+    got = ctc.ciss_alloc(ctc.Tensor.from_coo(ind, vals, dims=dims), mode + 1, 32)
+    ref = po.ref_ciss_alloc(po.Tensor(ind, vals, list(dims)), mode + 1)
+    w = got["written"]
+    assert got["size_rows"] == ref["size_rows"]
+    assert np.array_equal(got["directory"], ref["directory"]) and np.array_equal(got["dcounter"], ref["dcounter"])
+    assert np.array_equal(got["entries"].view(np.uint64)[w], ref["entries"].view(np.uint64)[w])
+
+
+_SERIAL_CISS = """
+import sys, numpy as np
+sys.path.insert(0, {root!r})
+import cutc_b200 as ctc
+z = np.load({src!r})
+c = ctc.ciss_alloc(ctc.Tensor.from_coo(z["ind"], z["vals"], dims=[int(x) for x in z["dims"]]),
+                   {mode}, {T}, ga={ga})
+np.savez({dst!r}, **{{k: v for k, v in c.items() if isinstance(v, np.ndarray)}})
+"""
+
+
+@pytest.mark.parametrize("T,ga", [(1, True), (16, True), (63, True), (32, False)])
+def test_parallel_ciss_equals_the_serial_loop(tmp_path, T, ga):
+    """The chunked builder against the same build on one host thread (the
+    reference loop as written), everything compared: written slots,
+    unwritten zeros and the written mask, GA counters and odd tile lengths."""
+    import subprocess
+    import sys
+    dims = (30000, 2000, 100)
+    ind, vals = _sorted_random(1_200_000, dims, 33, 0)
+    src, dst = str(tmp_path / "t.npz"), str(tmp_path / "serial.npz")
+    np.savez(src, ind=ind, vals=vals, dims=np.array(dims))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = _SERIAL_CISS.format(root=root, src=src, dst=dst, mode=1, T=T, ga=ga)
+    env = dict(os.environ, CTC_HOST_THREADS="1")
+    subprocess.run([sys.executable, "-c", code], env=env, check=True, timeout=600)
+    serial = np.load(dst)
+    got = ctc.ciss_alloc(ctc.Tensor.from_coo(ind, vals, dims=dims), 1, T, ga=ga)
+    for k in ("directory", "dcounter", "written"):
+        assert np.array_equal(got[k], serial[k]), k
+    assert np.array_equal(got["entries"].view(np.uint64), serial["entries"].view(np.uint64))
