@@ -826,6 +826,88 @@ extern "C" int ctc_tensor_export(const ctc_tensor *t, uint64_t *const *ind, doub
     });
 }
 
+// perm = the stable order of the pairs (k1[i], k2[i]).  When both fit one
+// 64-bit key (k1 << bits(k2) | k2), a parallel LSD radix sort: per-thread
+// digit histograms, offsets digit-major and thread-minor, and an in-order
+// scatter of each thread's chunk keep equal keys in input order.  Small or
+// wider inputs take the comparison sort.
+static void stable_order(const uint64_t *k1, const uint64_t *k2, uint64_t n, std::vector<uint64_t> &perm)
+{
+    perm.resize(n);
+    auto comparison = [&] {
+        std::iota(perm.begin(), perm.end(), 0);
+        __gnu_parallel::stable_sort(perm.begin(), perm.end(), [&](uint64_t a, uint64_t b) {
+            return k1[a] < k1[b] || (k1[a] == k1[b] && k2[a] < k2[b]);
+        });
+    };
+    const int P = host_threads();
+    if (n < 65536 || P == 1) return comparison();
+    std::vector<uint64_t> mx1(P, 0), mx2(P, 0);
+    const std::function<void(int)> maxima = [&](int q) {
+        uint64_t a = 0, b = 0;
+        for (uint64_t i = n * q / P; i < n * (q + 1) / P; ++i) {
+            a = std::max(a, k1[i]);
+            b = std::max(b, k2[i]);
+        }
+        mx1[q] = a;
+        mx2[q] = b;
+    };
+    host_run(P, maxima);
+    auto bits = [](uint64_t v) {
+        int b = 0;
+        while (b < 64 && (v >> b)) ++b;
+        return b;
+    };
+    const int b1 = bits(*std::max_element(mx1.begin(), mx1.end()));
+    const int b2 = bits(*std::max_element(mx2.begin(), mx2.end()));
+    const int B = b1 + b2;
+    if (B > 64) return comparison();
+    std::vector<uint64_t, NoInitAlloc<uint64_t>> key(n), key2(n), id2(n);  // filled before read
+    uint64_t *id = perm.data();
+    const std::function<void(int)> pack = [&](int q) {
+        for (uint64_t i = n * q / P; i < n * (q + 1) / P; ++i) {
+            key[i] = b2 == 64 ? k2[i] : ((b1 ? k1[i] << b2 : 0) | k2[i]);
+            id[i] = i;
+        }
+    };
+    host_run(P, pack);
+    const int passes = (B + 11) / 12;
+    const int D = passes ? (B + passes - 1) / passes : 0;
+    const uint64_t NB = (uint64_t)1 << D;
+    std::vector<uint64_t> hist((size_t)P * NB);
+    uint64_t *src_k = key.data(), *dst_k = key2.data(), *src_i = id, *dst_i = id2.data();
+    for (int pass = 0; pass < passes; ++pass) {
+        const int shift = pass * D;
+        const uint64_t mask = NB - 1;
+        const std::function<void(int)> histo = [&](int q) {
+            uint64_t *h = hist.data() + (size_t)q * NB;
+            std::fill(h, h + NB, 0);
+            for (uint64_t i = n * q / P; i < n * (q + 1) / P; ++i) ++h[(src_k[i] >> shift) & mask];
+        };
+        host_run(P, histo);
+        uint64_t run = 0;
+        for (uint64_t d = 0; d < NB; ++d)
+            for (int q = 0; q < P; ++q) {
+                uint64_t &h = hist[(size_t)q * NB + d];
+                const uint64_t c = h;
+                h = run;
+                run += c;
+            }
+        const std::function<void(int)> scatter = [&](int q) {
+            uint64_t *o = hist.data() + (size_t)q * NB;
+            for (uint64_t i = n * q / P; i < n * (q + 1) / P; ++i) {
+                const uint64_t at = o[(src_k[i] >> shift) & mask]++;
+                dst_k[at] = src_k[i];
+                dst_i[at] = src_i[i];
+            }
+        };
+        host_run(P, scatter);
+        std::swap(src_k, dst_k);
+        std::swap(src_i, dst_i);
+    }
+    if (src_i != id) std::copy(src_i, src_i + n, id);
+}
+
 extern "C" int ctc_tensor_sort(ctc_tensor *t, int mode)
 {
     return guarded([&] {
@@ -833,11 +915,8 @@ extern "C" int ctc_tensor_sort(ctc_tensor *t, int mode)
         const uint64_t n = t->nnz;
         const uint64_t *k1 = t->ind[mode].data();
         const uint64_t *k2 = t->ind[(mode + 1) % t->nmodes].data();
-        std::vector<uint64_t> perm(n);
-        std::iota(perm.begin(), perm.end(), 0);
-        __gnu_parallel::stable_sort(perm.begin(), perm.end(), [&](uint64_t a, uint64_t b) {
-            return k1[a] < k1[b] || (k1[a] == k1[b] && k2[a] < k2[b]);
-        });
+        std::vector<uint64_t> perm;
+        stable_order(k1, k2, n, perm);
         std::vector<uint64_t> tmp(n);
         for (int m = 0; m < t->nmodes; ++m) {
             const uint64_t *src = t->ind[m].data();

@@ -448,3 +448,26 @@ def test_parallel_ciss_equals_the_serial_loop(tmp_path, T, ga):
     for k in ("directory", "dcounter", "written"):
         assert np.array_equal(got[k], serial[k]), k
     assert np.array_equal(got["entries"].view(np.uint64), serial["entries"].view(np.uint64))
+
+
+@pytest.mark.parametrize("case", ["duplicates", "zero_and_large", "wide_keys"])
+def test_radix_sort_cases_are_numpys_stable_sort(case):
+    """Many equal pairs (stability), 0 indices with indices near 2^32, and
+    pairs too wide for one 64-bit key (the comparison sort)."""
+    rng = np.random.default_rng(12)
+    n = 200_000
+    if case == "duplicates":
+        ind = np.stack([rng.integers(1, 9, n), rng.integers(1, 5, n), rng.integers(1, 1000, n)]).astype(np.uint64)
+    elif case == "zero_and_large":
+        ind = np.stack([rng.integers(0, 3, n), rng.integers(2**32 - 50, 2**32 + 50, n),
+                        rng.integers(0, 7, n)]).astype(np.uint64)
+    else:
+        ind = np.stack([rng.integers(2**40, 2**40 + 9, n), rng.integers(2**39, 2**39 + 7, n),
+                        rng.integers(1, 5, n)]).astype(np.uint64)
+    vals = rng.random(n)
+    for m in range(3):
+        t = ctc.Tensor.from_coo(ind, vals)
+        api._check(api.lib().ctc_tensor_sort(t.h, m))
+        gi, gv = t.export()
+        o = np.lexsort((ind[(m + 1) % 3], ind[m]))
+        assert np.array_equal(gi, ind[:, o]) and np.array_equal(gv, vals[o]), (case, m)
