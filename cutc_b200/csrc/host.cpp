@@ -1090,19 +1090,33 @@ extern "C" int ctc_model_write_text(const ctc_model *m, int mode, const char *pa
         const double *v = m->U[mode].data();
         const uint64_t I = m->dims[mode];
         const int R = m->rank;
-        std::string line;
-        char buf[40];
-        for (uint64_t i = 0; i < I; ++i) {
-            line.clear();
-            for (int j = 0; j < R; ++j) {
-                snprintf(buf, sizeof buf, "%+0.8le ", v[i * (uint64_t)R + j]);
-                line += buf;
-            }
-            line += '\n';
-            if (fwrite(line.data(), 1, line.size(), f) != line.size()) {
-                fclose(f);
-                fail(CTC_E_IO, "write to %s failed", path);
-            }
+        // blocks of rows formatted on the host threads, written in order:
+        // the same bytes as one row after another
+        const int P = host_threads();
+        const uint64_t kRows = 8192;
+        std::vector<std::string> out(P);
+        bool ok = true;
+        for (uint64_t r0 = 0; r0 < I && ok; r0 += kRows * (uint64_t)P) {
+            const std::function<void(int)> fmt = [&](int q) {
+                std::string &o = out[q];
+                o.clear();
+                const uint64_t b = std::min(I, r0 + kRows * (uint64_t)q), e = std::min(I, b + kRows);
+                char buf[40];
+                for (uint64_t i = b; i < e; ++i) {
+                    for (int j = 0; j < R; ++j) {
+                        const int k = snprintf(buf, sizeof buf, "%+0.8le ", v[i * (uint64_t)R + j]);
+                        o.append(buf, (size_t)k);
+                    }
+                    o += '\n';
+                }
+            };
+            host_run(P, fmt);
+            for (int q = 0; q < P && ok; ++q)
+                ok = fwrite(out[q].data(), 1, out[q].size(), f) == out[q].size();
+        }
+        if (!ok) {
+            fclose(f);
+            fail(CTC_E_IO, "write to %s failed", path);
         }
         if (fclose(f) != 0) fail(CTC_E_IO, "closing %s failed", path);
     });

@@ -290,6 +290,19 @@ def test_factor_text_matches_reference_mat_write(tmp_path):
         assert open(ours, "rb").read() == open(ref, "rb").read()
 
 
+def test_large_factor_text_matches_reference_mat_write(tmp_path):
+    """200k rows: the rows are formatted in parallel blocks and written in
+    order; the file is the reference's byte for byte."""
+    rng = np.random.default_rng(6)
+    U = rng.standard_normal((200_000, 16)) * 10.0 ** rng.integers(-8, 8, (200_000, 16))
+    m = ctc.Model([200_000, 3, 2], 16)
+    m.set_factors([U, np.zeros((3, 16)), np.zeros((2, 16))])
+    ours, ref = str(tmp_path / "ours.txt"), str(tmp_path / "ref.txt")
+    m.write_text(0, ours)
+    _ref_mat_write(U, ref)
+    assert open(ours, "rb").read() == open(ref, "rb").read()
+
+
 def test_model_checkpoint_round_trip_and_rejects_bad_files(tmp_path):
     rng = np.random.default_rng(5)
     for dims in ([11, 7, 5], [6, 5, 4, 3]):
