@@ -338,14 +338,38 @@ static void read_bin(const char *path, ctc_tensor &t)
         t.nmodes = (int)nm;
         t.nnz = nnz;
         ok = fread(t.dims, 8, nm, f) == nm;
-        for (uint32_t m = 0; ok && m < nm; ++m) {
+    }
+    if (ok) {
+        // the arrays follow the header: read by byte ranges on the host threads
+        const off_t off0 = (off_t)(4 + 4 + 4 + 8 + 8 * (uint64_t)nm);
+        const int fd = fileno(f);
+        std::vector<char *> dst;
+        for (uint32_t m = 0; m < nm; ++m) {
             t.ind[m].resize(nnz);
-            ok = fread(t.ind[m].data(), 8, nnz, f) == nnz;
+            dst.push_back(reinterpret_cast<char *>(t.ind[m].data()));
         }
-        if (ok) {
-            t.vals.resize(nnz);
-            ok = fread(t.vals.data(), 8, nnz, f) == nnz;
-        }
+        t.vals.resize(nnz);
+        dst.push_back(reinterpret_cast<char *>(t.vals.data()));
+        const uint64_t bytes = nnz * 8;
+        const int P = bytes < ((uint64_t)4 << 20) ? 1 : host_threads();
+        std::atomic<int> short_read{0};
+        const std::function<void(int)> rd = [&](int q) {
+            for (size_t a = 0; a < dst.size(); ++a) {
+                uint64_t b = bytes * (uint64_t)q / P;
+                const uint64_t e = bytes * (uint64_t)(q + 1) / P;
+                const off_t base = off0 + (off_t)(a * bytes);
+                while (b < e) {
+                    const ssize_t r = pread(fd, dst[a] + b, e - b, base + (off_t)b);
+                    if (r <= 0) {
+                        short_read = 1;
+                        return;
+                    }
+                    b += (uint64_t)r;
+                }
+            }
+        };
+        host_run(P, rd);
+        ok = !short_read;
     }
     fclose(f);
     if (!ok) fail(CTC_E_IO, "'%s' is not a valid CTCB tensor file", path);

@@ -80,6 +80,23 @@ def test_binary_roundtrip(tmp_path):
         ctc.tt_read(str(tmp_path / "bad.ctcb"))
 
 
+def test_binary_large_roundtrip_and_truncation(tmp_path):
+    """A file read by byte ranges on the host threads: exact round trip; a
+    truncated file is rejected."""
+    rng = np.random.default_rng(9)
+    n = 600_000
+    ind = np.stack([rng.integers(1, d + 1, n) for d in (900, 800, 700)]).astype(np.uint64)
+    vals = rng.standard_normal(n)
+    p = str(tmp_path / "big.ctcb")
+    ctc.Tensor.from_coo(ind, vals).save_bin(p)
+    i2, v2 = ctc.tt_read(p).export()
+    assert np.array_equal(i2, ind) and np.array_equal(v2.view(np.uint64), vals.view(np.uint64))
+    q = tmp_path / "cut.ctcb"
+    q.write_bytes(open(p, "rb").read()[:-8])
+    with pytest.raises(ctc.CtcError):
+        ctc.tt_read(str(q))
+
+
 def test_tns_reader_large_parallel_matches_oracle(tmp_path):
     """A file big enough for the parallel chunked parse (> 1 MiB)."""
     ind, vals = synth.random_small(60000, (500, 400, 300), seed=4)
