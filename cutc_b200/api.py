@@ -74,7 +74,8 @@ class FoParams(C.Structure):
 
 class TuneTrial(C.Structure):
     _fields_ = [("tile_len", C.c_int), ("threads_per_row", C.c_int), ("smem_budget", C.c_int),
-                ("ms_epoch", C.c_double), ("cached", C.c_int), ("sgd_atomic", C.c_int)]
+                ("ms_epoch", C.c_double), ("cached", C.c_int), ("sgd_atomic", C.c_int),
+                ("threads_per_block", C.c_int)]
 
 
 TUNE_FORCE, TUNE_NO_WRITE = 1, 2
@@ -102,6 +103,9 @@ def lib():
             "ctc_ctx_stream": (P, [P]),
             "ctc_tensor_load_tns": (C.c_int, [C.c_char_p, C.POINTER(P)]),
             "ctc_tensor_save_bin": (C.c_int, [P, C.c_char_p]),
+            "ctc_tensor_save_splatt": (C.c_int, [P, C.c_char_p]),
+            "ctc_tensor_write_tns": (C.c_int, [P, C.c_char_p, C.c_int]),
+            "ctc_tensor_split": (C.c_int, [P, C.c_uint64, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
             "ctc_tensor_from_coo": (C.c_int, [C.c_int, C.c_uint64, _u64p, C.POINTER(_u64p), _f64p, C.POINTER(P)]),
             "ctc_tensor_info": (C.c_int, [P, C.POINTER(C.c_int), _u64p, _u64p]),
             "ctc_tensor_export": (C.c_int, [P, C.POINTER(_u64p), _f64p]),
@@ -116,6 +120,7 @@ def lib():
             "ctc_dataset_set_lr": (C.c_int, [P, C.c_double]),
             "ctc_dataset_evaluate": (C.c_int, [P, C.POINTER(EpochStats)]),
             "ctc_dataset_get_model": (C.c_int, [P, P]),
+            "ctc_dataset_probe_wait": (C.c_int, [P, C.c_uint64]),
             "ctc_ctx_set_profiling": (C.c_int, [P, C.c_int]),
             "ctc_ctx_kernel_time": (C.c_int, [P, C.c_char_p, _u64p, _f64p]),
             "ctc_ctx_reset_kernel_times": (C.c_int, [P]),
@@ -135,6 +140,7 @@ def lib():
             "ctc_model_save": (C.c_int, [P, C.c_char_p]),
             "ctc_model_load": (C.c_int, [C.c_char_p, C.POINTER(P)]),
             "ctc_params_default": (C.c_int, [C.c_int, C.POINTER(Params)]),
+            "ctc_params_check": (C.c_int, [C.POINTER(Params)]),
             "ctc_run": (C.c_int, [P, C.POINTER(P), P, P, P, P, C.POINTER(Params), EPOCH_CB, P,
                                   C.POINTER(Result)]),
             "ctc_dataset_create": (C.c_int, [P, C.POINTER(P), P, P, C.POINTER(Params), C.POINTER(P)]),
@@ -155,6 +161,7 @@ def lib():
             "ctc_fo_free": (C.c_int, [P]),
             "ctc_fo_dims": (C.c_int, [P, C.POINTER(C.c_int), _u64p]),
             "ctc_fo_run": (C.c_int, [P, P, C.POINTER(FoParams), EPOCH_CB, P, C.POINTER(Result)]),
+            "ctc_fo_grad": (C.c_int, [P, P, C.POINTER(_f64p), _f64p]),
             "ctc_batch_info": (C.c_int, [P, C.POINTER(C.c_int), _u64p, _u64p]),
             "ctc_batch_run": (C.c_int, [P, C.POINTER(P), C.POINTER(Params), BATCH_CB, P, C.POINTER(Result)]),
         }
@@ -262,6 +269,22 @@ class Tensor:
 
     def save_bin(self, path: str):
         _check(lib().ctc_tensor_save_bin(self.h, path.encode()))
+
+    def save_splatt(self, path: str):
+        """SPLATT binary coordinate file (the reference's .bin form)."""
+        _check(lib().ctc_tensor_save_splatt(self.h, path.encode()))
+
+    def write_tns(self, path: str, digits: int = -1):
+        """Text .tns: indices as stored, values "%.<digits>f" (digits >= 0)
+        or "%.17g" (digits < 0)."""
+        _check(lib().ctc_tensor_write_tns(self.h, path.encode(), digits))
+
+    def split(self, seed: int):
+        """(train, test, validation) by tvtensor.py's seeded 80/10/10 rule
+        (ctc_tensor_split)."""
+        hs = [C.c_void_p(), C.c_void_p(), C.c_void_p()]
+        _check(lib().ctc_tensor_split(self.h, seed, C.byref(hs[0]), C.byref(hs[1]), C.byref(hs[2])))
+        return tuple(Tensor(h) for h in hs)
 
     def info(self):
         nm = C.c_int()
@@ -531,6 +554,11 @@ class Dataset:
         _check(lib().ctc_dataset_get_model(self.h, model.h))
         return model
 
+    def probe_wait(self, limit_ns: int):
+        """Enqueue the bounded-wait self-test (ctc_dataset_probe_wait): its
+        wait expires after limit_ns and the next evaluate raises CTC_E_TIMEOUT."""
+        _check(lib().ctc_dataset_probe_wait(self.h, limit_ns))
+
     def free(self):
         if self.h:
             lib().ctc_dataset_free(self.h)
@@ -751,6 +779,15 @@ class FirstOrder:
         _check(lib().ctc_fo_run(self.h, model.h, C.byref(p), cb, None, C.byref(res)))
         out.result = _result_dict(res)
         return out
+
+    def grad(self, model: Model):
+        """(grads per mode, objective) from the training step's adjoint pass
+        (ctc_fo_grad: FP32 or BF16 gathers, FP32 accumulation)."""
+        G = [np.zeros((d, model.rank), dtype=np.float64) for d in model.dims]
+        ptrs = (_f64p * len(G))(*[g.ctypes.data_as(_f64p) for g in G])
+        obj = C.c_double()
+        _check(lib().ctc_fo_grad(self.h, model.h, ptrs, C.byref(obj)))
+        return G, obj.value
 
     def free(self):
         if self.h:

@@ -316,6 +316,7 @@ struct SessionBase {
     virtual void save_best() = 0;
     virtual uint64_t nonspd() = 0;
     virtual void set_params(const ctc_params &p) = 0;
+    virtual void probe_wait(uint64_t limit_ns) = 0;
     // squared error per batch instance over instance-aligned chunks of the
     // mode-1 training copy (which = 0) or the test tensor (which = 1)
     virtual void seg_sse(int which, const uint4 *chunks, uint32_t nchunks, const uint32_t *first, int ninst,
@@ -694,6 +695,7 @@ struct Session : SessionBase {
             CK(cudaStreamSynchronize(ctx->stream));
         }
         CK(cudaMemsetAsync(nonspd_dev.p, 0, sizeof(unsigned long long), ctx->stream));
+        CK(cudaMemsetAsync(dev_err.p, 0, sizeof(int), ctx->stream));
         set_lr(p.lr * (p.lr_scale > 0 ? p.lr_scale : 1.0));
         if (colmajor) ccdpp_init();
         if (tc)
@@ -806,14 +808,26 @@ struct Session : SessionBase {
 
     // device-side error flag: 1 = the tensor-core Gram's bounded wait for
     // its MMAs expired, 2 = a CCD++ pass's bounded wait for its staged
-    // columns expired (the pass left the column unfinished)
+    // columns expired (the pass left the column unfinished), 3 = the
+    // bounded-wait self-test expired (ctc_dataset_probe_wait).  An error is
+    // reported once: the flag is cleared when it is read here, and when a
+    // model is staged.
     void check_errors()
     {
         int e = 0;
         CK(cudaMemcpyAsync(&e, dev_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        if (!e) return;
+        CK(cudaMemsetAsync(dev_err.p, 0, sizeof(int), ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
         if (e == 1) fail(CTC_E_TIMEOUT, "tensor-core Gram: a bounded wait for the MMAs expired");
-        if (e) fail(CTC_E_TIMEOUT, "CCD++ pass: a bounded wait for the staged factor columns expired");
+        if (e == 3) fail(CTC_E_TIMEOUT, "bounded-wait self-test: the wait expired");
+        fail(CTC_E_TIMEOUT, "CCD++ pass: a bounded wait for the staged factor columns expired");
+    }
+
+    void probe_wait(uint64_t limit_ns) override
+    {
+        LAUNCH(ctx, k::k_wait_probe, 1, 32, 0, dev_err.p, 3, limit_ns);
     }
 
     void ccd_epoch()
@@ -846,12 +860,19 @@ struct Session : SessionBase {
         if (c >= 2 && base % 2 == 0) return 2;
         return 1;
     }
-    int sgd_groups_per_block() const { return 8 * (32 / (R / k::Vec<T>::n / sgd_vectors())); }
+    // Hogwild threads per block: ctc_params.threads_per_block (the
+    // reference GA's block-size gene, ga/sgd.cu:66-78), 256 when 0
+    int sgd_block() const { return p.threads_per_block > 0 ? p.threads_per_block : 256; }
+    int sgd_groups_per_block() const
+    {
+        return (sgd_block() / 32) * (32 / (R / k::Vec<T>::n / sgd_vectors()));
+    }
     template <int C>
     void set_sgd_smem()
     {
         if constexpr ((R / k::Vec<T>::n) % C == 0 && R / k::Vec<T>::n / C <= 32) {
-            const int gpb = 8 * (32 / (R / k::Vec<T>::n / C));
+            // the largest block (512 threads) sets the opt-in
+            const int gpb = 16 * (32 / (R / k::Vec<T>::n / C));
             const int smem = gpb * 2 * 3 * R * (int)sizeof(T);
             if (smem > 48 * 1024)
                 CK(cudaFuncSetAttribute(k::k_sgd<T, R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -890,7 +911,8 @@ struct Session : SessionBase {
         const bool bulk = !seq && p.sgd_atomic == 2 && std::is_same<T, float>::value;
         const size_t smem = bulk ? (size_t)gpb * 2 * 3 * R * sizeof(T) : 0;
         if constexpr ((R / k::Vec<T>::n) % C == 0)
-            LAUNCH(ctx, k::k_sgd<T, R, C>, g, seq ? 32 : 256, smem, (const uint4 *)c.rec.p, (const double *)c.v64.p,
+            LAUNCH(ctx, k::k_sgd<T, R, C>, g, seq ? 32 : sgd_block(), smem, (const uint4 *)c.rec.p,
+                   (const double *)c.v64.p,
                    c.n, tile_len, c.ntiles, U[0].p, U[1].p, U[2].p, (const T *)lr_dev.p, (T)p.lambda, p.sgd_atomic,
                    seq ? 1 : 0, stride, d0, d1, d2);
     }
@@ -1113,12 +1135,16 @@ static void run_loop(ctc_dataset *ds, SessionBase *S, ctc_model *model, ctc_mode
     int nbad = 0, best_epoch = 0;
     double prev_obj = 0, total_ms = 0;
     ctc_epoch_stats st{};
+    // tc_converge runs after every epoch from the first (sgpu/als.cu:803-806):
+    // the starting point (epoch 0) is reported but not tracked, so the first
+    // epoch always becomes the best one, as in the reference
     auto report = [&](int epoch, double ms) -> bool {
         S->evaluate(&st);
         st.epoch = epoch;
         st.ms_epoch = ms;
         st.lr = lr_base * scale;
         if (!std::isfinite(st.loss)) fail(CTC_E_NUMERIC, "training loss is not finite at epoch %d", epoch);
+        if (epoch == 0) return cb ? cb(user, &st) != 0 : false;
         const double conv = ds->has_val ? st.rmse_vl : st.rmse_tr;
         bool converged = false;
         if (conv - best_rmse < -p.tolerance) {
@@ -1188,6 +1214,11 @@ static void check_params(const ctc_params *p)
     if (p->tile_len < 0 || p->tile_len > (1 << 20)) fail(CTC_E_ARG, "tile_len %d", p->tile_len);
     if (p->iters < 0) fail(CTC_E_ARG, "iters %d", p->iters);
     if (p->mode_start < 0 || p->mode_start > 2) fail(CTC_E_ARG, "mode_start %d", p->mode_start);
+    const int tpb = p->threads_per_block;
+    if (tpb < 0 || (tpb & (tpb - 1)) != 0 || tpb > 512)
+        fail(CTC_E_ARG, "threads_per_block %d: 0 or a power of two up to 512", tpb);
+    if (tpb > 0 && tpb < 32)
+        fail(CTC_E_UNSUP, "threads_per_block %d: SGD blocks are whole warps here (32 to 512 threads)", tpb);
 }
 
 static void check_model(const ctc_dataset *d, const ctc_model *model, int rank)
@@ -1296,6 +1327,11 @@ extern "C" int ctc_ctx_reset_kernel_times(ctc_ctx *ctx)
         kt_flush(ctx);
         ctx->kt.acc.clear();
     });
+}
+
+extern "C" int ctc_params_check(const ctc_params *p)
+{
+    return guarded([&] { check_params(p); });
 }
 
 extern "C" int ctc_params_default(int alg, ctc_params *p)
@@ -1429,6 +1465,16 @@ extern "C" int ctc_dataset_evaluate(ctc_dataset *d, ctc_epoch_stats *st)
         CK(cudaSetDevice(d->ctx->device));
         memset(st, 0, sizeof(*st));
         d->session->evaluate(st);
+    });
+}
+
+extern "C" int ctc_dataset_probe_wait(ctc_dataset *d, uint64_t limit_ns)
+{
+    return guarded([&] {
+        if (!d || !d->session) fail(CTC_E_ARG, "no model staged on the dataset");
+        if (limit_ns == 0 || limit_ns > 2000000000ull) fail(CTC_E_ARG, "limit_ns must be in (0, 2e9]");
+        CK(cudaSetDevice(d->ctx->device));
+        d->session->probe_wait(limit_ns);
     });
 }
 
@@ -1861,7 +1907,7 @@ extern "C" int ctc_batch_run(ctc_batch *B, ctc_model *const *models, const ctc_p
 namespace ctc {
 
 struct TuneCand {
-    int tile_len = 0, threads_per_row = 0, smem_budget = 0, sgd_atomic = 0;
+    int tile_len = 0, threads_per_row = 0, smem_budget = 0, sgd_atomic = 0, threads_per_block = 0;
 };
 
 // shape key: algorithm, precision, rank, compat, SGD order, dimensions and
@@ -1888,8 +1934,9 @@ static bool tune_read(const char *path, const std::string &key, TuneCand &c, dou
         char k[300];
         TuneCand t;
         double x = 0;
-        if (sscanf(line, "%299s tile_len=%d threads_per_row=%d smem_budget=%d sgd_atomic=%d ms=%lf", k,
-                   &t.tile_len, &t.threads_per_row, &t.smem_budget, &t.sgd_atomic, &x) == 6 &&
+        if (sscanf(line, "%299s tile_len=%d threads_per_row=%d smem_budget=%d sgd_atomic=%d threads_per_block=%d ms=%lf",
+                   k, &t.tile_len, &t.threads_per_row, &t.smem_budget, &t.sgd_atomic, &t.threads_per_block,
+                   &x) == 7 &&
             key == k) {
             c = t;  // the last entry for a key wins
             ms = x;
@@ -1916,8 +1963,8 @@ static void tune_write(const char *path, const std::string &key, const TuneCand 
     FILE *f = fopen(path, "w");
     if (!f) fail(CTC_E_IO, "cannot write the tuning cache %s", path);
     for (const std::string &l : keep) fputs(l.c_str(), f);
-    fprintf(f, "%s tile_len=%d threads_per_row=%d smem_budget=%d sgd_atomic=%d ms=%.6f\n", key.c_str(),
-            c.tile_len, c.threads_per_row, c.smem_budget, c.sgd_atomic, ms);
+    fprintf(f, "%s tile_len=%d threads_per_row=%d smem_budget=%d sgd_atomic=%d threads_per_block=%d ms=%.6f\n",
+            key.c_str(), c.tile_len, c.threads_per_row, c.smem_budget, c.sgd_atomic, c.threads_per_block, ms);
     fclose(f);
 }
 
@@ -1930,6 +1977,7 @@ static std::vector<TuneCand> tune_space(const ctc_params &p)
         x.threads_per_row = c;
         x.smem_budget = s;
         x.sgd_atomic = a < 0 ? p.sgd_atomic : a;
+        x.threads_per_block = p.threads_per_block;
         v.push_back(x);
     };
     switch (p.alg) {
@@ -2003,6 +2051,7 @@ extern "C" int ctc_tune_lookup(const char *cache_path, const ctc_tensor *train, 
         out->threads_per_row = c.threads_per_row;
         out->smem_budget = c.smem_budget;
         out->sgd_atomic = c.sgd_atomic;
+        out->threads_per_block = c.threads_per_block;
     });
 }
 
@@ -2023,7 +2072,7 @@ extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], cons
         if (!(flags & CTC_TUNE_FORCE) && tune_read(cache_path, key, best, best_ms)) {
             if (trials && max_trials > 0) {
                 trials[0] = ctc_tune_trial{best.tile_len, best.threads_per_row, best.smem_budget, best_ms, 1,
-                                           best.sgd_atomic};
+                                           best.sgd_atomic, best.threads_per_block};
                 nt = 1;
             }
         } else {
@@ -2055,11 +2104,11 @@ extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], cons
                 if (ctc_model_init_uniform(&mdl, 12345, 1.0 / std::sqrt((double)q.rank)) != CTC_OK)
                     fail(CTC_E_ARG, "%s", ctc_last_error());
                 SessionBase *S = session_for(ds.get(), q.rank);
-                for (const TuneCand &c : space) {
-                    if (c.tile_len != tl) continue;
+                auto trial = [&](const TuneCand &c) {
                     q.threads_per_row = c.threads_per_row;
                     q.smem_budget = c.smem_budget;
                     q.sgd_atomic = c.sgd_atomic;
+                    q.threads_per_block = c.threads_per_block;
                     ds->p = q;
                     S->set_params(q);
                     S->set_model(&mdl);
@@ -2073,12 +2122,35 @@ extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], cons
                     const double per = ms / 2.0;
                     if (trials && nt < max_trials)
                         trials[nt] = ctc_tune_trial{c.tile_len, c.threads_per_row, c.smem_budget, per, 0,
-                                                    c.sgd_atomic};
+                                                    c.sgd_atomic, c.threads_per_block};
                     ++nt;
-                    if (per < best_ms) {
-                        best_ms = per;
-                        best = c;
+                    return per;
+                };
+                TuneCand tile_best;
+                double tile_ms = 1e300;
+                for (const TuneCand &c : space) {
+                    if (c.tile_len != tl) continue;
+                    const double per = trial(c);
+                    if (per < tile_ms) {
+                        tile_ms = per;
+                        tile_best = c;
                     }
+                }
+                // Hogwild SGD: the block size (the reference GA's other gene)
+                // around this tile length's fastest candidate
+                if (q.alg == CTC_ALG_SGD && q.sgd_order == CTC_SGD_HOGWILD)
+                    for (int b : {128, 512}) {
+                        TuneCand c = tile_best;
+                        c.threads_per_block = b;
+                        const double per = trial(c);
+                        if (per < tile_ms) {
+                            tile_ms = per;
+                            tile_best = c;
+                        }
+                    }
+                if (tile_ms < best_ms) {
+                    best_ms = tile_ms;
+                    best = tile_best;
                 }
                 ds.reset();
             }
@@ -2088,6 +2160,7 @@ extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], cons
         out->threads_per_row = best.threads_per_row;
         out->smem_budget = best.smem_budget;
         out->sgd_atomic = best.sgd_atomic;
+        out->threads_per_block = best.threads_per_block;
         if (ntrials) *ntrials = nt;
     });
 }

@@ -276,6 +276,54 @@ static void fo_run(ctc_fo *f, ctc_model *model, const ctc_fo_params &p, ctc_epoc
     }
 }
 
+// Gradient of the whole training loss at `model` through the minibatch
+// kernel: one pass over every staged training nonzero (scale 1), with the
+// precision the first-order training was created with (FP32 or BF16
+// gathers, FP32 accumulation); the lambda term is added in FP64.
+template <int R, int D>
+static void fo_grad_pass(ctc_fo *f, const ctc_model *model, double *const *grads, double *obj)
+{
+    ctc_ctx *ctx = f->ctx;
+    fo_alloc(f, R);
+    {
+        std::vector<float> h(f->U.n);
+        for (int m = 0; m < D; ++m)
+            for (uint64_t i = 0; i < f->dims[m] * (uint64_t)R; ++i) h[f->off[m] + i] = (float)model->U[m][i];
+        f->U.upload(h.data(), h.size(), ctx->stream);
+    }
+    const uint64_t n = f->U.n;
+    CK(cudaMemsetAsync(f->G.p, 0, n * sizeof(float), ctx->stream));
+    const bool bf = f->p.precision == CTC_PREC_MIXED;
+    if (bf) {
+        // BF16 copies (an Adam step with lr 0 is a copy)
+        CK(cudaMemsetAsync(f->M.p, 0, n * sizeof(float), ctx->stream));
+        CK(cudaMemsetAsync(f->V.p, 0, n * sizeof(float), ctx->stream));
+        LAUNCH(ctx, fo::k_fo_adam, grid_for(n, 256, kSMs * 16), 256, 0, f->U.p, f->M.p, f->V.p, f->G.p, f->Ub.p, n,
+               0.f, 0.f, 0.f, 1.f, 1.f, 1.f, 0.f);
+    }
+    const void *Ug[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int m = 0; m < D; ++m) Ug[m] = bf ? (const void *)(f->Ub.p + f->off[m]) : (const void *)(f->U.p + f->off[m]);
+    if (bf) fo_pass<__nv_bfloat16, R, D, true>(f, f->idx.p, f->val.p, 0, f->ntrain, 1.0, Ug);
+    else fo_pass<float, R, D, true>(f, f->idx.p, f->val.p, 0, f->ntrain, 1.0, Ug);
+    const unsigned g = grid_for(f->ntrain, 256, kMaxPartials);
+    LAUNCH(ctx, k::k_sum_partials, 1, 256, 0, (const double *)ctx->partial.p, (int)g, ctx->scalars.p + 8);
+    double half = 0;
+    CK(cudaMemcpyAsync(&half, ctx->scalars.p + 8, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<float> h(n);
+    CK(cudaMemcpyAsync(h.data(), f->G.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double lam = f->p.lambda;
+    double reg = 0;
+    for (int m = 0; m < D; ++m) {
+        const std::vector<double> &u = model->U[m];
+        for (uint64_t i = 0; i < u.size(); ++i) {
+            grads[m][i] = (double)h[f->off[m] + i] + 2.0 * lam * u[i];
+            reg += u[i] * u[i];
+        }
+    }
+    if (obj) *obj = half + lam * reg;
+}
+
 template <typename F>
 static void with_rank_order(int R, int D, F &&f)
 {
@@ -436,6 +484,23 @@ extern "C" int ctc_fo_run(ctc_fo *f, ctc_model *model, const ctc_fo_params *p, c
         CK(cudaSetDevice(f->ctx->device));
         with_rank_order(p->rank, f->D, [&](auto RC, auto DC) {
             fo_run<decltype(RC)::value, decltype(DC)::value>(f, model, *p, cb, user, res);
+        });
+    });
+}
+
+extern "C" int ctc_fo_grad(ctc_fo *f, const ctc_model *model, double *const *grads, double *obj)
+{
+    using namespace ctc;
+    return guarded([&] {
+        if (!f || !model || !grads) fail(CTC_E_ARG, "null argument");
+        if (model->nmodes != f->D || model->rank != f->p.rank) fail(CTC_E_ARG, "model order/rank mismatch");
+        for (int m = 0; m < f->D; ++m)
+            if (model->dims[m] != f->dims[m]) fail(CTC_E_ARG, "model mode %d has %llu rows, the tensors need %llu",
+                                                   m, (unsigned long long)model->dims[m],
+                                                   (unsigned long long)f->dims[m]);
+        CK(cudaSetDevice(f->ctx->device));
+        with_rank_order(f->p.rank, f->D, [&](auto RC, auto DC) {
+            fo_grad_pass<decltype(RC)::value, decltype(DC)::value>(f, model, grads, obj);
         });
     });
 }

@@ -324,6 +324,37 @@ static void read_tns(const char *path, ctc_tensor &t)
 
 static const char kMagic[4] = {'C', 'T', 'C', 'B'};
 
+// Reads `bytes` bytes at offset `off` of `fd` into dst, by byte ranges on
+// the host threads; false on a short read.
+static bool pread_parallel(int fd, char *dst, uint64_t bytes, off_t off)
+{
+    const int P = bytes < ((uint64_t)4 << 20) ? 1 : host_threads();
+    std::atomic<int> short_read{0};
+    const std::function<void(int)> rd = [&](int q) {
+        uint64_t b = bytes * (uint64_t)q / P;
+        const uint64_t e = bytes * (uint64_t)(q + 1) / P;
+        while (b < e) {
+            const ssize_t r = pread(fd, dst + b, e - b, off + (off_t)b);
+            if (r <= 0) {
+                short_read = 1;
+                return;
+            }
+            b += (uint64_t)r;
+        }
+    };
+    host_run(P, rd);
+    return !short_read;
+}
+
+// True when `nnz` records of `per_nnz` bytes fit in the file after `off0`
+// (checked before anything is sized from the header's nnz).
+static bool fits_file(int fd, uint64_t off0, uint64_t nnz, uint64_t per_nnz)
+{
+    struct stat st;
+    if (fstat(fd, &st) != 0 || st.st_size < 0 || (uint64_t)st.st_size < off0) return false;
+    return nnz <= ((uint64_t)st.st_size - off0) / per_nnz;
+}
+
 static void read_bin(const char *path, ctc_tensor &t)
 {
     FILE *f = fopen(path, "rb");
@@ -334,45 +365,96 @@ static void read_bin(const char *path, ctc_tensor &t)
     bool ok = fread(mg, 1, 4, f) == 4 && memcmp(mg, kMagic, 4) == 0 &&
               fread(&ver, 4, 1, f) == 1 && ver == 1 && fread(&nm, 4, 1, f) == 1 &&
               nm >= 1 && nm <= 4 && fread(&nnz, 8, 1, f) == 1;
+    if (ok) ok = fread(t.dims, 8, nm, f) == nm;
+    const off_t off0 = (off_t)(4 + 4 + 4 + 8 + 8 * (uint64_t)nm);
+    const int fd = fileno(f);
+    // the arrays must be in the file before the header's nnz sizes anything
+    if (ok) ok = fits_file(fd, (uint64_t)off0, nnz, 8 * ((uint64_t)nm + 1));
     if (ok) {
         t.nmodes = (int)nm;
         t.nnz = nnz;
-        ok = fread(t.dims, 8, nm, f) == nm;
-    }
-    if (ok) {
-        // the arrays follow the header: read by byte ranges on the host threads
-        const off_t off0 = (off_t)(4 + 4 + 4 + 8 + 8 * (uint64_t)nm);
-        const int fd = fileno(f);
-        std::vector<char *> dst;
-        for (uint32_t m = 0; m < nm; ++m) {
-            t.ind[m].resize(nnz);
-            dst.push_back(reinterpret_cast<char *>(t.ind[m].data()));
-        }
-        t.vals.resize(nnz);
-        dst.push_back(reinterpret_cast<char *>(t.vals.data()));
         const uint64_t bytes = nnz * 8;
-        const int P = bytes < ((uint64_t)4 << 20) ? 1 : host_threads();
-        std::atomic<int> short_read{0};
-        const std::function<void(int)> rd = [&](int q) {
-            for (size_t a = 0; a < dst.size(); ++a) {
-                uint64_t b = bytes * (uint64_t)q / P;
-                const uint64_t e = bytes * (uint64_t)(q + 1) / P;
-                const off_t base = off0 + (off_t)(a * bytes);
-                while (b < e) {
-                    const ssize_t r = pread(fd, dst[a] + b, e - b, base + (off_t)b);
-                    if (r <= 0) {
-                        short_read = 1;
-                        return;
-                    }
-                    b += (uint64_t)r;
-                }
-            }
-        };
-        host_run(P, rd);
-        ok = !short_read;
+        for (uint32_t m = 0; ok && m < nm; ++m) {
+            t.ind[m].resize(nnz);
+            ok = pread_parallel(fd, reinterpret_cast<char *>(t.ind[m].data()), bytes, off0 + (off_t)(m * bytes));
+        }
+        if (ok) {
+            t.vals.resize(nnz);
+            ok = pread_parallel(fd, reinterpret_cast<char *>(t.vals.data()), bytes, off0 + (off_t)(nm * bytes));
+        }
     }
     fclose(f);
     if (!ok) fail(CTC_E_IO, "'%s' is not a valid CTCB tensor file", path);
+}
+
+// SPLATT coordinate binary form, as the reference writes it
+// (sgpu/io.c:116-150 p_write_tt_binary_header, io.c:347-431
+// tt_write_binary_file): int32 magic 0 (SPLATT_BIN_COORD, sgpu/io.h:67-84),
+// u64 idx_width, u64 val_width, then idx_width-byte words: nmodes,
+// dims[nmodes], nnz, the nmodes index arrays, and nnz values of val_width
+// bytes.  The reference's reader (io.c:160-188, 436-509) exits on its own
+// files (idx_width 8 > 4) and reads narrow indices with an uninitialised
+// count; here idx_width 4 or 8 and val_width 4 or 8 are all read, indices
+// kept as stored (1-based from .tns files), dims as in the header.
+static void read_splatt_bin(const char *path, ctc_tensor &t)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) fail(CTC_E_IO, "cannot open '%s'", path);
+    int32_t magic = -1;
+    uint64_t iw = 0, vw = 0;
+    bool ok = fread(&magic, 4, 1, f) == 1 && magic == 0 && fread(&iw, 8, 1, f) == 1 && fread(&vw, 8, 1, f) == 1 &&
+              (iw == 4 || iw == 8) && (vw == 4 || vw == 8);
+    auto word = [&](uint64_t *v) {
+        if (iw == 8) return fread(v, 8, 1, f) == 1;
+        uint32_t w = 0;
+        const bool r = fread(&w, 4, 1, f) == 1;
+        *v = w;
+        return r;
+    };
+    uint64_t nm = 0, nnz = 0;
+    if (ok) ok = word(&nm) && nm >= 1 && nm <= 4;
+    for (uint64_t m = 0; ok && m < nm; ++m) ok = word(&t.dims[m]);
+    if (ok) ok = word(&nnz);
+    const uint64_t off0 = 4 + 8 + 8 + iw * (nm + 2);
+    const int fd = fileno(f);
+    if (ok) ok = fits_file(fd, off0, nnz, iw * nm + vw);
+    if (ok) {
+        t.nmodes = (int)nm;
+        t.nnz = nnz;
+        std::vector<uint32_t, NoInitAlloc<uint32_t>> narrow;
+        std::vector<float, NoInitAlloc<float>> fvals;
+        const uint64_t ib = nnz * iw;
+        for (uint64_t m = 0; ok && m < nm; ++m) {
+            t.ind[m].resize(nnz);
+            const off_t at = (off_t)(off0 + m * ib);
+            if (iw == 8) {
+                ok = pread_parallel(fd, reinterpret_cast<char *>(t.ind[m].data()), ib, at);
+            } else {
+                narrow.resize(nnz);
+                ok = pread_parallel(fd, reinterpret_cast<char *>(narrow.data()), ib, at);
+                uint64_t *dst = t.ind[m].data();
+                parallel_for(nnz, [&](int, uint64_t b, uint64_t e) {
+                    for (uint64_t i = b; i < e; ++i) dst[i] = narrow[i];
+                });
+            }
+        }
+        if (ok) {
+            t.vals.resize(nnz);
+            const off_t at = (off_t)(off0 + nm * ib);
+            if (vw == 8) {
+                ok = pread_parallel(fd, reinterpret_cast<char *>(t.vals.data()), nnz * 8, at);
+            } else {
+                fvals.resize(nnz);
+                ok = pread_parallel(fd, reinterpret_cast<char *>(fvals.data()), nnz * 4, at);
+                double *dst = t.vals.data();
+                parallel_for(nnz, [&](int, uint64_t b, uint64_t e) {
+                    for (uint64_t i = b; i < e; ++i) dst[i] = (double)fvals[i];
+                });
+            }
+        }
+    }
+    fclose(f);
+    if (!ok) fail(CTC_E_IO, "'%s' is not a valid SPLATT binary coordinate tensor", path);
 }
 
 // ------------------------------------------------------------------
@@ -777,6 +859,7 @@ extern "C" int ctc_tensor_load_tns(const char *path, ctc_tensor **out)
         try {
             size_t L = strlen(path);
             if (L > 5 && strcmp(path + L - 5, ".ctcb") == 0) read_bin(path, *t);
+            else if (L > 4 && strcmp(path + L - 4, ".bin") == 0) read_splatt_bin(path, *t);
             else read_tns(path, *t);
         } catch (...) {
             delete t;
@@ -955,6 +1038,235 @@ extern "C" int ctc_tensor_sort(ctc_tensor *t, int mode)
             for (uint64_t i = b; i < e; ++i) tv[i] = t->vals[perm[i]];
         });
         t->vals.swap(tv);
+    });
+}
+
+// ------------------------------------------------------------------
+// Data preparation (software/scripts/tvtensor.py, stensor.py)
+// ------------------------------------------------------------------
+namespace ctc {
+
+// MT19937 (Matsumoto and Nishimura, 1998) with the 2002 init_by_array
+// seeding, as Python's `random` module uses it: random.seed(a) for an int
+// a seeds with the 32-bit words of |a|, least significant first ([0] for
+// 0); getrandbits(k <= 32) is the top k bits of one 32-bit output;
+// randint(0, n-1) draws getrandbits(bit_length(n)) until the value is
+// below n.
+class PyMersenne {
+    static constexpr int N = 624, M = 397;
+    uint32_t mt[N];
+    int mti = N + 1;
+
+    void init_genrand(uint32_t s)
+    {
+        mt[0] = s;
+        for (mti = 1; mti < N; ++mti) mt[mti] = 1812433253u * (mt[mti - 1] ^ (mt[mti - 1] >> 30)) + (uint32_t)mti;
+    }
+
+public:
+    explicit PyMersenne(uint64_t seed)
+    {
+        uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+        const int klen = key[1] ? 2 : 1;
+        init_genrand(19650218u);
+        int i = 1, j = 0;
+        for (int k = std::max(N, klen); k; --k) {
+            mt[i] = (mt[i] ^ ((mt[i - 1] ^ (mt[i - 1] >> 30)) * 1664525u)) + key[j] + (uint32_t)j;
+            ++i;
+            ++j;
+            if (i >= N) {
+                mt[0] = mt[N - 1];
+                i = 1;
+            }
+            if (j >= klen) j = 0;
+        }
+        for (int k = N - 1; k; --k) {
+            mt[i] = (mt[i] ^ ((mt[i - 1] ^ (mt[i - 1] >> 30)) * 1566083941u)) - (uint32_t)i;
+            ++i;
+            if (i >= N) {
+                mt[0] = mt[N - 1];
+                i = 1;
+            }
+        }
+        mt[0] = 0x80000000u;
+        mti = N;
+    }
+
+    uint32_t next()
+    {
+        static const uint32_t mag01[2] = {0u, 0x9908b0dfu};
+        if (mti >= N) {
+            int kk = 0;
+            for (; kk < N - M; ++kk) {
+                const uint32_t y = (mt[kk] & 0x80000000u) | (mt[kk + 1] & 0x7fffffffu);
+                mt[kk] = mt[kk + M] ^ (y >> 1) ^ mag01[y & 1u];
+            }
+            for (; kk < N - 1; ++kk) {
+                const uint32_t y = (mt[kk] & 0x80000000u) | (mt[kk + 1] & 0x7fffffffu);
+                mt[kk] = mt[kk + (M - N)] ^ (y >> 1) ^ mag01[y & 1u];
+            }
+            const uint32_t y = (mt[N - 1] & 0x80000000u) | (mt[0] & 0x7fffffffu);
+            mt[N - 1] = mt[M - 1] ^ (y >> 1) ^ mag01[y & 1u];
+            mti = 0;
+        }
+        uint32_t y = mt[mti++];
+        y ^= (y >> 11);
+        y ^= (y << 7) & 0x9d2c5680u;
+        y ^= (y << 15) & 0xefc60000u;
+        y ^= (y >> 18);
+        return y;
+    }
+
+    // randint(0, n - 1) for 1 <= n <= 2^32 - 1
+    uint32_t below(uint32_t n)
+    {
+        int k = 0;
+        while (k < 32 && (n >> k)) ++k;
+        for (;;) {
+            const uint32_t r = next() >> (32 - k);
+            if (r < n) return r;
+        }
+    }
+};
+
+static ctc_tensor *subset(const ctc_tensor &t, const std::vector<uint64_t> &pick)
+{
+    auto *o = new ctc_tensor();
+    o->nmodes = t.nmodes;
+    o->nnz = pick.size();
+    for (int m = 0; m < t.nmodes; ++m) {
+        o->ind[m].resize(pick.size());
+        uint64_t mx = 0;
+        bool zero = false;
+        for (size_t i = 0; i < pick.size(); ++i) {
+            const uint64_t v = t.ind[m][pick[i]];
+            o->ind[m][i] = v;
+            mx = std::max(mx, v);
+            zero |= v == 0;
+        }
+        o->dims[m] = mx + (zero ? 1 : 0);
+    }
+    o->vals.resize(pick.size());
+    for (size_t i = 0; i < pick.size(); ++i) o->vals[i] = t.vals[pick[i]];
+    return o;
+}
+
+}  // namespace ctc
+
+extern "C" int ctc_tensor_split(const ctc_tensor *t, uint64_t seed, ctc_tensor **train, ctc_tensor **test,
+                                ctc_tensor **val)
+{
+    return guarded([&] {
+        if (!t) fail(CTC_E_ARG, "null tensor");
+        if (t->nmodes < 2) fail(CTC_E_ARG, "the split orders by the first two modes: order >= 2");
+        std::vector<uint64_t> perm;
+        stable_order(t->ind[0].data(), t->ind[1].data(), t->nnz, perm);
+        PyMersenne rng(seed);
+        std::vector<uint64_t> pick[3];
+        for (uint64_t i = 0; i < t->nnz; ++i) {
+            const uint32_t flag = rng.below(10);
+            pick[flag < 8 ? 0 : (flag == 8 ? 1 : 2)].push_back(perm[i]);
+        }
+        std::unique_ptr<ctc_tensor> out[3];
+        ctc_tensor **dst[3] = {train, test, val};
+        for (int k = 0; k < 3; ++k)
+            if (dst[k]) out[k].reset(subset(*t, pick[k]));
+        for (int k = 0; k < 3; ++k)
+            if (dst[k]) *dst[k] = out[k].release();
+    });
+}
+
+extern "C" int ctc_tensor_write_tns(const ctc_tensor *t, const char *path, int digits)
+{
+    return guarded([&] {
+        if (!t || !path) fail(CTC_E_ARG, "null argument");
+        if (digits > 40) fail(CTC_E_ARG, "at most 40 digits after the point");
+        char vfmt[16];
+        if (digits < 0) snprintf(vfmt, sizeof vfmt, "%%.17g\n");
+        else snprintf(vfmt, sizeof vfmt, "%%.%df\n", digits);
+        FILE *f = fopen(path, "w");
+        if (!f) fail(CTC_E_IO, "cannot open %s for writing", path);
+        const uint64_t n = t->nnz;
+        const int nm = t->nmodes;
+        // blocks of lines formatted on the host threads, written in order
+        const int P = host_threads();
+        const uint64_t kLines = 16384;
+        std::vector<std::string> out(P);
+        bool ok = true;
+        for (uint64_t l0 = 0; l0 < n && ok; l0 += kLines * (uint64_t)P) {
+            const std::function<void(int)> fmt = [&](int q) {
+                std::string &o = out[q];
+                o.clear();
+                const uint64_t b = std::min(n, l0 + kLines * (uint64_t)q), e = std::min(n, b + kLines);
+                char buf[400];
+                for (uint64_t i = b; i < e; ++i) {
+                    for (int m = 0; m < nm; ++m) {
+                        const int k = snprintf(buf, sizeof buf, "%llu ", (unsigned long long)t->ind[m][i]);
+                        o.append(buf, (size_t)k);
+                    }
+                    const int k = snprintf(buf, sizeof buf, vfmt, t->vals[i]);
+                    o.append(buf, (size_t)std::min<int>(k, (int)sizeof buf - 1));
+                }
+            };
+            host_run(P, fmt);
+            for (int q = 0; q < P && ok; ++q) ok = fwrite(out[q].data(), 1, out[q].size(), f) == out[q].size();
+        }
+        if (fclose(f) != 0) ok = false;
+        if (!ok) fail(CTC_E_IO, "write to %s failed", path);
+    });
+}
+
+extern "C" int ctc_tensor_save_splatt(const ctc_tensor *t, const char *path)
+{
+    return guarded([&] {
+        if (!t || !path) fail(CTC_E_ARG, "null argument");
+        const uint64_t n = t->nnz;
+        const int nm = t->nmodes;
+        // 4-byte words when the counts, dims and indices all fit, 4-byte
+        // values when every value is exactly a float (the test the
+        // reference's header writer means to make, sgpu/io.c:124-145)
+        bool narrow = n <= 0xffffffffull;
+        for (int m = 0; m < nm && narrow; ++m) {
+            narrow = t->dims[m] <= 0xffffffffull;
+            for (uint64_t i = 0; i < n && narrow; ++i) narrow = t->ind[m][i] <= 0xffffffffull;
+        }
+        bool fl = true;
+        for (uint64_t i = 0; i < n && fl; ++i) {
+            const double v = t->vals[i];
+            fl = std::isnan(v) || (double)(float)v == v;
+        }
+        const uint64_t iw = narrow ? 4 : 8, vw = fl ? 4 : 8;
+        FILE *f = fopen(path, "wb");
+        if (!f) fail(CTC_E_IO, "cannot create '%s'", path);
+        const int32_t magic = 0;
+        bool ok = fwrite(&magic, 4, 1, f) == 1 && fwrite(&iw, 8, 1, f) == 1 && fwrite(&vw, 8, 1, f) == 1;
+        auto word = [&](uint64_t v) {
+            if (iw == 8) return fwrite(&v, 8, 1, f) == 1;
+            const uint32_t w = (uint32_t)v;
+            return fwrite(&w, 4, 1, f) == 1;
+        };
+        ok = ok && word((uint64_t)nm);
+        for (int m = 0; m < nm && ok; ++m) ok = word(t->dims[m]);
+        ok = ok && word(n);
+        std::vector<uint32_t> w32;
+        for (int m = 0; m < nm && ok; ++m) {
+            if (iw == 8) {
+                ok = fwrite(t->ind[m].data(), 8, n, f) == n;
+            } else {
+                w32.assign(t->ind[m].begin(), t->ind[m].end());
+                ok = fwrite(w32.data(), 4, n, f) == n;
+            }
+        }
+        if (ok) {
+            if (vw == 8) {
+                ok = fwrite(t->vals.data(), 8, n, f) == n;
+            } else {
+                std::vector<float> fv(t->vals.begin(), t->vals.end());
+                ok = fwrite(fv.data(), 4, n, f) == n;
+            }
+        }
+        if (fclose(f) != 0) ok = false;
+        if (!ok) fail(CTC_E_IO, "write to '%s' failed", path);
     });
 }
 

@@ -264,7 +264,7 @@ static __global__ void __launch_bounds__(256) k_sum_partials(const double *__res
 //   one is processed.
 // ---------------------------------------------------------------------
 template <typename T, int R, int C>
-__global__ void __launch_bounds__(256) k_sgd(const uint4 *__restrict__ rec,
+__global__ void __launch_bounds__(512) k_sgd(const uint4 *__restrict__ rec,
                                              const double *__restrict__ v64, uint32_t n,
                                              uint32_t tile_len, uint32_t ntiles, T *U0, T *U1,
                                              T *U2, const T *__restrict__ lr_dev, T lambda,
@@ -1641,6 +1641,19 @@ __global__ void k_scale(const T *__restrict__ x, T *__restrict__ y, uint64_t n, 
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x)
         y[i] = alpha * x[i];
+}
+
+// Self-test of the bounded-wait path: one thread waits, with the same
+// bounded wait the tensor-core Gram and the CCD++ pass use, on an mbarrier
+// that nothing arrives on.  The wait gives up after limit_ns and the kernel
+// records `code` in the session's error flag, then returns (no copy is in
+// flight, nothing else to release).
+static __global__ void k_wait_probe(int *__restrict__ err, int code, uint64_t limit_ns)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) px::mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0 && !px::mbar_wait_bounded(px::smem_u32(&bar), 0, limit_ns)) atomicExch(err, code);
 }
 
 }  // namespace k

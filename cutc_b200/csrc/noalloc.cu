@@ -19,7 +19,16 @@
 //
 // The device address of the array is looked up once per device, with that
 // device current, on the first call made there: that first call should come
-// before any stream capture on the device.
+// before any stream capture on the device.  With CUDA's lazy module loading
+// (the default), the library's device code and this array are loaded onto a
+// device by that same first call (or the first launch of any kernel of the
+// library there), and loading takes device memory: make the first call, or
+// a warm-up call, before another allocator reserves the device's memory.
+//
+// Inputs are read with 16-byte vector loads: rec, U0, U1 and U2 must be
+// 16-byte aligned (out_sse 8-byte aligned), which is checked before any
+// launch.  The kernel trusts the indices: each record's i0, i1, i2 must be
+// below the row count of U0, U1, U2.
 #include "ctc_internal.h"
 
 #include <cuda_runtime.h>
@@ -125,6 +134,15 @@ extern "C" int ctc_sse_noalloc(const void *rec, uint64_t n, const float *U0, con
 {
     if (!rec || !U0 || !U1 || !U2 || !out_sse) {
         ctc::set_last_error("ctc_sse_noalloc: null pointer argument");
+        return CTC_E_ARG;
+    }
+    if ((reinterpret_cast<uintptr_t>(rec) | reinterpret_cast<uintptr_t>(U0) | reinterpret_cast<uintptr_t>(U1) |
+         reinterpret_cast<uintptr_t>(U2)) & 15u) {
+        ctc::set_last_error("ctc_sse_noalloc: rec, U0, U1 and U2 must be 16-byte aligned");
+        return CTC_E_ARG;
+    }
+    if (reinterpret_cast<uintptr_t>(out_sse) & 7u) {
+        ctc::set_last_error("ctc_sse_noalloc: out_sse must be 8-byte aligned");
         return CTC_E_ARG;
     }
     if (n == 0) {

@@ -47,8 +47,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar_addr, uint32_t parit
     return done != 0;
 }
 
-// Bounded wait: gives up after ~2 s (globaltimer) and reports false.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar_addr, uint32_t parity)
+// Bounded wait: gives up after limit_ns of globaltimer (~2 s by default)
+// and reports false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar_addr, uint32_t parity,
+                                                  uint64_t limit_ns = 2000000000ull)
 {
     uint64_t t0;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
@@ -57,7 +59,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar_addr, uint32_t p
         if ((it & 1023u) == 1023u) {
             uint64_t t1;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-            if (t1 - t0 > 2000000000ull) return false;
+            if (t1 - t0 > limit_ns) return false;
         }
     }
 }

@@ -70,8 +70,41 @@ void *ctc_ctx_stream(ctc_ctx *ctx);
  * io.c:58-106 + tt_get_dims io.c:234-308): whitespace "i j k v" lines,
  * '#' and empty lines skipped, mode count from the first data line,
  * dims[m] = max index (+1 when an index 0 occurs).  Parsed in parallel.
- * Files ending in ".ctcb" use the binary form of ctc_tensor_save_bin. */
+ * Files ending in ".ctcb" use the binary form of ctc_tensor_save_bin;
+ * files ending in ".bin" are SPLATT binary coordinate tensors (see
+ * ctc_tensor_save_splatt).  A binary file too short for its header's
+ * nonzero count is rejected (CTC_E_IO) before anything is allocated. */
 int ctc_tensor_load_tns(const char *path, ctc_tensor **out);
+/* SPLATT binary coordinate form, the reference's .bin path
+ * (sgpu/io.c:116-150 p_write_tt_binary_header, io.c:347-431
+ * tt_write_binary_file; header sgpu/io.h:67-84): int32 magic 0, u64
+ * idx_width, u64 val_width, then idx_width-byte nmodes, dims[nmodes], nnz,
+ * the index arrays (as stored: 1-based from .tns files) and nnz values of
+ * val_width bytes.  The reference writes idx_width 8 and, through a
+ * comparison of a double with itself (io.c:137-143), always val_width 4,
+ * and its reader exits on idx_width 8 (io.c:444-449): its own files are
+ * unreadable.  Here the loader reads idx_width 4 or 8 and val_width 4 or 8
+ * (so the reference's files too), and the writer uses 4-byte words when
+ * every count and index fits, 4-byte values only when every value is
+ * exactly a float. */
+int ctc_tensor_save_splatt(const ctc_tensor *t, const char *path);
+/* Text output, one line per nonzero: the indices as stored ("%llu "), then
+ * the value with "%.<digits>f" (digits 0..40), or "%.17g" (round trip of
+ * the double) when digits < 0.  The reference's data-prep scripts write
+ * "%d %d %d %.1f" (software/scripts/tvtensor.py:122-129, stensor.py:39-43):
+ * digits = 1 gives their bytes. */
+int ctc_tensor_write_tns(const ctc_tensor *t, const char *path, int digits);
+/* Seeded train / test / validation split of software/scripts/tvtensor.py
+ * (:64-120): the nonzeros are sorted stably by (ind[0], ind[1]) (:103),
+ * then each in that order draws flag = random.randint(0, 9) from Python's
+ * Mersenne Twister seeded by random.seed(seed) (the script leaves it
+ * unseeded) and goes to train (flag < 8), test (flag == 8) or validation
+ * (flag == 9).  Outputs keep that order; dims are each output's maximum
+ * index.  Any output pointer may be NULL.  The script's mode-2 and mode-3
+ * copies (stensor.py:36-43) are ctc_tensor_sort(t, 1) and (t, 2) of the
+ * training output. */
+int ctc_tensor_split(const ctc_tensor *t, uint64_t seed, ctc_tensor **train, ctc_tensor **test,
+                     ctc_tensor **val);
 /* Binary form (replaces the broken .bin path, sgpu/io.c:125, 444-476):
  * header "CTCB", u32 version, u32 nmodes, u64 nnz, u64 dims[nmodes], then
  * nmodes arrays of u64 indices and one array of f64 values. */
@@ -195,7 +228,13 @@ typedef struct {
     int iters;             /* epochs (reference DEFAULT_MAX_ITERATE 1000)           */
     int inner;             /* CCD++ inner sweeps per column                         */
     int tile_len;          /* nonzeros per warp work unit (0 = tuned)               */
-    int threads_per_block; /* 0 = tuned                                             */
+    int threads_per_block; /* Hogwild SGD threads per block, the reference GA's
+                              block-size gene (ga/sgd.cu:66-78, fitness.c:67-75:
+                              2^(2..9)): 32, 64, 128, 256 or 512; 0 = 256 (an
+                              autotuner axis).  4-16 are rejected (CTC_E_UNSUP:
+                              a block is whole warps here).  The other
+                              algorithms' kernels have fixed block shapes and do
+                              not read it                                        */
     int precision;         /* enum ctc_precision                                    */
     int compat;            /* 1: reference kernel semantics (values stored through
                               an integer, sgpu/ciss.c:163; ALS/CCD per-tile lane
@@ -231,6 +270,12 @@ typedef struct {
 
 /* Reference-default parameters for an algorithm (sgpu/base.h:19-64). */
 int ctc_params_default(int alg, ctc_params *p);
+/* The checks ctc_run / ctc_dataset_create / ctc_autotune make on `p`
+ * (algorithm, precision, rank, tile length, block size ...), on the host:
+ * CTC_OK, or the code and message those calls would fail with.  Lets a
+ * parameter search (the reference's GA, ga/fitness.c:67-79) drop invalid
+ * candidates without a device. */
+int ctc_params_check(const ctc_params *p);
 
 typedef struct {
     int epoch;
@@ -297,6 +342,15 @@ int ctc_dataset_epochs(ctc_dataset *d, int n);
 int ctc_dataset_set_lr(ctc_dataset *d, double lr);
 int ctc_dataset_evaluate(ctc_dataset *d, ctc_epoch_stats *st);
 int ctc_dataset_get_model(ctc_dataset *d, ctc_model *model);
+/* Bounded device waits (the tensor-core Gram's wait for its MMAs, the
+ * CCD++ pass's wait for its staged columns) give up after about 2 s and
+ * set the session's error flag; the next ctc_dataset_evaluate (or the
+ * evaluation inside ctc_dataset_run) returns CTC_E_TIMEOUT once and clears
+ * the flag, as does ctc_dataset_set_model.  probe_wait is a self-test of
+ * that path with no reference counterpart: it enqueues one kernel whose
+ * bounded wait, on a barrier nothing arrives at, expires after limit_ns
+ * (at most 2e9) and sets the flag. */
+int ctc_dataset_probe_wait(ctc_dataset *d, uint64_t limit_ns);
 
 /* Batches of independent completion problems (no reference counterpart;
  * the reference runs one problem per process).  Instance b's training and
@@ -342,6 +396,7 @@ typedef struct {
     double ms_epoch;   /* device time of one update epoch */
     int cached;
     int sgd_atomic;    /* SGD: the Hogwild reduction mode tried */
+    int threads_per_block; /* SGD: the block size tried (0 = 256) */
 } ctc_tune_trial;
 int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], const ctc_params *p,
                  const char *cache_path, int flags, ctc_params *out, ctc_tune_trial *trials,
@@ -386,6 +441,14 @@ int ctc_fo_dims(const ctc_fo *f, int *order, uint64_t *dims);
  * (lambda sum ||U||^2) and the train/test RMSE after evaluated epochs. */
 int ctc_fo_run(ctc_fo *f, ctc_model *model, const ctc_fo_params *p, ctc_epoch_cb cb, void *user,
                ctc_result *res);
+/* The gradient the training step uses, for checking it: at `model`, over
+ * every training nonzero of f in one pass of the minibatch adjoint kernel
+ * (scale 1), with the precision and lambda f was created with (FP32 or
+ * BF16 gathers, FP32 accumulation), plus 2 lambda U added in FP64.
+ * grads[m]: dims[m] x rank row-major doubles; obj (may be NULL): the
+ * pass's FP64 loss sum + lambda sum ||U||^2.  ctc_grad gives the same
+ * quantities in FP64. */
+int ctc_fo_grad(ctc_fo *f, const ctc_model *model, double *const *grads, double *obj);
 
 /* Per-kernel device time: with profiling on, every launch of this library
  * on the context is bracketed by a CUDA event pair; kernel_time sums the
@@ -408,11 +471,18 @@ int ctc_rmse(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double *
  * 0-based indices, FP32 value); U0..U2: device row-major FP32 factors
  * (dims x rank); out_sse: one device double receiving sum (x - xhat)^2;
  * stream: a cudaStream_t (NULL = legacy default stream).  Asynchronous.
+ * rec, U0, U1, U2 must be 16-byte aligned and out_sse 8-byte aligned
+ * (CTC_E_ARG otherwise, before any launch); every record's i0, i1, i2 must
+ * be below the row count of U0, U1, U2 (not checked: there is no dims
+ * argument, and an index past the rows reads out of bounds).
  * Scratch is a fixed 512 KiB file-scope device array (65536 partial sums
  * of 16384 nonzeros), held until exit by every GPU that loads the library:
  * n above 2^30 is rejected (CTC_E_ARG).  All calls share that array, so
  * calls that overlap on the GPU race.  The first call on a device looks up
- * the array's address (make it before any stream capture there). */
+ * the array's address (make it before any stream capture there); under
+ * CUDA's lazy module loading that first call, or the library's first kernel
+ * launch on the device, also loads the array, which takes device memory:
+ * make it before another allocator reserves the device. */
 int ctc_sse_noalloc(const void *rec, uint64_t n, const float *U0, const float *U1,
                     const float *U2, int rank, double *out_sse, void *stream);
 

@@ -272,6 +272,8 @@ def ref_host():
         L.tt_free.argtypes = [C.POINTER(_RefSptensor)]
         L.ciss_alloc.argtypes = [C.POINTER(_RefSptensor), C.c_uint64]
         L.ciss_alloc.restype = C.POINTER(_RefCiss)
+        L.tt_write_binary.argtypes = [C.POINTER(_RefSptensor), C.c_char_p]
+        L.tt_write_binary.restype = None
         _ref = L
     return _ref
 
@@ -288,6 +290,16 @@ def ref_tt_read(path):
     dims = [t.dims[m] for m in range(nm)]
     ref_host().tt_free(p)
     return Tensor(ind, vals, dims)
+
+
+def ref_tns_to_bin(tns_path, bin_path):
+    """sgpu/sptensor.c:64 tt_read of a .tns file, then sgpu/io.c:347
+    tt_write_binary of the result, both run from the reference's own code."""
+    p = ref_host().tt_read(tns_path.encode())
+    if not p:
+        raise OSError(tns_path)
+    ref_host().tt_write_binary(p, bin_path.encode())
+    ref_host().tt_free(p)
 
 
 def ref_ciss_alloc(T: Tensor, mode1: int):
@@ -349,3 +361,32 @@ def cp_grad(ind, vals, U, lam):
         np.add.at(g, idx[m], -e[:, None] * others)
         G.append(g)
     return G
+
+
+# ---------------------------------------------------------------------------
+# tc_converge bookkeeping (sgpu/completion.c:296-362), called after every
+# epoch from the first (sgpu/als.cu:803-806): the convergence RMSE is the
+# validation RMSE when a validation tensor is given (:318-324), else the
+# training RMSE; an improvement by more than the tolerance (TOLERANCE 1e-4,
+# sgpu/base.h:32) resets the bad-epoch count and saves the model as the best
+# (:330-338); otherwise the count grows and reaching MAX_BADEPOCHS (3,
+# base.h:36) converges (:339-345).  best_rmse starts at BEST_RMSE (1e7,
+# base.h:35).
+# ---------------------------------------------------------------------------
+class Converge:
+    def __init__(self, tolerance=1e-4, max_bad=3):
+        self.tolerance = tolerance
+        self.max_bad = max_bad
+        self.best_rmse = 10000000.0
+        self.nbad = 0
+        self.best_epoch = 0
+
+    def step(self, epoch, rmse):
+        """Returns (improved, converged)."""
+        if rmse - self.best_rmse < -self.tolerance:
+            self.nbad = 0
+            self.best_rmse = rmse
+            self.best_epoch = epoch
+            return True, False
+        self.nbad += 1
+        return False, self.nbad == self.max_bad

@@ -16,16 +16,20 @@ def test_tune_sgd_searches_caches_and_hits(ctx, tmp_path):
     p = ctc.params(ctc.SGD, rank=16, lr=0.01, lr_scale=1.0, **{"lambda": 0.01})
     path = str(tmp_path / "tune.txt")
     q, trials = ctc.autotune(ctx, P.c_sorted(), p, cache_path=path)
-    # tile length x lanes per nonzero x reduction mode (vector atomics, bulk rows)
-    assert len(trials) == 24 and all(t["cached"] == 0 and t["ms_epoch"] > 0 for t in trials)
+    # tile length x lanes per nonzero x reduction mode (vector atomics, bulk
+    # rows) at 256 threads per block, then 128 and 512 threads for each tile
+    # length's fastest candidate
+    assert len(trials) == 24 + 8 and all(t["cached"] == 0 and t["ms_epoch"] > 0 for t in trials)
     assert {t["sgd_atomic"] for t in trials} == {1, 2}
+    assert {t["threads_per_block"] for t in trials} == {0, 128, 512}
     assert q.tile_len in (128, 256, 512, 1024) and q.threads_per_row in (4, 2, 1) and q.sgd_atomic in (1, 2)
+    assert q.threads_per_block in (0, 128, 512)
     best = min(trials, key=lambda t: t["ms_epoch"])
-    assert (q.tile_len, q.threads_per_row, q.sgd_atomic) == (best["tile_len"], best["threads_per_row"],
-                                                             best["sgd_atomic"])
+    keys = ("tile_len", "threads_per_row", "sgd_atomic", "threads_per_block")
+    assert tuple(getattr(q, k) for k in keys) == tuple(best[k] for k in keys)
     q2, trials2 = ctc.autotune(ctx, P.c_sorted(), p, cache_path=path)
     assert len(trials2) == 1 and trials2[0]["cached"] == 1
-    assert (q2.tile_len, q2.threads_per_row, q2.sgd_atomic) == (q.tile_len, q.threads_per_row, q.sgd_atomic)
+    assert tuple(getattr(q2, k) for k in keys) == tuple(getattr(q, k) for k in keys)
     assert ctc.tune_lookup(path, P.c_sorted()[0], p) is not None
 
 

@@ -33,13 +33,28 @@ def test_lookup_hit_miss_and_last_entry_wins(tmp_path):
     with open(path, "w") as f:
         f.write("garbage line\n")
         f.write("alg=9,other 1 2 3\n")
-        f.write(f"{key} tile_len=128 threads_per_row=0 smem_budget=-1 sgd_atomic=1 ms=1.5\n")
-        f.write(f"{key} tile_len=512 threads_per_row=0 smem_budget=0 sgd_atomic=2 ms=1.2\n")
-        # a line without the reduction mode (an older cache) is not an entry
+        f.write(f"{key} tile_len=128 threads_per_row=0 smem_budget=-1 sgd_atomic=1 threads_per_block=0 ms=1.5\n")
+        f.write(f"{key} tile_len=512 threads_per_row=0 smem_budget=0 sgd_atomic=2 threads_per_block=128 ms=1.2\n")
+        # lines without the reduction mode or the block size (older caches) are not entries
         f.write(f"{key} tile_len=256 threads_per_row=0 smem_budget=0 ms=1.0\n")
+        f.write(f"{key} tile_len=256 threads_per_row=0 smem_budget=0 sgd_atomic=2 ms=1.0\n")
     q = ctc.tune_lookup(path, t, p)
     assert q is not None
-    assert (q.tile_len, q.threads_per_row, q.smem_budget, q.sgd_atomic) == (512, 0, 0, 2)
+    assert (q.tile_len, q.threads_per_row, q.smem_budget, q.sgd_atomic, q.threads_per_block) == (512, 0, 0, 2, 128)
     # everything else is the caller's
     assert q.rank == 32 and q.alg == ctc.CCDPP and abs(q.lambda_ - p.lambda_) == 0
     assert ctc.tune_lookup(path, t, ctc.params(ctc.CCDPP, rank=16)) is None
+
+
+def test_block_size_is_validated_on_the_host():
+    """threads_per_block: 0 or a power of two up to 512; the reference GA's
+    4-16 thread blocks are below a warp and rejected as unsupported.  The
+    checks run before any device is touched."""
+    import ctypes as C
+    L = ctc.lib()
+    for ok in (0, 32, 64, 128, 256, 512):
+        assert L.ctc_params_check(C.byref(ctc.params(ctc.SGD, rank=16, threads_per_block=ok))) == 0
+    for bad, code in ((100, -1), (1024, -1), (-32, -1), (16, -5), (4, -5)):
+        p = ctc.params(ctc.SGD, rank=16, threads_per_block=bad)
+        assert L.ctc_params_check(C.byref(p)) == code, bad
+        assert b"threads_per_block" in L.ctc_last_error()
