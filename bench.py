@@ -664,7 +664,7 @@ def als_leg(ctc, ctx, args, device):
     out = {"workload": w.name, "dims": list(w.dims), "nnz_train": ntr, "rank": w.rank, "lambda": lam,
            "generate_s": time.time() - t0}
     iters = 3
-    forms = [("fp32", ctc.PREC_F32)] + ([("mixed_tc", ctc.PREC_MIXED)] if w.rank == 64 else [])
+    forms = [("fp32", ctc.PREC_F32)] + ([("mixed_tc", ctc.PREC_MIXED)] if w.rank in (32, 64) else [])
     for name, prec in forms:
         p = ctc.params("als", rank=w.rank, precision=prec, iters=iters, early_stop=0, eval_every=0,
                        **{"lambda": lam})

@@ -1,10 +1,11 @@
 // als_tc.cuh -- ALS Gram blocks on the 5th-generation tensor cores
-// (tcgen05.mma, accumulator in tensor memory), rank 64, mixed precision.
+// (tcgen05.mma, accumulator in tensor memory), ranks 64 and 32, mixed
+// precision.
 //
 // For one piece of a long row (tile_len nonzeros of one row of the mode's
 // sorted copy) the CTA forms
-//     G = sum_k h_k h_k^T      (64 x 64, FP32 in TMEM)
-//     b = sum_k x_k h_k        (64, FP32 on the CUDA cores)
+//     G = sum_k h_k h_k^T      (R x R, FP32 in TMEM)
+//     b = sum_k x_k h_k        (R, FP32 on the CUDA cores)
 // with h_k = U_a(q1) o U_b(q2) read from BF16 copies of the factors, and
 // writes them to the piece's slot ({G row-major, b}, the layout the FP64
 // fixup solve k_als_fix reads).
@@ -29,10 +30,8 @@
 namespace ctc {
 namespace tc {
 
-constexpr int kR = 64;        // rank handled here
 constexpr int kChunk = 128;   // nonzeros staged per round (one per thread)
 constexpr int kThreads = 128;
-constexpr int kSmemBytes = kChunk * 128 + 1024;  // operand tile + alignment slack
 
 using px::smem_u32;
 using px::mbar_try_wait;
@@ -99,25 +98,41 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 }
 
 // Gram + right-hand side of the heavy pieces listed in `pieces` (tile
-// indices of the mode's plan); slot[t] = {G (64 x 64 row-major), b (64)}.
-// err[0] is set when a bounded wait expires.
-static __global__ void __launch_bounds__(kThreads, 2)
+// indices of the mode's plan), rank R = 64 or 32; slot[t] = {G (R x R
+// row-major), b (R)}.  err[0] is set when a bounded wait expires.
+//
+// Operand rows are 128 bytes.  At R = 64 a row is one nonzero's h.  At
+// R = 32 a row holds two nonzeros, h(k) in its first 64 bytes and h(k + 64)
+// in its second: the 64 x 64 product of such rows has the Grams of the two
+// halves on its diagonal blocks (the off-diagonal blocks are not read), so
+// a 128-nonzero chunk is 64 rows and 4 MMAs, and G = block(0,0) +
+// block(1,1), added in that order.
+//
+// Two operand tiles alternate: while the MMAs of one chunk run, the CTA
+// gathers the next chunk into the other tile; a tile is rewritten only
+// after the MMAs that read it have arrived on its mbarrier.
+template <int R>
+__global__ void __launch_bounds__(kThreads, R == 64 ? 2 : 4)
     k_als_gram_tc(const int4 *__restrict__ tiles, const uint32_t *__restrict__ pieces, uint32_t npieces,
                   const uint4 *__restrict__ rec, int m, const __nv_bfloat16 *__restrict__ Ua,
                   const __nv_bfloat16 *__restrict__ Ub, float *__restrict__ slot, int *err)
 {
-    // the swizzled operand tile: kChunk x 128 B, 1 KiB aligned inside the
-    // dynamic shared memory (launched with kSmemBytes)
+    static_assert(R == 64 || R == 32, "tensor-core Gram ranks");
+    constexpr int kRows = R == 64 ? kChunk : kChunk / 2;  // operand rows per chunk
+    constexpr int kTile = kRows * 128;                     // bytes per operand tile
+    constexpr int kVec = R / 8;                            // 16-byte words of a BF16 factor row
     extern __shared__ uint8_t dsm[];
-    uint8_t *hs = dsm + ((1024u - (smem_u32(dsm) & 1023u)) & 1023u);
-    __shared__ float rhs_part[kThreads / 32][kR];
-    __shared__ __align__(8) uint64_t mbar;
+    uint8_t *hs0 = dsm + ((1024u - (smem_u32(dsm) & 1023u)) & 1023u);
+    __shared__ float rhs_part[kThreads / 32][R];
+    __shared__ float gsum[R == 32 ? 32 * 32 : 1];
+    __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t tmem_base_sh;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
-    const uint32_t mbar_addr = smem_u32(&mbar);
-    const uint32_t hs_addr = smem_u32(hs);
     const uint32_t idesc = idesc_bf16_m64_n64();
+    // this thread's operand row and its first 16-byte chunk within the row
+    const int orow = R == 64 ? tid : (tid & 63);
+    const int ochunk = R == 64 ? 0 : (tid >> 6) * 4;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -126,38 +141,61 @@ static __global__ void __launch_bounds__(kThreads, 2)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_addr));
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[b])));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem_d = tmem_base_sh;
-    uint32_t phase = 0;
+    // bit b: the phase tile b's mbarrier completes next / MMAs reading tile b
+    // are in flight (bits, not arrays, so they stay in registers)
+    uint32_t phases = 0u, pending = 0u;
+    uint32_t nchunk = 0;  // chunks issued by this CTA (selects the tile)
     bool ok = true;
+    // wait for the MMAs that read tile b (every thread; the outcome is made
+    // CTA-uniform so that no thread leaves while others sit at a barrier)
+    auto drain = [&](int b) {
+        if (!((pending >> b) & 1u) || !ok) return;
+        const int got = mbar_wait_bounded(smem_u32(&mbar[b]), (phases >> b) & 1u) ? 1 : 0;
+        ok = __syncthreads_and(got) != 0;
+        phases ^= 1u << b;
+        pending &= ~(1u << b);
+    };
 
     for (uint32_t pi = blockIdx.x; pi < npieces && ok; pi += gridDim.x) {
         const uint32_t tile = pieces[pi];
         const int4 td = tiles[tile];
         const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
-        float rhs[kR];
+        float rhs[R];
 #pragma unroll
-        for (int f = 0; f < kR; ++f) rhs[f] = 0.f;
+        for (int f = 0; f < R; ++f) rhs[f] = 0.f;
         for (uint32_t c0 = start; c0 < end && ok; c0 += kChunk) {
+            const int b = (int)(nchunk & 1u);
+            drain(b);
+            if (!ok) break;
+            uint8_t *hs = hs0 + b * kTile;
+            uint8_t *row = hs + orow * 128;
             const uint32_t p = c0 + tid;
-            uint8_t *row = hs + tid * 128;
             if (p < end) {
                 const uint4 r = rec[p];
                 const float x = __uint_as_float(r.w);
                 const uint32_t q1 = m1 == 0 ? r.x : (m1 == 1 ? r.y : r.z);
                 const uint32_t q2 = m2 == 0 ? r.x : (m2 == 1 ? r.y : r.z);
-                const uint4 *ba = reinterpret_cast<const uint4 *>(Ua + (size_t)q1 * kR);
-                const uint4 *bb = reinterpret_cast<const uint4 *>(Ub + (size_t)q2 * kR);
+                const uint4 *ba = reinterpret_cast<const uint4 *>(Ua + (size_t)q1 * R);
+                const uint4 *bb = reinterpret_cast<const uint4 *>(Ub + (size_t)q2 * R);
+                uint4 va[kVec], vb[kVec];
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    const uint4 va = ba[c], vb = bb[c];
-                    const __nv_bfloat162 *pa = reinterpret_cast<const __nv_bfloat162 *>(&va);
-                    const __nv_bfloat162 *pb = reinterpret_cast<const __nv_bfloat162 *>(&vb);
+                for (int c = 0; c < kVec; ++c) {
+                    va[c] = ba[c];
+                    vb[c] = bb[c];
+                }
+#pragma unroll
+                for (int c = 0; c < kVec; ++c) {
+                    const __nv_bfloat162 *pa = reinterpret_cast<const __nv_bfloat162 *>(&va[c]);
+                    const __nv_bfloat162 *pb = reinterpret_cast<const __nv_bfloat162 *>(&vb[c]);
                     uint32_t outw[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
@@ -168,12 +206,13 @@ static __global__ void __launch_bounds__(kThreads, 2)
                         rhs[8 * c + 2 * q + 1] += x * h1;
                         outw[q] = pack_bf16(h0, h1);
                     }
-                    *reinterpret_cast<uint4 *>(row + ((c ^ (tid & 7)) << 4)) =
+                    *reinterpret_cast<uint4 *>(row + (((ochunk + c) ^ (orow & 7)) << 4)) =
                         make_uint4(outw[0], outw[1], outw[2], outw[3]);
                 }
             } else {
 #pragma unroll
-                for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4 *>(row + (c << 4)) = make_uint4(0, 0, 0, 0);
+                for (int c = 0; c < kVec; ++c)
+                    *reinterpret_cast<uint4 *>(row + (((ochunk + c) ^ (orow & 7)) << 4)) = make_uint4(0, 0, 0, 0);
             }
             // make the generic-proxy stores visible to the tensor core
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -181,56 +220,86 @@ static __global__ void __launch_bounds__(kThreads, 2)
             if (tid == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t nk = min((uint32_t)kChunk, end - c0);
-                const uint32_t nmma = (nk + 15) / 16;
+                const uint32_t rows = R == 64 ? nk : min(nk, (uint32_t)kRows);
+                const uint32_t nmma = (rows + 15) / 16;
+                const uint32_t hs_addr = smem_u32(hs);
                 for (uint32_t kk = 0; kk < nmma; ++kk) {
                     const uint64_t d = smem_desc_sw128(hs_addr + kk * 16 * 128);
                     mma_bf16(tmem_d, d, d, idesc, (c0 != start || kk != 0) ? 1u : 0u);
                 }
-                mma_commit(mbar_addr);
+                mma_commit(smem_u32(&mbar[b]));
             }
-            // every thread waits; the outcome is made CTA-uniform so no
-            // thread can leave the loop while others sit at a barrier
-            const int got = mbar_wait_bounded(mbar_addr, phase) ? 1 : 0;
-            ok = __syncthreads_and(got) != 0;
-            if (!ok) break;
-            phase ^= 1;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            pending |= 1u << b;
+            ++nchunk;
         }
+        // the accumulator is complete once both tiles' MMAs have arrived
+        drain(0);
+        drain(1);
         if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         // right-hand side: warp butterflies, then a fixed-order sum over warps
 #pragma unroll
-        for (int f = 0; f < kR; ++f) {
+        for (int f = 0; f < R; ++f) {
             float v = rhs[f];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) rhs_part[warp][f] = v;
         }
-        // Gram rows 16w..16w+15 from this warp's TMEM lanes
+        // accumulator rows 16w..16w+15 live in TMEM lanes 32w..32w+15
         uint32_t g[64];
         tmem_ld_32x32b_x64(tmem_d + ((uint32_t)(32 * warp) << 16), g);
-        float *dst = slot + (size_t)tile * (kR * kR + kR);
-        if (lane < 16) {
-            const int grow = 16 * warp + lane;
-            float4 *d4 = reinterpret_cast<float4 *>(dst + grow * kR);
+        float *dst = slot + (size_t)tile * (R * R + R);
+        if constexpr (R == 64) {
+            if (lane < 16) {
+                const int grow = 16 * warp + lane;
+                float4 *d4 = reinterpret_cast<float4 *>(dst + grow * R);
 #pragma unroll
-            for (int q = 0; q < 16; ++q)
-                d4[q] = make_float4(__uint_as_float(g[4 * q]), __uint_as_float(g[4 * q + 1]),
-                                    __uint_as_float(g[4 * q + 2]), __uint_as_float(g[4 * q + 3]));
+                for (int q = 0; q < 16; ++q)
+                    d4[q] = make_float4(__uint_as_float(g[4 * q]), __uint_as_float(g[4 * q + 1]),
+                                        __uint_as_float(g[4 * q + 2]), __uint_as_float(g[4 * q + 3]));
+            }
+        } else {
+            // block (1,1): accumulator rows 32..63, columns 32..63 (warps 2, 3)
+            if (warp >= 2 && lane < 16) {
+                const int grow = 16 * (warp - 2) + lane;
+#pragma unroll
+                for (int q = 0; q < 32; ++q) gsum[grow * 32 + q] = __uint_as_float(g[32 + q]);
+            }
+            __syncthreads();
+            // block (0,0): rows 0..31, columns 0..31 (warps 0, 1), plus block (1,1)
+            if (warp < 2 && lane < 16) {
+                const int grow = 16 * warp + lane;
+                float4 *d4 = reinterpret_cast<float4 *>(dst + grow * R);
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    d4[q] = make_float4(__uint_as_float(g[4 * q]) + gsum[grow * 32 + 4 * q],
+                                        __uint_as_float(g[4 * q + 1]) + gsum[grow * 32 + 4 * q + 1],
+                                        __uint_as_float(g[4 * q + 2]) + gsum[grow * 32 + 4 * q + 2],
+                                        __uint_as_float(g[4 * q + 3]) + gsum[grow * 32 + 4 * q + 3]);
+            }
         }
         __syncthreads();
-        if (tid < kR) dst[kR * kR + tid] = ((rhs_part[0][tid] + rhs_part[1][tid]) + rhs_part[2][tid]) + rhs_part[3][tid];
+        if (tid < R) dst[R * R + tid] = ((rhs_part[0][tid] + rhs_part[1][tid]) + rhs_part[2][tid]) + rhs_part[3][tid];
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     }
     if (!ok) {
-        // report, and give the MMAs in flight one more bounded wait before
-        // the tensor memory they write is released
+        // report, and give the MMAs in flight one more bounded wait each
+        // before the tensor memory they write is released
         if (tid == 0) atomicExch(err, 1);
-        mbar_wait_bounded(mbar_addr, phase);
+        for (int b = 0; b < 2; ++b)
+            if ((pending >> b) & 1u) mbar_wait_bounded(smem_u32(&mbar[b]), (phases >> b) & 1u);
     }
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(64u));
+}
+
+// dynamic shared memory of k_als_gram_tc<R>: two operand tiles + alignment
+template <int R>
+constexpr int gram_smem_bytes()
+{
+    return 2 * (R == 64 ? kChunk : kChunk / 2) * 128 + 1024;
 }
 
 // FP32 factor rows -> BF16 copies (row-major, same shape)

@@ -568,10 +568,14 @@ struct Session : SessionBase {
             set_ccdpp_smem<8>();
             set_ccdpp_smem<16>();
         }
-        tc = p.alg == CTC_ALG_ALS && p.precision == CTC_PREC_MIXED && R == 64 && std::is_same<T, float>::value;
-        if (tc) {
-            for (int m = 0; m < 3; ++m) Ubf[m].alloc((size_t)dims[m] * R);
-            CK(cudaFuncSetAttribute(tc::k_als_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
+        tc = p.alg == CTC_ALG_ALS && p.precision == CTC_PREC_MIXED && (R == 64 || R == 32) &&
+             std::is_same<T, float>::value;
+        if constexpr (R == 64 || R == 32) {
+            if (tc) {
+                for (int m = 0; m < 3; ++m) Ubf[m].alloc((size_t)dims[m] * R);
+                CK(cudaFuncSetAttribute(tc::k_als_gram_tc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        tc::gram_smem_bytes<R>()));
+            }
         }
         if (p.alg == CTC_ALG_SGD && std::is_same<T, float>::value) {
             // bulk row reductions stage 2 x 3 rows per group in shared memory
@@ -797,10 +801,10 @@ struct Session : SessionBase {
 
     void als_gram_tc(DevTensor<T> &c, int m)
     {
-        if constexpr (std::is_same<T, float>::value) {
+        if constexpr (std::is_same<T, float>::value && (R == 64 || R == 32)) {
             const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
-            const unsigned g = std::min<unsigned>(c.npieces, 2 * kSMs);
-            LAUNCH(ctx, tc::k_als_gram_tc, g, tc::kThreads, tc::kSmemBytes, (const int4 *)c.tiles.p,
+            const unsigned g = std::min<unsigned>(c.npieces, (R == 64 ? 2 : 4) * kSMs);
+            LAUNCH(ctx, tc::k_als_gram_tc<R>, g, tc::kThreads, tc::gram_smem_bytes<R>(), (const int4 *)c.tiles.p,
                    (const uint32_t *)c.pieces.p, c.npieces, (const uint4 *)c.rec.p, m,
                    (const __nv_bfloat16 *)Ubf[m1].p, (const __nv_bfloat16 *)Ubf[m2].p, (float *)slot.p, dev_err.p);
         }
@@ -1207,8 +1211,8 @@ static void check_params(const ctc_params *p)
     if (p->alg < CTC_ALG_ALS || p->alg > CTC_ALG_CCDPP) fail(CTC_E_ARG, "unknown algorithm %d", p->alg);
     if (p->precision != CTC_PREC_F32 && p->precision != CTC_PREC_F64 && p->precision != CTC_PREC_MIXED)
         fail(CTC_E_ARG, "unknown precision %d", p->precision);
-    if (p->precision == CTC_PREC_MIXED && !(p->alg == CTC_ALG_ALS && p->rank == 64))
-        fail(CTC_E_UNSUP, "mixed precision (BF16 tensor-core Gram) is available for ALS at rank 64");
+    if (p->precision == CTC_PREC_MIXED && !(p->alg == CTC_ALG_ALS && (p->rank == 64 || p->rank == 32)))
+        fail(CTC_E_UNSUP, "mixed precision (BF16 tensor-core Gram) is available for ALS at ranks 32 and 64");
     if (p->rank != 8 && p->rank != 16 && p->rank != 32 && p->rank != 64)
         fail(CTC_E_UNSUP, "rank %d not supported (8, 16, 32, 64)", p->rank);
     if (p->tile_len < 0 || p->tile_len > (1 << 20)) fail(CTC_E_ARG, "tile_len %d", p->tile_len);

@@ -108,26 +108,29 @@ def test_als_heavy_rows(ctx):
     assert max_factor_rel(G, U) < 1e-9
 
 
-def test_als_mixed_tensor_core(ctx):
-    """Rank 64, mixed precision: pieces of long rows get their Gram from
-    tcgen05 MMAs on BF16 factor copies (FP32 accumulation in tensor memory),
-    every row its FP64 solve.  Final test RMSE within 0.5 % of plain FP32,
+@pytest.mark.parametrize("R,tile_len", [(64, 256), (32, 256), (32, 96), (32, 48)])
+def test_als_mixed_tensor_core(ctx, R, tile_len):
+    """Ranks 64 and 32, mixed precision: pieces of long rows get their Gram
+    from tcgen05 MMAs on BF16 factor copies (FP32 accumulation in tensor
+    memory), every row its FP64 solve.  At rank 32 one 128-byte operand row
+    carries two nonzeros; tile lengths 96 and 48 give chunks of more and of
+    fewer than 64 nonzeros.  Final test RMSE within 0.5 % of plain FP32,
     first-iteration factors within BF16-level error of the FP64 oracle."""
-    P = Problem(60000, (200, 150, 100), 64, seed=30, heavy_row=20000)
+    P = Problem(60000, (200, 150, 100), R, seed=30, heavy_row=20000)
     lam = {"lambda": 0.05}
-    # tile length 256: every mode has rows longer than a tile, so the
-    # tensor-core Gram runs once per mode and iteration
-    _, o32 = engine_run(ctx, P, ctc.ALS, 5, precision=ctc.PREC_F32, tile_len=256, **lam)
+    # every mode has rows longer than a tile, so the tensor-core Gram runs
+    # once per mode and iteration
+    _, o32 = engine_run(ctx, P, ctc.ALS, 5, precision=ctc.PREC_F32, tile_len=tile_len, **lam)
     ctx.set_profiling(True)
     ctx.reset_kernel_times()
-    Gm, om = engine_run(ctx, P, ctc.ALS, 5, precision=ctc.PREC_MIXED, tile_len=256, **lam)
+    Gm, om = engine_run(ctx, P, ctc.ALS, 5, precision=ctc.PREC_MIXED, tile_len=tile_len, **lam)
     n_tc, ms_tc = ctx.kernel_time("k_als_gram_tc")
     ctx.set_profiling(False)
     assert n_tc == 3 * 5, n_tc
     te32, tem = o32.epochs[-1]["rmse_te"], om.epochs[-1]["rmse_te"]
     assert abs(tem - te32) / te32 < 0.005, (tem, te32)
     U, _ = oracle_als(P, 1, 0.05)
-    G1, _ = engine_run(ctx, P, ctc.ALS, 1, precision=ctc.PREC_MIXED, tile_len=256, **lam)
+    G1, _ = engine_run(ctx, P, ctc.ALS, 1, precision=ctc.PREC_MIXED, tile_len=tile_len, **lam)
     assert max_factor_rel(G1, U) < 3e-2
 
 
