@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="library defaults instead of autotuned parameters")
     ap.add_argument("--als", action="store_true",
                     help="the ALS leg alone on --workload (zipf-400m runs it by default)")
+    ap.add_argument("--ref-cuda", action="store_true",
+                    help="with --impl reference: time the reference's own CUDA kernels (built from its sources "
+                         "for sm_100a) on this GPU instead of the CPU restatement")
     return ap.parse_args()
 
 
@@ -155,16 +158,15 @@ def measured_peaks():
 
 
 def profile_traffic(kernel_tag):
-    """DRAM bytes per launch of a kernel from the committed ncu summary
-    (profiles/<kernel>.md, line 'dram_bytes_per_launch_full: <bytes>')."""
-    p = os.path.join(ROOT, "profiles", f"{kernel_tag}.md")
+    """DRAM bytes per launch of a kernel at the full workload, from the
+    committed record of its ncu capture (profiles/<kernel_tag>.json, which
+    holds the capture command and how the figure was scaled)."""
+    p = os.path.join(ROOT, "profiles", f"{kernel_tag}.json")
     try:
-        for line in open(p):
-            if line.strip().startswith("dram_bytes_per_launch_full:"):
-                return float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
-    return None
+        with open(p) as f:
+            return float(json.load(f)["dram_bytes_per_launch_full"])
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 def max_over_ranks(x: float, device, world: int) -> float:
@@ -352,6 +354,7 @@ def run_ours(args):
                                                                 **{"lambda": 0.1}))
         out["time_to_rmse"] = time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, args.seed, ds_als)
         ds_als.free()
+        out["mixed_vs_plain"] = mixed_vs_plain(ctc, ctx, tr, te, mdims, R, args.seed, p_ccd, out["time_to_rmse"])
         out["e2e"] = e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args, p_ccd, p_sgd)
         out["ciss_build"] = ciss_build_times(ctc, ctx, tr[0])
         v, s, threads, nsamp = cpu_baseline(base0, dims, R, args.sample, args.seed)
@@ -492,15 +495,17 @@ def fo_leg(ctc, ctx, args, device):
     return out
 
 
-def time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, seed, ds_als=None):
+def time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, seed, ds_als=None, legs=None, targets=None):
     """Plain FP32 schedules (CCD++ 10 outer x 3 inner, SGD 20 epochs, ALS
-    10 iterations); the target is 1.005 x the final test RMSE; time =
-    device time of the update epochs until the test RMSE first reaches it."""
+    10 iterations); the target is 1.005 x the final test RMSE (or the given
+    targets[name]); time = device time of the update epochs until the test
+    RMSE first reaches it."""
     import torch
     res = {}
-    legs = [("ccdpp", ds_ccd, 10), ("sgd", ds_sgd, 20)]
-    if ds_als is not None:
-        legs.append(("als", ds_als, 10))
+    if legs is None:
+        legs = [("ccdpp", ds_ccd, 10), ("sgd", ds_sgd, 20)]
+        if ds_als is not None:
+            legs.append(("als", ds_als, 10))
     for name, ds, iters in legs:
         m = ctc.Model(mdims, R).init_uniform(seed + 1, 1.0 / np.sqrt(R))
         ds.set_model(m)
@@ -523,11 +528,46 @@ def time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, seed, ds_als=None):
                 lr *= 0.95
                 ds.set_lr(lr)
         final = hist[-1][1]
-        target = final * 1.005
+        target = targets[name] if targets and name in targets else final * 1.005
         reach = next((h[0] for h in hist if h[1] <= target), None)
         res[name] = {"epochs": iters, "final_test_rmse": final, "final_train_rmse": hist[-1][2],
                      "target_test_rmse": target, "time_to_target_s": reach, "total_s": hist[-1][0],
                      "epoch_s": hist[-1][0] / iters}
+    return res
+
+
+def mixed_vs_plain(ctc, ctx, tr, te, mdims, R, seed, p_ccd, plain):
+    """The mixed-precision forms on the same tensor and schedules, against
+    the plain FP32 runs of time_to_rmse (`plain`): ALS with BF16 factor
+    copies into tcgen05 Gram blocks for the pieces of long rows (FP64 row
+    solves), and CCD++ with packed 8-byte slots (the residual in the key
+    word's low bits).  Target: 1.005 x the plain form's final test RMSE.
+    Hogwild SGD has no mixed form (its epoch is bound by same-row L2
+    reductions into the FP32 rows, which a narrower gather does not
+    remove)."""
+    legs = []
+    ds_als = ctc.Dataset(ctx, [tr[0]], None, te, ctc.params("als", rank=R, precision=ctc.PREC_MIXED, early_stop=0,
+                                                            iters=10, **{"lambda": 0.1}))
+    q = ctc.params("ccdpp", rank=R, inner=3, early_stop=0, iters=10, precision=ctc.PREC_MIXED,
+                   tile_len=p_ccd.tile_len, smem_budget=p_ccd.smem_budget, **{"lambda": 0.1})
+    ds_ccd = ctc.Dataset(ctx, [tr[0]], None, te, q)
+    legs = [("ccdpp", ds_ccd, 10), ("als", ds_als, 10)]
+    targets = {k: plain[k]["final_test_rmse"] * 1.005 for k in ("ccdpp", "als")}
+    mixed = time_to_rmse(ctc, None, None, mdims, R, seed, legs=legs, targets=targets)
+    ds_als.free()
+    ds_ccd.free()
+    res = {}
+    for k in ("ccdpp", "als"):
+        a, b = plain[k], mixed[k]
+        res[k] = {"plain_epoch_s": a["epoch_s"], "mixed_epoch_s": b["epoch_s"],
+                  "epoch_speedup": a["epoch_s"] / b["epoch_s"],
+                  "plain_final_test_rmse": a["final_test_rmse"], "mixed_final_test_rmse": b["final_test_rmse"],
+                  "final_rmse_rel_diff": (b["final_test_rmse"] - a["final_test_rmse"]) / a["final_test_rmse"],
+                  "target_test_rmse": targets[k], "plain_time_to_target_s": a["time_to_target_s"],
+                  "mixed_time_to_target_s": b["time_to_target_s"],
+                  "time_to_target_speedup": (a["time_to_target_s"] / b["time_to_target_s"]
+                                             if a["time_to_target_s"] and b["time_to_target_s"] else None)}
+    res["sgd"] = None
     return res
 
 
@@ -751,9 +791,104 @@ def run_batch_only(args):
     ctx.close()
 
 
+def run_reference_cuda(args):
+    """The reference's own CUDA kernels (sgpu/als.cu, ccd.cu, sgd.cu, built
+    from its sources for sm_100a at the workload's rank by
+    oracle/build_ref.sh and driven by oracle/ref_kernels_harness.cu with the
+    reference drivers' launch sequences and grids), timed with CUDA events
+    on this GPU on the workload's training tensor: its CISS copies come from
+    the reference's own ciss_alloc (oracle/_ref/libref_host.so), its
+    factors are U(0,1)/sqrt(R).  ALS: one iteration of three mode updates
+    (lambda 0.1; MTTKRP + Gram kernel, batched cuSOLVER Cholesky); CCD:
+    the reference's "CCD+" iteration of three modes (lambda 0.1; its grid
+    reaches about 1/32 of the tiles, sgpu/ccd.cu:520); SGD: one Hogwild
+    epoch with FP64 atomics (lr 1e-3, lambda 0.01).  All FP64, as the
+    reference computes.  Data transfers are outside the timed region."""
+    import ctypes as C
+
+    import torch
+
+    from oracle import pyoracle as po
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    device = f"cuda:{local}"
+    w, data = make_workload(args, device)
+    R = w.rank
+    suffix = "" if R == 16 else f"_r{R}"
+    libs = {}
+    for alg in ("als", "ccd", "sgd"):
+        path = os.path.join(po.REF_DIR, f"libref_{alg}{suffix}.so")
+        if not os.path.exists(path):
+            print(json.dumps({"impl": "reference", "unavailable": f"{path} not built (oracle/build_ref.sh)"}))
+            return
+        L = C.CDLL(path)
+        L.refh_rank.restype = C.c_int
+        if L.refh_rank() != R:
+            raise RuntimeError(f"{path} is built for rank {L.refh_rank()}, the workload needs {R}")
+        libs[alg] = L
+    ti, tv = data["train"]
+    n = int(tv.size)
+    del data
+    srt = sort_modes_torch(ti, tv, w.dims, device)
+    del ti, tv
+    torch.cuda.empty_cache()
+    dims = [int(d) for d in w.dims]
+    t0 = time.time()
+    ciss = []
+    for m in range(3):
+        T = po.Tensor(srt[m][0], srt[m][1], dims)
+        ciss.append(po.ref_ciss_alloc(T, m + 1))
+        del T
+    del srt
+    ciss_s = time.time() - t0
+    _u64p, _f64p = C.POINTER(C.c_uint64), C.POINTER(C.c_double)
+    rng = np.random.default_rng(args.seed + 1)
+    U0 = [rng.uniform(0, 1, (d, R)) / np.sqrt(R) for d in dims]
+    dims3 = np.array(dims, dtype=np.uint64)
+
+    def arr(xs, t):
+        return (C.POINTER(t) * len(xs))(*[x.ctypes.data_as(C.POINTER(t)) for x in xs])
+
+    ent = arr([c["entries"] for c in ciss], C.c_double)
+    dirs = arr([c["directory"] for c in ciss], C.c_uint64)
+    size_rows = (C.c_uint64 * 3)(*[c["size_rows"] for c in ciss])
+    dlen = (C.c_uint64 * 3)(*[c["dlength"] for c in ciss])
+    out = {}
+    ms = C.c_double()
+    for alg, lam, iters in (("als", 0.1, 1), ("ccd", 0.1, 2)):
+        U = [u.copy() for u in U0]
+        fn = getattr(libs[alg], f"refh_{alg}_bench")
+        fn.argtypes = [C.POINTER(_f64p), _u64p, C.POINTER(_u64p), _u64p, C.c_uint64, _u64p, C.POINTER(_f64p),
+                       C.c_double, C.c_int, C.POINTER(C.c_double)]
+        rc = fn(ent, size_rows, dirs, dlen, n, dims3.ctypes.data_as(_u64p), arr(U, C.c_double), lam, iters,
+                C.byref(ms))
+        out[alg] = {"rc": rc, "ms_per_iteration": ms.value if rc == 0 else None,
+                    "nnz_per_s": n / (ms.value / 1000.0) if rc == 0 and ms.value > 0 else None,
+                    "iterations_timed": iters}
+    U = [u.copy() for u in U0]
+    fn = libs["sgd"].refh_sgd_bench
+    fn.argtypes = [_f64p, C.c_uint64, _u64p, _u64p, C.c_uint64, C.c_uint64, _u64p, C.POINTER(_f64p), C.c_double,
+                   C.c_double, C.c_int, C.POINTER(C.c_double)]
+    c0 = ciss[0]
+    rc = fn(c0["entries"].ctypes.data_as(_f64p), c0["size_rows"], c0["directory"].ctypes.data_as(_u64p),
+            c0["dcounter"].ctypes.data_as(_u64p), c0["dlength"], n, dims3.ctypes.data_as(_u64p),
+            arr(U, C.c_double), 1e-3, 0.01, 2, C.byref(ms))
+    out["sgd"] = {"rc": rc, "ms_per_epoch": ms.value if rc == 0 else None,
+                  "nnz_per_s": n / (ms.value / 1000.0) if rc == 0 and ms.value > 0 else None, "epochs_timed": 2,
+                  "note": "refused by the harness when nnz % 32 == 0 (the reference kernel's endless loop)"}
+    print(json.dumps({"impl": "reference", "kind": "reference CUDA kernels on this GPU", "dtype": "f64",
+                      "config": {"workload": w.name, "dims": dims, "nnz_train": n, "rank": R},
+                      "ciss_build_s": ciss_s, "reference_cuda": out,
+                      "gpu": torch.cuda.get_device_name(local)}))
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.impl == "reference" and a.ref_cuda:
+        run_reference_cuda(a)
+    elif a.impl == "reference":
         run_reference(a)
     elif a.workload.startswith("batch"):
         run_batch_only(a)

@@ -35,7 +35,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "--ex
 
 HOST_SOURCES = ["host.cpp"]
 CUDA_SOURCES = ["engine.cu", "noalloc.cu", "fo.cu", "ciss_gpu.cu", "stage_gpu.cu"]
-HEADERS = ["ctc_internal.h", "kernels.cuh", "als_tc.cuh", "ptx.cuh", "runtime.cuh", "fo.cuh"]
+HEADERS = ["ctc_internal.h", "kernels.cuh", "als_tc.cuh", "ptx.cuh", "runtime.cuh", "fo.cuh", "stage_gpu.h"]
 
 
 def _newer(src_list, out):

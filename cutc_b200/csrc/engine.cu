@@ -18,6 +18,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <thread>
 #include <type_traits>
@@ -125,15 +126,30 @@ static int bits_for(uint64_t d)
 // coalesced.  Unused slot entries hold kPadKey, value 0 and residual 0.
 // The slots are gathered on the device from records in mode-m order
 // (rec, or rec through perm); the residual is formed on the device.
+// packed (mixed precision, FP32 only): the residual lives in the key word's
+// low rbits = min(32, 64 - key bits) bits (at least 16), so a slot entry is
+// 8 bytes instead of 12 and there is no residual array.
+static int ccdpp_packed_rbits(const uint64_t *dims)
+{
+    const int kb = bits_for(dims[0]) + bits_for(dims[1]) + bits_for(dims[2]);
+    return std::min(32, 64 - kb);
+}
+
 template <typename T>
 static void stage_keys(ctc_ctx *ctx, const DevTensor<T> &src, const uint32_t *perm, int m, const uint64_t *dims,
-                       const TilePlan &plan, int E, DevTensor<T> &d)
+                       const TilePlan &plan, int E, bool packed, DevTensor<T> &d)
 {
     const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
     const int b0 = bits_for(dims[m]), b1 = bits_for(dims[m1]), b2 = bits_for(dims[m2]);
     if (b0 + b1 + b2 > 64) fail(CTC_E_UNSUP, "CCD++ keys need %d bits (> 64) for these dimensions", b0 + b1 + b2);
-    d.ks.s_row = (uint32_t)(b1 + b2);
-    d.ks.s_q1 = (uint32_t)b2;
+    const int rb = packed ? ccdpp_packed_rbits(dims) : 0;
+    if (packed && (rb < 16 || sizeof(T) != 4))
+        fail(CTC_E_UNSUP, "mixed-precision CCD++ packs an FP32 residual of at least 16 bits beside the %d key bits",
+             b0 + b1 + b2);
+    d.ks.s_row = (uint32_t)(b1 + b2 + rb);
+    d.ks.s_q1 = (uint32_t)(b2 + rb);
+    d.ks.s_q2 = (uint32_t)rb;
+    d.ks.rbits = (uint32_t)rb;
     d.ks.m_q1 = (b1 == 64) ? ~0ull : ((1ull << b1) - 1);
     d.ks.m_q2 = (b2 == 64) ? ~0ull : ((1ull << b2) - 1);
     int eshift = 0;
@@ -146,7 +162,7 @@ static void stage_keys(ctc_ctx *ctx, const DevTensor<T> &src, const uint32_t *pe
     d.keys.alloc(nslots);
     d.x.alloc(nslots);
     dev_fill_slots<T>(ctx, src.rec.p, sizeof(T) == 8 ? src.v64.p : nullptr, perm, m, d.tiles.p, nslots, eshift,
-                      d.ks.s_row, d.ks.s_q1, d.keys.p, d.x.p);
+                      d.ks.s_row, d.ks.s_q1, d.ks.s_q2, d.keys.p, d.x.p);
     // warp tasks: a light tile, or up to kCcdppGroup consecutive pieces of a
     // long row; the long-row table becomes {row, first group, groups, 0}
     std::vector<int32_t> tasks;
@@ -174,8 +190,10 @@ static void stage_keys(ctc_ctx *ctx, const DevTensor<T> &src, const uint32_t *pe
     d.heavy.upload(reinterpret_cast<const uint4 *>(hv.data()), hv.size() / 4, ctx->stream);
     d.n = src.n;
     d.nslots = (uint32_t)nslots;
-    d.res.alloc(nslots);
-    CK(cudaMemsetAsync(d.res.p, 0, nslots * sizeof(T), ctx->stream));
+    if (!packed) {
+        d.res.alloc(nslots);
+        CK(cudaMemsetAsync(d.res.p, 0, nslots * sizeof(T), ctx->stream));
+    }
     CK(cudaStreamSynchronize(ctx->stream));
 }
 
@@ -430,7 +448,7 @@ static void stage_copies_dev(ctc_ctx *ctx, const ctc_params &p, uint32_t tl, con
         }
         if (ccdpp) {
             TracePhase tp("CCD++ slots");
-            stage_keys<T>(ctx, *src, pp, m, dims, plan, (int)(tl / 32), d);
+            stage_keys<T>(ctx, *src, pp, m, dims, plan, (int)(tl / 32), p.precision == CTC_PREC_MIXED, d);
             continue;
         }
         TracePhase tp("record copy");
@@ -607,6 +625,10 @@ struct Session : SessionBase {
         const int smem = ccdpp_smem_max();
         CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, true, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, false, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, true, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem));
+        CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, false, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem));
     }
 
     // shared memory per block of a CCD++ pass for staged factor columns: two
@@ -642,6 +664,39 @@ struct Session : SessionBase {
     // groups in flight (see ctc_params.sgd_conflicts)
     DevBuf<float> damp[3];
     bool damp_ready = false, damp_on = false;
+    // block-merged hot rows (sgd_atomic 3): slot codes per nonzero of copy 0
+    // and the rows of the slots, mode-major
+    DevBuf<uint32_t> hot_codes, hot_rows;
+    bool hot_ready = false;
+    void prepare_hot()
+    {
+        hot_ready = true;
+        const DevTensor<T> &c = D->copy[0];
+        std::vector<uint32_t> rows(3 * k::kSgdHot, 0u);
+        DevBuf<uint16_t> map[3];
+        for (int m = 0; m < 3; ++m) {
+            // the kSgdHot most frequent rows (ties: lower row first)
+            const auto &cnt = D->rowcnt[m];
+            std::vector<uint32_t> order(dims[m]);
+            std::iota(order.begin(), order.end(), 0u);
+            const size_t h = std::min<size_t>(k::kSgdHot, order.size());
+            auto count = [&](uint32_t r) -> uint32_t { return r < cnt.size() ? cnt[r] : 0u; };
+            std::partial_sort(order.begin(), order.begin() + h, order.end(), [&](uint32_t a, uint32_t b) {
+                return count(a) != count(b) ? count(a) > count(b) : a < b;
+            });
+            std::vector<uint16_t> mp(dims[m], (uint16_t)k::kSgdCold);
+            for (size_t s = 0; s < h; ++s) {
+                mp[order[s]] = (uint16_t)s;
+                rows[m * k::kSgdHot + s] = order[s];
+            }
+            map[m].upload(mp.data(), mp.size(), ctx->stream);
+        }
+        hot_rows.upload(rows.data(), rows.size(), ctx->stream);
+        hot_codes.alloc(c.n);
+        LAUNCH(ctx, k::k_sgd_hot_codes, grid_for(c.n, 256, kSMs * 16), 256, 0, (const uint4 *)c.rec.p, c.n,
+               (const uint16_t *)map[0].p, (const uint16_t *)map[1].p, (const uint16_t *)map[2].p, hot_codes.p);
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     unsigned sgd_grid(int gpb) const
     {
         const unsigned cap = p.sgd_groups > 0 ? (unsigned)std::max(1, p.sgd_groups / gpb) : kSMs * 8;
@@ -911,6 +966,17 @@ struct Session : SessionBase {
                     break;
                 }
         }
+        if constexpr (std::is_same<T, float>::value && (R / 4) % C == 0 && R / 4 / C <= 32) {
+            if (!seq && p.sgd_atomic == 3) {
+                // block-merged hot rows: 256 threads at most per block
+                const int blk = std::min(sgd_block(), 256);
+                const int gpb_h = (blk / 32) * (32 / (R / 4 / C));
+                LAUNCH(ctx, (k::k_sgd_hot<R, C>), sgd_grid(gpb_h), blk, 0, (const uint4 *)c.rec.p,
+                       (const uint32_t *)hot_codes.p, c.n, tile_len, c.ntiles, U[0].p, U[1].p, U[2].p,
+                       (const float *)lr_dev.p, (float)p.lambda, stride, d0, d1, d2, (const uint32_t *)hot_rows.p);
+                return;
+            }
+        }
         // bulk row reductions: two staged deltas of three rows per group
         const bool bulk = !seq && p.sgd_atomic == 2 && std::is_same<T, float>::value;
         const size_t smem = bulk ? (size_t)gpb * 2 * 3 * R * sizeof(T) : 0;
@@ -928,10 +994,14 @@ struct Session : SessionBase {
                    (const T *)U[m].p, Urow[m].p, dims[m], R);
         for (int m = 0; m < 3; ++m) {
             DevTensor<T> &c = D->copy[m];
-            LAUNCH(ctx, k::k_ccdpp_init<T, R>, grid_for(c.nslots, 256, kSMs * 16), 256, 0,
-                   (const uint64_t *)c.keys.p, (const T *)c.x.p, c.res.p, c.nslots, c.ks, m, (const T *)Urow[0].p,
-                   (const T *)Urow[1].p,
-                   (const T *)Urow[2].p);
+            if (c.ks.rbits)
+                LAUNCH(ctx, (k::k_ccdpp_init<T, R, true>), grid_for(c.nslots, 256, kSMs * 16), 256, 0, c.keys.p,
+                       (const T *)c.x.p, c.res.p, c.nslots, c.ks, m, (const T *)Urow[0].p, (const T *)Urow[1].p,
+                       (const T *)Urow[2].p);
+            else
+                LAUNCH(ctx, (k::k_ccdpp_init<T, R, false>), grid_for(c.nslots, 256, kSMs * 16), 256, 0, c.keys.p,
+                       (const T *)c.x.p, c.res.p, c.nslots, c.ks, m, (const T *)Urow[0].p, (const T *)Urow[1].p,
+                       (const T *)Urow[2].p);
         }
     }
 
@@ -961,13 +1031,23 @@ struct Session : SessionBase {
         }
         const size_t smem = (cols.stage[0] ? need[0] : 0) + (cols.stage[1] ? need[1] : 0);
         const unsigned g = grid_for((uint64_t)c.ntasks, 16, kSMs * 2);
-        if (first)
-            LAUNCH(ctx, k::k_ccdpp_pass<T, true, E>, g, 512, smem, (const int4 *)c.tasks.p, c.ntasks,
-                   (const uint64_t *)c.keys.p, c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p,
-                   (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p);
+        if (c.ks.rbits)
+            ccdpp_launch<E, true>(c, first, g, smem, cols, out, m);
         else
-            LAUNCH(ctx, k::k_ccdpp_pass<T, false, E>, g, 512, smem, (const int4 *)c.tasks.p, c.ntasks,
-                   (const uint64_t *)c.keys.p, c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p,
+            ccdpp_launch<E, false>(c, first, g, smem, cols, out, m);
+    }
+
+    template <int E, bool PK>
+    void ccdpp_launch(DevTensor<T> &c, bool first, unsigned g, size_t smem, const k::CcdppCols<T> &cols, T *out,
+                      int m)
+    {
+        if (first)
+            LAUNCH(ctx, (k::k_ccdpp_pass<T, true, E, PK>), g, 512, smem, (const int4 *)c.tasks.p, c.ntasks, c.keys.p,
+                   c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p, (const uint4 *)c.heavy.p,
+                   hcnt[m].p, dev_err.p);
+        else
+            LAUNCH(ctx, (k::k_ccdpp_pass<T, false, E, PK>), g, 512, smem, (const int4 *)c.tasks.p, c.ntasks,
+                   c.keys.p, c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p,
                    (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p);
     }
 
@@ -1003,9 +1083,15 @@ struct Session : SessionBase {
         for (int m = 0; m < 3; ++m) {
             DevTensor<T> &c = D->copy[m];
             const unsigned g = grid_for(c.nslots, 256, kMaxPartials);
-            LAUNCH(ctx, k::k_ccdpp_finish<T>, g, 256, 0, (const uint64_t *)c.keys.p, c.res.p, c.nslots, c.ks, m,
-                   (const T *)(U[0].p + (size_t)(R - 1) * dims[0]), (const T *)(U[1].p + (size_t)(R - 1) * dims[1]),
-                   (const T *)(U[2].p + (size_t)(R - 1) * dims[2]), m == 0 ? ctx->partial.p : (double *)nullptr);
+            const T *c0 = U[0].p + (size_t)(R - 1) * dims[0], *c1 = U[1].p + (size_t)(R - 1) * dims[1],
+                    *c2 = U[2].p + (size_t)(R - 1) * dims[2];
+            double *part = m == 0 ? ctx->partial.p : (double *)nullptr;
+            if (c.ks.rbits)
+                LAUNCH(ctx, (k::k_ccdpp_finish<T, true>), g, 256, 0, c.keys.p, c.res.p, c.nslots, c.ks, m, c0, c1, c2,
+                       part);
+            else
+                LAUNCH(ctx, (k::k_ccdpp_finish<T, false>), g, 256, 0, c.keys.p, c.res.p, c.nslots, c.ks, m, c0, c1,
+                       c2, part);
             if (m == 0)
                 LAUNCH(ctx, k::k_sum_partials, 1, 256, 0, (const double *)ctx->partial.p, (int)g, ctx->scalars.p + 0);
         }
@@ -1025,6 +1111,9 @@ struct Session : SessionBase {
     {
         if (!model_set) fail(CTC_E_ARG, "no model staged on the dataset");
         if (p.alg == CTC_ALG_SGD && !damp_ready) prepare_damping(sgd_groups_per_block());
+        if constexpr (std::is_same<T, float>::value)
+            if (p.alg == CTC_ALG_SGD && p.sgd_atomic == 3 && p.sgd_order != CTC_SGD_SEQUENTIAL && !hot_ready)
+                prepare_hot();
         const bool use_graph = p.use_graph && !ctx->kt.on && p.sgd_order != CTC_SGD_SEQUENTIAL;
         for (int i = 0; i < n; ++i) {
             if (!use_graph) {
@@ -1087,7 +1176,14 @@ struct Session : SessionBase {
         check_errors();
         const T *Urm[3];
         row_factors(Urm);
-        if (colmajor) {
+        if (colmajor && D->copy[0].ks.rbits) {
+            // packed slots of copy 0 hold r = x - model in the key words
+            const DevTensor<T> &c = D->copy[0];
+            const unsigned g = grid_for(c.nslots, 256, kMaxPartials);
+            LAUNCH(ctx, k::k_ccdpp_res_sumsq, g, 256, 0, (const uint64_t *)c.keys.p, c.nslots, c.ks.rbits,
+                   ctx->partial.p);
+            LAUNCH(ctx, k::k_sum_partials, 1, 256, 0, (const double *)ctx->partial.p, (int)g, ctx->scalars.p + 0);
+        } else if (colmajor) {
             // copy 0 holds r = x - model: its SSE is the sum of squares
             sumsq_into(D->copy[0].res.p, D->copy[0].nslots, 0);
         } else {
@@ -1211,13 +1307,18 @@ static void check_params(const ctc_params *p)
     if (p->alg < CTC_ALG_ALS || p->alg > CTC_ALG_CCDPP) fail(CTC_E_ARG, "unknown algorithm %d", p->alg);
     if (p->precision != CTC_PREC_F32 && p->precision != CTC_PREC_F64 && p->precision != CTC_PREC_MIXED)
         fail(CTC_E_ARG, "unknown precision %d", p->precision);
-    if (p->precision == CTC_PREC_MIXED && !(p->alg == CTC_ALG_ALS && (p->rank == 64 || p->rank == 32)))
-        fail(CTC_E_UNSUP, "mixed precision (BF16 tensor-core Gram) is available for ALS at ranks 32 and 64");
+    if (p->precision == CTC_PREC_MIXED && !(p->alg == CTC_ALG_ALS && (p->rank == 64 || p->rank == 32)) &&
+        p->alg != CTC_ALG_CCDPP)
+        fail(CTC_E_UNSUP, "mixed precision is available for ALS at ranks 32 and 64 (BF16 tensor-core Gram) and for "
+                          "CCD++ (packed residual slots)");
     if (p->rank != 8 && p->rank != 16 && p->rank != 32 && p->rank != 64)
         fail(CTC_E_UNSUP, "rank %d not supported (8, 16, 32, 64)", p->rank);
     if (p->tile_len < 0 || p->tile_len > (1 << 20)) fail(CTC_E_ARG, "tile_len %d", p->tile_len);
     if (p->iters < 0) fail(CTC_E_ARG, "iters %d", p->iters);
     if (p->mode_start < 0 || p->mode_start > 2) fail(CTC_E_ARG, "mode_start %d", p->mode_start);
+    if (p->sgd_atomic < 0 || p->sgd_atomic > 3) fail(CTC_E_ARG, "sgd_atomic %d (0 to 3)", p->sgd_atomic);
+    if (p->alg == CTC_ALG_SGD && p->sgd_atomic == 3 && p->precision == CTC_PREC_F64)
+        fail(CTC_E_UNSUP, "sgd_atomic 3 (block-merged hot rows) is FP32 only");
     const int tpb = p->threads_per_block;
     if (tpb < 0 || (tpb & (tpb - 1)) != 0 || tpb > 512)
         fail(CTC_E_ARG, "threads_per_block %d: 0 or a power of two up to 512", tpb);

@@ -123,6 +123,11 @@ __device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const 
     const int lane = threadIdx.x & 31;
     const int gl = lane % GL, gw = lane / GL;
     double acc = 0;
+    // group gw takes the GL consecutive records gw*GL .. gw*GL+GL-1 of the
+    // 32, so in a mode-0-sorted copy it mostly sees one mode-0 row: that
+    // row's slice stays in registers until the index changes
+    uint32_t cur0 = 0xffffffffu;
+    V va{};
     for (uint64_t base = first; base < end; base += stride) {
         const uint64_t mine = base + lane;
         uint4 r = make_uint4(0u, 0u, 0u, 0u);  // row 0 for the tail: in bounds, result unused
@@ -134,12 +139,15 @@ __device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const 
         const uint64_t cnt = end - base;
 #pragma unroll 4
         for (int j = 0; j < GL; ++j) {
-            const int src = j * GPW + gw;
+            const int src = gw * GL + j;
             const uint32_t i0 = __shfl_sync(0xffffffffu, r.x, src);
             const uint32_t i1 = __shfl_sync(0xffffffffu, r.y, src);
             const uint32_t i2 = __shfl_sync(0xffffffffu, r.z, src);
             const T xv = __shfl_sync(0xffffffffu, x, src);
-            const V va = reinterpret_cast<const V *>(U0 + (size_t)i0 * R)[gl];
+            if (i0 != cur0) {
+                va = reinterpret_cast<const V *>(U0 + (size_t)i0 * R)[gl];
+                cur0 = i0;
+            }
             const V vb = reinterpret_cast<const V *>(U1 + (size_t)i1 * R)[gl];
             const V vc = reinterpret_cast<const V *>(U2 + (size_t)i2 * R)[gl];
             T p = 0;
@@ -415,6 +423,158 @@ __global__ void __launch_bounds__(512) k_sgd(const uint4 *__restrict__ rec,
 }
 
 // ---------------------------------------------------------------------
+// Hogwild SGD with block-merged updates of the hot rows (FP32,
+// sgd_atomic 3).  The most frequent kSgdHot rows of each mode are "hot";
+// hot[p] codes the hot slots of nonzero p's three rows (10 bits per mode,
+// kSgdCold when the row is not hot).  The block's groups advance in
+// lockstep, one nonzero each per step: every group reads its three rows
+// from global memory, adds the deltas of cold rows with vector atomics
+// as k_sgd does, and adds the deltas of hot rows into the block's
+// shared-memory accumulators; after the step the block adds each touched
+// hot row's summed delta with one vector atomic per 16 bytes and clears
+// it.  The nonzeros of one block step are thus applied as simultaneous
+// Hogwild updates (each computed from the rows it read, their sum added),
+// and a hot row receives one reduction per block step instead of one per
+// nonzero: the same-address reductions queued at the L2 slice that holds
+// it, behind which its readers wait, shrink by the number of the block's
+// nonzeros that touch it.
+// ---------------------------------------------------------------------
+constexpr int kSgdHot = 32;          // hot rows per mode
+constexpr uint32_t kSgdCold = 1023u; // slot code of a row that is not hot
+
+template <int R, int C>
+__global__ void __launch_bounds__(256) k_sgd_hot(const uint4 *__restrict__ rec, const uint32_t *__restrict__ hot,
+                                                 uint32_t n, uint32_t tile_len, uint32_t ntiles, float *U0,
+                                                 float *U1, float *U2, const float *__restrict__ lr_dev, float lambda,
+                                                 uint64_t tile_stride, const float *__restrict__ damp0,
+                                                 const float *__restrict__ damp1, const float *__restrict__ damp2,
+                                                 const uint32_t *__restrict__ hot_rows)
+{
+    constexpr int VN = 4;
+    constexpr int G = R / (VN * C);
+    static_assert(G >= 1 && G <= 32 && (32 % G) == 0 && G * VN * C == R, "unsupported rank / lanes");
+    constexpr int GPW = 32 / G;
+    constexpr int NV = R / VN;  // float4 per row
+    __shared__ __align__(16) float4 acc[3 * kSgdHot * NV];
+    __shared__ uint32_t touched[3];  // bit s of word m: slot s of mode m got a delta this step
+    __shared__ uint32_t hrow[3 * kSgdHot];
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;
+    const int gw = lane / G;
+    for (int i = threadIdx.x; i < 3 * kSgdHot * NV; i += blockDim.x) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = threadIdx.x; i < 3 * kSgdHot; i += blockDim.x) hrow[i] = hot_rows[i];
+    if (threadIdx.x < 3) touched[threadIdx.x] = 0u;
+    __syncthreads();
+    const uint64_t ngb = (uint64_t)(blockDim.x >> 5) * GPW;  // groups per block
+    const uint64_t group = blockIdx.x * ngb + (uint64_t)(threadIdx.x >> 5) * GPW + gw;
+    const uint64_t ngroups = (uint64_t)gridDim.x * ngb;
+    const uint64_t rounds = (ntiles + ngroups - 1) / ngroups;
+    const float s = *lr_dev;
+    for (uint64_t k = 0; k < rounds; ++k) {
+        const uint64_t t = group + k * ngroups;
+        const bool has_tile = t < ntiles;
+        const uint64_t tile = has_tile ? (t * tile_stride) % ntiles : 0;
+        const uint64_t start = tile * tile_len;
+        const uint64_t end = has_tile ? min(start + tile_len, (uint64_t)n) : start;
+        // every group of the block takes tile_len steps per round
+        for (uint32_t step = 0; step < tile_len; ++step) {
+            const uint64_t p = start + step;
+            if (p < end) {
+                const uint4 r = rec[p];
+                const uint32_t hc = hot[p];
+                const float x = __uint_as_float(r.w);
+                float4 *arow = reinterpret_cast<float4 *>(U0 + (size_t)r.x * R) + gl * C;
+                float4 *brow = reinterpret_cast<float4 *>(U1 + (size_t)r.y * R) + gl * C;
+                float4 *crow = reinterpret_cast<float4 *>(U2 + (size_t)r.z * R) + gl * C;
+                float4 a[C], b[C], c[C];
+#pragma unroll
+                for (int q = 0; q < C; ++q) {
+                    a[q] = __ldcg(arow + q);
+                    b[q] = __ldcg(brow + q);
+                    c[q] = __ldcg(crow + q);
+                }
+                float part = 0;
+#pragma unroll
+                for (int q = 0; q < C; ++q)
+                    part += a[q].x * b[q].x * c[q].x + a[q].y * b[q].y * c[q].y + a[q].z * b[q].z * c[q].z +
+                            a[q].w * b[q].w * c[q].w;
+                const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (gw * G));
+#pragma unroll
+                for (int o = G / 2; o > 0; o >>= 1) part += __shfl_xor_sync(gmask, part, o);
+                const float e = x - part;
+                float sa = s, sb = s, sc = s;
+                if (damp0) {
+                    sa *= damp0[r.x];
+                    sb *= damp1[r.y];
+                    sc *= damp2[r.z];
+                }
+                const uint32_t slot[3] = {hc & 1023u, (hc >> 10) & 1023u, (hc >> 20) & 1023u};
+                float4 *row[3] = {arow, brow, crow};
+#pragma unroll
+                for (int q = 0; q < C; ++q) {
+                    float4 d[3];
+                    d[0] = make_float4(sa * (e * b[q].x * c[q].x - lambda * a[q].x),
+                                       sa * (e * b[q].y * c[q].y - lambda * a[q].y),
+                                       sa * (e * b[q].z * c[q].z - lambda * a[q].z),
+                                       sa * (e * b[q].w * c[q].w - lambda * a[q].w));
+                    d[1] = make_float4(sb * (e * a[q].x * c[q].x - lambda * b[q].x),
+                                       sb * (e * a[q].y * c[q].y - lambda * b[q].y),
+                                       sb * (e * a[q].z * c[q].z - lambda * b[q].z),
+                                       sb * (e * a[q].w * c[q].w - lambda * b[q].w));
+                    d[2] = make_float4(sc * (e * b[q].x * a[q].x - lambda * c[q].x),
+                                       sc * (e * b[q].y * a[q].y - lambda * c[q].y),
+                                       sc * (e * b[q].z * a[q].z - lambda * c[q].z),
+                                       sc * (e * b[q].w * a[q].w - lambda * c[q].w));
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) {
+                        if (slot[m] == kSgdCold) {
+                            vatomic_add(row[m] + q, d[m]);
+                        } else {
+                            float *ac = reinterpret_cast<float *>(&acc[(m * kSgdHot + slot[m]) * NV + gl * C + q]);
+                            atomicAdd(ac + 0, d[m].x);
+                            atomicAdd(ac + 1, d[m].y);
+                            atomicAdd(ac + 2, d[m].z);
+                            atomicAdd(ac + 3, d[m].w);
+                        }
+                    }
+                }
+                if (gl == 0)
+#pragma unroll
+                    for (int m = 0; m < 3; ++m)
+                        if (slot[m] != kSgdCold) atomicOr(&touched[m], 1u << slot[m]);
+            }
+            __syncthreads();
+            // one vector atomic per 16 bytes of every touched hot row
+            for (int i = threadIdx.x; i < 3 * kSgdHot * NV; i += blockDim.x) {
+                const int m = i / (kSgdHot * NV), sl = (i / NV) % kSgdHot, v = i % NV;
+                if ((touched[m] >> sl) & 1u) {
+                    const float4 d = acc[i];
+                    acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    float *um = m == 0 ? U0 : (m == 1 ? U1 : U2);
+                    vatomic_add(reinterpret_cast<float4 *>(um + (size_t)hrow[m * kSgdHot + sl] * R) + v, d);
+                }
+            }
+            __syncthreads();
+            // cleared before any thread can mark a slot in the next step
+            if (threadIdx.x < 3) touched[threadIdx.x] = 0u;
+            __syncthreads();
+        }
+    }
+}
+
+// hot[p] = the three hot-slot codes of nonzero p (k_sgd_hot), from per-mode
+// row -> slot maps (kSgdCold for rows that are not hot)
+static __global__ void k_sgd_hot_codes(const uint4 *__restrict__ rec, uint32_t n, const uint16_t *__restrict__ map0,
+                                       const uint16_t *__restrict__ map1, const uint16_t *__restrict__ map2,
+                                       uint32_t *__restrict__ hot)
+{
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint4 r = rec[p];
+        hot[p] = (uint32_t)map0[r.x] | ((uint32_t)map1[r.y] << 10) | ((uint32_t)map2[r.z] << 20);
+    }
+}
+
+// ---------------------------------------------------------------------
 // CCD++ (rank-one column updates).  Each mode copy of the training tensor
 // is kept as packed 64-bit keys (row | q1 | q2, the row index of the copy's
 // mode and the indices of the next two modes) plus a separate residual
@@ -437,7 +597,9 @@ __global__ void __launch_bounds__(512) k_sgd(const uint4 *__restrict__ rec,
 // ---------------------------------------------------------------------
 struct KeyShape {
     uint32_t s_row, s_q1;   // key >> s_row = row ; (key >> s_q1) & m_q1 = q1
-    uint64_t m_q1, m_q2;    // key & m_q2 = q2
+    uint64_t m_q1, m_q2;    // (key >> s_q2) & m_q2 = q2
+    uint32_t s_q2;          // 0, or rbits when the residual is packed below the key
+    uint32_t rbits;         // packed form: residual bits in the low end of the word
 };
 
 __device__ __forceinline__ void unpack_key(uint64_t k, const KeyShape &ks, uint32_t &row, uint32_t &q1,
@@ -445,7 +607,27 @@ __device__ __forceinline__ void unpack_key(uint64_t k, const KeyShape &ks, uint3
 {
     row = (uint32_t)(k >> ks.s_row);
     q1 = (uint32_t)((k >> ks.s_q1) & ks.m_q1);
-    q2 = (uint32_t)(k & ks.m_q2);
+    q2 = (uint32_t)((k >> ks.s_q2) & ks.m_q2);
+}
+
+// Packed CCD++ slots (mixed precision): the residual lives in the low
+// rbits (16..32) of the key word, as an FP32 value with its low 32 - rbits
+// mantissa bits rounded off (round to nearest even): sign, the full 8-bit
+// exponent and rbits - 9 mantissa bits.  A finite residual never encodes
+// as all ones, so a real entry never equals kPadKey.
+__device__ __forceinline__ float packed_res(uint64_t k, uint32_t rbits)
+{
+    const uint32_t field = (uint32_t)(k & ((1ull << rbits) - 1ull));
+    return __uint_as_float(field << (32u - rbits));
+}
+
+__device__ __forceinline__ uint64_t with_res(uint64_t k, float r, uint32_t rbits)
+{
+    uint32_t b = __float_as_uint(r);
+    const uint32_t d = 32u - rbits;
+    if (d) b = (b + ((1u << (d - 1u)) - 1u) + ((b >> d) & 1u)) >> d;
+    const uint64_t mask = (1ull << rbits) - 1ull;
+    return (k & ~mask) | ((uint64_t)b & mask);
 }
 
 template <typename T>
@@ -470,25 +652,36 @@ constexpr uint64_t kPadKey = ~0ull;
 // pieces of a long row one warp task covers (one slot partial per group)
 constexpr int kCcdppGroup = 8;
 
-template <typename T, int E>
+template <typename T, int E, bool PK>
 __device__ __forceinline__ void ccdpp_load_slot(const uint64_t *__restrict__ keys, const T *__restrict__ res,
-                                                uint64_t base, int lane, uint64_t (&kv)[E], T (&rv)[E])
+                                                uint64_t base, int lane, uint32_t rbits, uint64_t (&kv)[E],
+                                                T (&rv)[E])
 {
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         kv[e] = __ldcs(keys + base + 32u * e + lane);
-        rv[e] = __ldcs(res + base + 32u * e + lane);
+        if constexpr (PK) rv[e] = (T)packed_res(kv[e], rbits);
+        else rv[e] = __ldcs(res + base + 32u * e + lane);
     }
 }
 
-// FIRST: the refreshed residuals of the lane's valid entries back
-template <typename T, int E>
-__device__ __forceinline__ void ccdpp_store_slot(T *__restrict__ res, uint64_t base, int lane, int cnt,
-                                                 const T (&rv)[E])
+// FIRST: the refreshed residual of one entry back (into its key word when
+// packed)
+template <typename T, bool PK>
+__device__ __forceinline__ void ccdpp_store_res(uint64_t *keys, T *res, uint64_t at, uint64_t k, T r,
+                                                uint32_t rbits)
+{
+    if constexpr (PK) keys[at] = with_res(k, (float)r, rbits);
+    else res[at] = r;
+}
+
+template <typename T, int E, bool PK>
+__device__ __forceinline__ void ccdpp_store_slot(uint64_t *keys, T *res, uint64_t base, int lane, int cnt,
+                                                 const uint64_t (&kv)[E], const T (&rv)[E], uint32_t rbits)
 {
 #pragma unroll
     for (int e = 0; e < E; ++e)
-        if (e < cnt) res[base + 32u * e + lane] = rv[e];
+        if (e < cnt) ccdpp_store_res<T, PK>(keys, res, base + 32u * e + lane, kv[e], rv[e], rbits);
 }
 
 // The two gathered modes of a pass.  Non-FIRST passes read column f of each
@@ -520,9 +713,10 @@ __device__ __forceinline__ uint32_t ccdpp_stage_span(const CcdppCols<T> &c, int 
     }
 }
 
-template <typename T, bool FIRST, int E>
+// PK: packed slots (residual in the key word, no residual array).
+template <typename T, bool FIRST, int E, bool PK = false>
 __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ tasks, uint32_t ntasks,
-                                                       const uint64_t *__restrict__ keys, T *__restrict__ res,
+                                                       uint64_t *__restrict__ keys, T *__restrict__ res,
                                                        KeyShape ks, Pack3<T> *pkm, CcdppCols<T> cols, T *out,
                                                        T lambda, T *__restrict__ slot_nu, T *__restrict__ slot_de,
                                                        const uint4 *__restrict__ heavy, unsigned int *hcnt, int *err)
@@ -597,7 +791,7 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
             T nu = 0, de = 0;
             for (int j = 0; j < td.y; ++j) {
                 const uint64_t base = (uint64_t)(td.x + j) * (uint64_t)(32 * E);
-                ccdpp_load_slot<T, E>(keys, res, base, lane, kv, rv);
+                ccdpp_load_slot<T, E, PK>(keys, res, base, lane, ks.rbits, kv, rv);
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
                     if (kv[e] != kPadKey) {
@@ -620,7 +814,8 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
                 if constexpr (FIRST) {
 #pragma unroll
                     for (int e = 0; e < E; ++e)
-                        if (kv[e] != kPadKey) res[base + 32u * e + lane] = rv[e];
+                        if (kv[e] != kPadKey)
+                            ccdpp_store_res<T, PK>(keys, res, base + 32u * e + lane, kv[e], rv[e], ks.rbits);
                 }
             }
 #pragma unroll
@@ -658,7 +853,7 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
         const uint64_t base = (uint64_t)td.x * (uint64_t)(32 * E);
         // valid entries of this lane: the tile's positions lane*E .. +E-1
         const int cnt = max(0, min(E, td.y - lane * E));
-        ccdpp_load_slot<T, E>(keys, res, base, lane, kv, rv);
+        ccdpp_load_slot<T, E, PK>(keys, res, base, lane, ks.rbits, kv, rv);
         // light tile: runs of equal rows inside the lane, then one segmented
         // warp scan joins the runs that cross lanes
         uint32_t hk = kNone, tk = kNone;
@@ -697,7 +892,7 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
                 tdd += h * h;
             }
         }
-        if constexpr (FIRST) ccdpp_store_slot<T, E>(res, base, lane, cnt, rv);
+        if constexpr (FIRST) ccdpp_store_slot<T, E, PK>(keys, res, base, lane, cnt, kv, rv, ks.rbits);
         const uint32_t in_key = nruns >= 2 ? hk : tk;
         const uint32_t out_key = tk;
         uint32_t prev_out = __shfl_up_sync(0xffffffffu, out_key, 1);
@@ -784,8 +979,8 @@ __device__ __forceinline__ void key_modes(uint64_t k, const KeyShape &ks, int m,
 // walks them with groups of R / VN lanes per slot, lane gl reading the
 // 16-byte slice gl of each row (whole rows per warp load), and a butterfly
 // sum; unused slot entries (kPadKey) keep their zero residual.
-template <typename T, int R>
-__global__ void __launch_bounds__(256) k_ccdpp_init(const uint64_t *__restrict__ keys, const T *__restrict__ x,
+template <typename T, int R, bool PK = false>
+__global__ void __launch_bounds__(256) k_ccdpp_init(uint64_t *__restrict__ keys, const T *__restrict__ x,
                                                     T *__restrict__ res, uint32_t n, KeyShape ks, int m,
                                                     const T *__restrict__ U0, const T *__restrict__ U1,
                                                     const T *__restrict__ U2)
@@ -823,15 +1018,15 @@ __global__ void __launch_bounds__(256) k_ccdpp_init(const uint64_t *__restrict__
             for (int v = 0; v < VN; ++v) p += vget(va, v) * vget(vb, v) * vget(vc, v);
 #pragma unroll
             for (int o = GL / 2; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
-            if (real && gl == 0) res[base + src] = xs - p;
+            if (real && gl == 0) ccdpp_store_res<T, PK>(keys, res, base + src, k, xs - p, ks.rbits);
         }
     }
 }
 
 // res -= U0(i0,c) U1(i1,c) U2(i2,c) for one column c (column-major
 // pointers); optional SSE partials of the new residual.
-template <typename T>
-__global__ void __launch_bounds__(256) k_ccdpp_finish(const uint64_t *__restrict__ keys, T *__restrict__ res,
+template <typename T, bool PK = false>
+__global__ void __launch_bounds__(256) k_ccdpp_finish(uint64_t *__restrict__ keys, T *__restrict__ res,
                                                       uint32_t n, KeyShape ks, int m, const T *__restrict__ c0,
                                                       const T *__restrict__ c1, const T *__restrict__ c2,
                                                       double *__restrict__ partial)
@@ -842,14 +1037,32 @@ __global__ void __launch_bounds__(256) k_ccdpp_finish(const uint64_t *__restrict
         if (key == kPadKey) continue;
         uint32_t idx[3];
         key_modes(key, ks, m, idx);
-        const T r = res[p] - c0[idx[0]] * c1[idx[1]] * c2[idx[2]];
-        res[p] = r;
-        acc += (double)r * (double)r;
+        const T r0 = PK ? (T)packed_res(key, ks.rbits) : res[p];
+        const T r = r0 - c0[idx[0]] * c1[idx[1]] * c2[idx[2]];
+        ccdpp_store_res<T, PK>(keys, res, p, key, r, ks.rbits);
+        // the SSE of the residual as stored
+        const T rs = PK ? (T)packed_res(with_res(key, (float)r, ks.rbits), ks.rbits) : r;
+        acc += (double)rs * (double)rs;
     }
     if (partial) {
         acc = block_sum(acc);
         if (threadIdx.x == 0) partial[blockIdx.x] = acc;
     }
+}
+
+// Sum of squares of the residuals held in packed slots (pads skipped).
+static __global__ void __launch_bounds__(256) k_ccdpp_res_sumsq(const uint64_t *__restrict__ keys, uint32_t n,
+                                                                uint32_t rbits, double *__restrict__ partial)
+{
+    double acc = 0;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[p];
+        if (key == kPadKey) continue;
+        const double r = (double)packed_res(key, rbits);
+        acc += r * r;
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
 
 // column-major (R x d) -> row-major (d x R)

@@ -51,8 +51,8 @@ static __global__ void k_rows_in_order(const uint4 *__restrict__ rec, const uint
 template <typename T>
 __global__ void k_fill_slots(const uint4 *__restrict__ rec, const double *__restrict__ v64,
                              const uint32_t *__restrict__ perm, int m, const int4 *__restrict__ tiles,
-                             uint64_t nslots, int eshift, uint32_t s_row, uint32_t s_q1, uint64_t *__restrict__ keys,
-                             T *__restrict__ x)
+                             uint64_t nslots, int eshift, uint32_t s_row, uint32_t s_q1, uint32_t s_q2,
+                             uint64_t *__restrict__ keys, T *__restrict__ x)
 {
     const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
     const int sshift = 5 + eshift;
@@ -68,7 +68,8 @@ __global__ void k_fill_slots(const uint4 *__restrict__ rec, const double *__rest
             const uint32_t p = (uint32_t)t.x + q;
             const uint32_t j = perm ? perm[p] : p;
             const uint4 r = rec[j];
-            key = ((uint64_t)field(r, m) << s_row) | ((uint64_t)field(r, m1) << s_q1) | field(r, m2);
+            key = ((uint64_t)field(r, m) << s_row) | ((uint64_t)field(r, m1) << s_q1) |
+                  ((uint64_t)field(r, m2) << s_q2);
             if constexpr (sizeof(T) == 8) v = v64[j];
             else v = __uint_as_float(r.w);
         }
@@ -187,15 +188,16 @@ bool dev_row_runs(ctc_ctx *ctx, const uint4 *rec, const uint32_t *perm, uint32_t
 
 template <typename T>
 void dev_fill_slots(ctc_ctx *ctx, const uint4 *rec, const double *v64, const uint32_t *perm, int m,
-                    const int4 *tiles, uint64_t nslots, int eshift, uint32_t s_row, uint32_t s_q1, uint64_t *keys, T *x)
+                    const int4 *tiles, uint64_t nslots, int eshift, uint32_t s_row, uint32_t s_q1, uint32_t s_q2,
+                    uint64_t *keys, T *x)
 {
     LAUNCH(ctx, sg::k_fill_slots<T>, grid_for(nslots, 256, kSMs * 16), 256, 0, rec, v64, perm, m, tiles, nslots,
-           eshift, s_row, s_q1, keys, x);
+           eshift, s_row, s_q1, s_q2, keys, x);
 }
 template void dev_fill_slots<float>(ctc_ctx *, const uint4 *, const double *, const uint32_t *, int, const int4 *,
-                                    uint64_t, int, uint32_t, uint32_t, uint64_t *, float *);
+                                    uint64_t, int, uint32_t, uint32_t, uint32_t, uint64_t *, float *);
 template void dev_fill_slots<double>(ctc_ctx *, const uint4 *, const double *, const uint32_t *, int, const int4 *,
-                                     uint64_t, int, uint32_t, uint32_t, uint64_t *, double *);
+                                     uint64_t, int, uint32_t, uint32_t, uint32_t, uint64_t *, double *);
 
 void dev_gather_records(ctc_ctx *ctx, const uint4 *rec, const double *v64, const uint32_t *perm, uint32_t n,
                         uint4 *out, double *v64_out)

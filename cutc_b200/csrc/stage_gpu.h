@@ -29,12 +29,13 @@ bool dev_row_runs(ctc_ctx *ctx, const uint4 *rec, const uint32_t *perm, uint32_t
                   std::vector<uint32_t> &rows, std::vector<uint32_t> &counts);
 
 // CCD++ slots of the tile plan `tiles` ({start, len, heavy, piece}, slot
-// length 32 << eshift): key (row | q1 | q2 packed with shifts s_row, s_q1)
-// and value of entry lane * E + step of each tile, pads kPadKey / 0.
+// length 32 << eshift): key (row | q1 | q2 packed with shifts s_row, s_q1,
+// s_q2; the bits below s_q2 zero) and value of entry lane * E + step of
+// each tile, pads kPadKey / 0.
 template <typename T>
 void dev_fill_slots(ctc_ctx *ctx, const uint4 *rec, const double *v64, const uint32_t *perm, int m,
-                    const int4 *tiles, uint64_t nslots, int eshift, uint32_t s_row, uint32_t s_q1, uint64_t *keys,
-                    T *x);
+                    const int4 *tiles, uint64_t nslots, int eshift, uint32_t s_row, uint32_t s_q1, uint32_t s_q2,
+                    uint64_t *keys, T *x);
 
 // out[i] = rec[perm[i]] (and the FP64 values when v64 is given)
 void dev_gather_records(ctc_ctx *ctx, const uint4 *rec, const double *v64, const uint32_t *perm, uint32_t n,

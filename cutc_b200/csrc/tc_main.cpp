@@ -27,7 +27,9 @@ static void usage()
             "  --iters N                 epochs (default 1000)\n"
             "  --inner K                 CCD++ inner sweeps (default 1)\n"
             "  --tile-len T              nonzeros per warp work unit (default tuned)\n"
-            "  --precision f32|f64       (default f32)\n"
+            "  --precision f32|f64|mixed (default f32; mixed: ALS tensor-core Gram at rank 32/64,\n"
+            "                            CCD++ packed residual slots)\n"
+            "  --threads-per-block B     SGD block size, 32..512 (default 256)\n"
             "  --compat                  reference kernel semantics\n"
             "  --no-early-stop           run all epochs\n"
             "  --seed S                  factor initialisation seed (default 0)\n"
@@ -62,7 +64,7 @@ int main(int argc, char **argv)
         return 2;
     }
     int alg = CTC_ALG_SGD, rank = 16, iters = -1, inner = -1, tile = 0, prec = CTC_PREC_F32, compat = 0;
-    int early = 1, device = 0;
+    int early = 1, device = 0, tpb = 0;
     double lambda = NAN, lr = NAN, lr_scale = NAN, decay = NAN;
     unsigned long long seed = 0;
     const char *load_path = nullptr, *save_path = nullptr, *factors_prefix = nullptr;
@@ -91,7 +93,14 @@ int main(int argc, char **argv)
         else if (a == "--iters") iters = atoi(next());
         else if (a == "--inner") inner = atoi(next());
         else if (a == "--tile-len") tile = atoi(next());
-        else if (a == "--precision") prec = std::string(next()) == "f64" ? CTC_PREC_F64 : CTC_PREC_F32;
+        else if (a == "--precision") {
+            const std::string v = next();
+            prec = v == "f64" ? CTC_PREC_F64 : v == "mixed" ? CTC_PREC_MIXED : v == "f32" ? CTC_PREC_F32 : -1;
+            if (prec < 0) {
+                usage();
+                return 2;
+            }
+        } else if (a == "--threads-per-block") tpb = atoi(next());
         else if (a == "--compat") compat = 1;
         else if (a == "--no-early-stop") early = 0;
         else if (a == "--seed") seed = strtoull(next(), nullptr, 10);
@@ -133,6 +142,8 @@ int main(int argc, char **argv)
     p.precision = prec;
     p.compat = compat;
     p.early_stop = early;
+    p.threads_per_block = tpb;
+    check(ctc_params_check(&p), "parameters");
     ctc_ctx *ctx = nullptr;
     check(ctc_ctx_create(device, &ctx), "context");
     ctc_model *model = nullptr, *best = nullptr;

@@ -109,6 +109,43 @@ static void free_mat(DevMat &m)
 
 extern "C" int refh_rank(void) { return DEFAULT_NFACTORS; }
 
+namespace {
+// Three mode CISS copies and the three factors resident on the device, for
+// timing the reference's per-epoch kernel sequences (refh_*_bench).
+struct Resident {
+    DevCiss c[3];
+    DevMat U[3];
+    bool ok = true;
+    Resident(const double *const *entries, const uint64_t *size_rows, const uint64_t *const *directory,
+             const uint64_t *const *dcounter, const uint64_t *dlength, uint64_t nnz, const uint64_t *dims3,
+             const double *const *U0, int ncopies)
+    {
+        for (int m = 0; m < ncopies && ok; ++m)
+            ok = put_ciss(c[m], entries[m], size_rows[m], directory[m], dcounter ? dcounter[m] : nullptr, dlength[m],
+                          nnz, dims3) == 0;
+        for (int m = 0; m < 3 && ok; ++m) ok = put_mat(U[m], U0[m], dims3[m]) == 0;
+        used = ncopies;
+    }
+    ~Resident()
+    {
+        for (int m = 0; m < used; ++m) free_ciss(c[m]);
+        for (int m = 0; m < 3; ++m) free_mat(U[m]);
+    }
+    void get(double *const *U1)
+    {
+        for (int m = 0; m < 3; ++m) get_mat(U[m], U1[m]);
+    }
+    int used = 0;
+};
+
+static float elapsed(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+}  // namespace
+
 #ifdef REF_HARNESS_ALS
 /* Update factor `t` (target) from CISS of its mode; b and c are the factors
  * of the CISS's first and second stored index (sgpu/als.cu:701, 726, 753). */
@@ -157,6 +194,68 @@ extern "C" int refh_als_mode(const double *entries, uint64_t size_rows,
     free_mat(C);
     return rc;
 }
+
+/* `iters` ALS iterations (modes 0, 1, 2, each with the reference driver's
+ * kernel sequence, sgpu/als.cu:691-716 and its case 1 / case 2) on
+ * resident copies; *ms = device time per iteration (CUDA events, after one
+ * untimed warm-up iteration); U (host, row-major) in and out. */
+extern "C" int refh_als_bench(const double *const *entries, const uint64_t *size_rows,
+                              const uint64_t *const *directory, const uint64_t *dlength, uint64_t nnz,
+                              const uint64_t *dims3, double *const *U, double lambda, int iters, double *ms)
+{
+    Resident S(entries, size_rows, directory, nullptr, dlength, nnz, dims3, U, 3);
+    if (!S.ok) return -1;
+    uint64_t maxd = 0;
+    for (int m = 0; m < 3; ++m) maxd = dlength[m] > maxd ? dlength[m] : maxd;
+    double *hbuf = nullptr, **hptr = nullptr, **fptr = nullptr;
+    int *info = nullptr;
+    int rc = 0;
+    rc |= cudaMalloc(&hbuf, (size_t)DEFAULT_NFACTORS * DEFAULT_NFACTORS * maxd * sizeof(double));
+    rc |= cudaMalloc(&hptr, maxd * sizeof(double *));
+    rc |= cudaMalloc(&fptr, maxd * sizeof(double *));
+    rc |= cudaMalloc(&info, maxd * sizeof(int));
+    cusolverDnHandle_t handle = nullptr;
+    if (!rc && cusolverDnCreate(&handle) != CUSOLVER_STATUS_SUCCESS) rc = -2;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    idx_t tilenum = nnz / DEFAULT_T_TILE_LENGTH + 1;
+    idx_t blocknum_m = tilenum / (((idx_t)DEFAULT_BLOCKSIZE) / ((idx_t)ALS_WARPSIZE)) + 1;
+    cublasFillMode_t uplo = CUBLAS_FILL_MODE_UPPER;
+    for (int it = 0; it <= iters && !rc; ++it) {
+        if (it == 1) cudaEventRecord(e0);
+        for (int m = 0; m < 3 && !rc; ++m) {
+            const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+            idx_t blocknum_u = dlength[m] / DEFAULT_BLOCKSIZE + 1;
+            cudaMemset(hbuf, 0, (size_t)DEFAULT_NFACTORS * DEFAULT_NFACTORS * dlength[m] * sizeof(double));
+            cudaMemset(S.U[m].vals, 0, dims3[m] * DEFAULT_NFACTORS * sizeof(double));
+            p_mttkrp_gpu_as<<<blocknum_m, DEFAULT_BLOCKSIZE, 0>>>(S.c[m].dev, S.U[m].dev, S.U[m1].dev, S.U[m2].dev,
+                                                                  hbuf, tilenum);
+            p_update_matrice<<<blocknum_u, DEFAULT_BLOCKSIZE, 0>>>(S.c[m].dev, S.U[m].vals, hbuf, hptr, fptr,
+                                                                   dlength[m], lambda);
+            if (cusolverDnDpotrfBatched(handle, uplo, DEFAULT_NFACTORS, hptr, DEFAULT_NFACTORS, info,
+                                        (int)dlength[m]) != CUSOLVER_STATUS_SUCCESS)
+                rc = -3;
+            if (!rc && cusolverDnDpotrsBatched(handle, uplo, DEFAULT_NFACTORS, 1, hptr, DEFAULT_NFACTORS, fptr,
+                                               DEFAULT_NFACTORS, info, (int)dlength[m]) != CUSOLVER_STATUS_SUCCESS)
+                rc = -4;
+        }
+    }
+    cudaEventRecord(e1);
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = -5;
+    if (!rc) {
+        *ms = iters > 0 ? elapsed(e0, e1) / iters : 0.0;
+        S.get(U);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (handle) cusolverDnDestroy(handle);
+    cudaFree(hbuf);
+    cudaFree(hptr);
+    cudaFree(fptr);
+    cudaFree(info);
+    return rc;
+}
 #endif
 
 #ifdef REF_HARNESS_CCD
@@ -194,6 +293,52 @@ extern "C" int refh_ccd_mode(const double *entries, uint64_t size_rows,
     free_mat(C);
     return rc;
 }
+
+/* `iters` reference CCD+ iterations (modes 0, 1, 2 with the driver's
+ * sequence and grid, sgpu/ccd.cu:561-586) on resident copies; *ms per
+ * iteration after one untimed warm-up iteration. */
+extern "C" int refh_ccd_bench(const double *const *entries, const uint64_t *size_rows,
+                              const uint64_t *const *directory, const uint64_t *dlength, uint64_t nnz,
+                              const uint64_t *dims3, double *const *U, double lambda, int iters, double *ms)
+{
+    Resident S(entries, size_rows, directory, nullptr, dlength, nnz, dims3, U, 3);
+    if (!S.ok) return -1;
+    uint64_t maxd = 0;
+    for (int m = 0; m < 3; ++m) maxd = dlength[m] > maxd ? dlength[m] : maxd;
+    double *num = nullptr, *den = nullptr;
+    int rc = 0;
+    rc |= cudaMalloc(&num, (size_t)DEFAULT_NFACTORS * maxd * sizeof(double));
+    rc |= cudaMalloc(&den, (size_t)DEFAULT_NFACTORS * maxd * sizeof(double));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    idx_t tilenum = nnz / DEFAULT_T_TILE_LENGTH + 1;
+    idx_t blocknum_m = tilenum / ((idx_t)DEFAULT_BLOCKSIZE) + 1;
+    for (int it = 0; it <= iters && !rc; ++it) {
+        if (it == 1) cudaEventRecord(e0);
+        for (int m = 0; m < 3; ++m) {
+            const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
+            idx_t blocknum_u = dlength[m] / DEFAULT_BLOCKSIZE + 1;
+            cudaMemset(num, 0, (size_t)DEFAULT_NFACTORS * dlength[m] * sizeof(double));
+            cudaMemset(den, 0, (size_t)DEFAULT_NFACTORS * dlength[m] * sizeof(double));
+            update_frac_gpu_as<<<blocknum_m, DEFAULT_BLOCKSIZE, 0>>>(S.c[m].dev, S.U[m].dev, S.U[m1].dev,
+                                                                     S.U[m2].dev, num, den, tilenum);
+            update_ccd_gpu<<<blocknum_u, DEFAULT_BLOCKSIZE, 0>>>(S.c[m].dev, S.U[m].dev, num, den, dlength[m],
+                                                                 lambda);
+        }
+    }
+    cudaEventRecord(e1);
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = -5;
+    if (!rc) {
+        *ms = iters > 0 ? elapsed(e0, e1) / iters : 0.0;
+        S.get(U);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(num);
+    cudaFree(den);
+    return rc;
+}
 #endif
 
 #ifdef REF_HARNESS_SGD
@@ -225,6 +370,40 @@ extern "C" int refh_sgd_epoch(const double *entries, uint64_t size_rows,
     free_mat(A);
     free_mat(B);
     free_mat(C);
+    return rc;
+}
+
+/* `epochs` reference SGD epochs (sgpu/sgd.cu:270-287) on the resident
+ * mode-1 copy; *ms per epoch after one untimed warm-up epoch.  Refused
+ * when nnz % 32 == 0, as refh_sgd_epoch. */
+extern "C" int refh_sgd_bench(const double *entries, uint64_t size_rows, const uint64_t *directory,
+                              const uint64_t *dcounter, uint64_t dlength, uint64_t nnz, const uint64_t *dims3,
+                              double *const *U, double lr, double lambda, int epochs, double *ms)
+{
+    if (nnz % DEFAULT_T_TILE_LENGTH == 0) return -10;
+    const double *e[1] = {entries};
+    const uint64_t *d[1] = {directory}, *dc[1] = {dcounter};
+    Resident S(e, &size_rows, d, dc, &dlength, nnz, dims3, U, 1);
+    if (!S.ok) return -1;
+    int rc = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    idx_t tilenum = nnz / DEFAULT_T_TILE_LENGTH + 1;
+    idx_t blocknum_m = tilenum / DEFAULT_BLOCKSIZE + 1;
+    for (int ep = 0; ep <= epochs; ++ep) {
+        if (ep == 1) cudaEventRecord(e0);
+        p_update_sgd_gpu<<<blocknum_m, DEFAULT_BLOCKSIZE, 0>>>(S.c[0].dev, S.U[0].dev, S.U[1].dev, S.U[2].dev, lr,
+                                                                lambda, tilenum);
+    }
+    cudaEventRecord(e1);
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = -5;
+    if (!rc) {
+        *ms = epochs > 0 ? elapsed(e0, e1) / epochs : 0.0;
+        S.get(U);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return rc;
 }
 #endif

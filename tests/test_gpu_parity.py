@@ -269,11 +269,11 @@ def test_sgd_sequential_f32_trajectory(ctx):
         assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-3, e
 
 
-@pytest.mark.parametrize("atomic,R", [(1, 32), (2, 32), (2, 8), (2, 64)])
+@pytest.mark.parametrize("atomic,R", [(1, 32), (2, 32), (2, 8), (2, 64), (3, 8), (3, 32), (3, 64)])
 def test_sgd_hogwild_final_rmse(ctx, atomic, R):
-    """Hogwild with vector atomic adds (1) or bulk row reductions from
-    shared memory (2, the default): final test RMSE within 0.5 % of the
-    deterministic sequential order."""
+    """Hogwild with vector atomic adds (1), bulk row reductions from shared
+    memory (2, the default) or block-merged hot rows (3): final test RMSE
+    within 0.5 % of the deterministic sequential order."""
     P = Problem(200000, (2000, 1500, 200), R, seed=13)
     U, hist = oracle_sgd(P, 10, 0.01, 0.01, decay=0.95)
     G, out = engine_run(ctx, P, ctc.SGD, 10, precision=ctc.PREC_F32, sgd_order=ctc.SGD_HOGWILD,

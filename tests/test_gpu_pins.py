@@ -79,7 +79,7 @@ def zipf2m_oracle(zipf2m):
     return po.rmse(D.o(D.test), U, nthreads=8), po.rmse(T, U, nthreads=8)
 
 
-@pytest.mark.parametrize("atomic", [1, 2])
+@pytest.mark.parametrize("atomic", [1, 2, 3])
 def test_sgd_hogwild_damped_on_zipf_matches_sequential_oracle(ctx, zipf2m, zipf2m_oracle, atomic):
     """The benchmarked Hogwild form: per-row damping at its default bound
     (rows whose expected in-flight updates exceed 128 take proportionally
@@ -214,3 +214,45 @@ def test_adjoint_fp32_bf16_against_fp64_gradient(ctx, order, R, prec):
             assert np.mean(np.abs(g - g64)) / scale < bound / 10
     assert abs(obj - obj64) / obj64 < (1e-6 if prec == ctc.PREC_F32 else 1e-2)
     assert rel(G[0], G64[0]) < bound
+
+
+# ------------------------------------------------------------------ CCD++ mixed precision (packed slots)
+def test_ccdpp_packed_with_full_residual_bits_equals_plain(ctx):
+    """Small dimensions leave 32 bits beside the key, so the packed slots
+    hold the FP32 residual unrounded: the mixed-precision run must equal
+    the plain FP32 run bit for bit (same arithmetic, other layout)."""
+    from tests.helpers import Problem
+    P = Problem(40000, (900, 700, 40), 16, seed=44, heavy_row=3000)
+    outs = {}
+    for prec in (ctc.PREC_F32, ctc.PREC_MIXED):
+        p = ctc.params("ccdpp", rank=16, iters=2, inner=2, precision=prec, early_stop=0, eval_every=1,
+                       tile_len=128, **{"lambda": 0.1})
+        m = P.c_model()
+        out = ctc.run(ctx, P.c_sorted(), None, P.c_test(), m, p)
+        outs[prec] = (m.factors(), [e["rmse_tr"] for e in out.epochs], [e["rmse_te"] for e in out.epochs])
+    for a, b in zip(outs[ctc.PREC_F32][0], outs[ctc.PREC_MIXED][0]):
+        assert np.array_equal(a, b)
+    assert outs[ctc.PREC_F32][1:] == outs[ctc.PREC_MIXED][1:]
+
+
+def test_ccdpp_packed_on_zipf_tracks_plain(ctx, zipf2m):
+    """The 100M workload's dimensions need 45 key bits, leaving 19 for the
+    residual (FP32 sign and exponent, 10 mantissa bits).  Per outer
+    iteration the test RMSE stays within 0.5 % of plain FP32, and the
+    training RMSE read from the packed residuals agrees with the record
+    squared-error kernel on the final factors."""
+    D = zipf2m
+    runs = {}
+    for prec in (ctc.PREC_F32, ctc.PREC_MIXED):
+        p = ctc.params("ccdpp", rank=32, iters=4, inner=3, precision=prec, early_stop=0, eval_every=1,
+                       **{"lambda": 0.1})
+        m = D.model()
+        out = ctc.run(ctx, [D.c(D.train)], None, D.c(D.test), m, p)
+        runs[prec] = (out, m)
+    for e in range(5):
+        a = runs[ctc.PREC_F32][0].epochs[e]["rmse_te"]
+        b = runs[ctc.PREC_MIXED][0].epochs[e]["rmse_te"]
+        assert abs(a - b) / a < 0.005, (e, a, b)
+    out, m = runs[ctc.PREC_MIXED]
+    tr = ctc.rmse(ctx, D.c(D.train), m)
+    assert abs(out.epochs[-1]["rmse_tr"] - tr) / tr < 1e-3, (out.epochs[-1]["rmse_tr"], tr)
