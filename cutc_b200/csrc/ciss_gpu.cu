@@ -236,8 +236,15 @@ static void ciss_build_gpu(ctc_ctx *ctx, const ctc_tensor &t, int mode, int T, b
     c.written.resize(size_rows * 3);
     CK(cudaMemcpyAsync(c.directory.data(), dir.p, dlength * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(c.dcounter.data(), dcnt.p, (dlength + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(c.entries.data(), E.p, size_rows * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(c.written.data(), W.p, size_rows * 3, cudaMemcpyDeviceToHost, ctx->stream));
+    // the layout and the written mask come back through the pinned double
+    // buffer, drained into the (not yet touched) host arrays on the host
+    // threads while the next chunk copies
+    double *ent = c.entries.data();
+    uint8_t *wr = c.written.data();
+    download_drained(ctx, (const double *)E.p, size_rows * 3,
+                     [&](uint64_t b, uint64_t e, const double *h) { memcpy(ent + b, h, (e - b) * sizeof(double)); });
+    download_drained(ctx, (const uint8_t *)W.p, size_rows * 3,
+                     [&](uint64_t b, uint64_t e, const uint8_t *h) { memcpy(wr + b, h, e - b); });
     CK(cudaStreamSynchronize(ctx->stream));
 }
 

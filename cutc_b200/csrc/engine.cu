@@ -2104,8 +2104,8 @@ static std::vector<TuneCand> tune_space(const ctc_params &p)
             add(p.tile_len, 0, 0);
             break;
         }
-        // FP32: vector atomic adds or bulk row reductions (which one is
-        // faster depends on how hot the hottest rows are)
+        // FP32: vector atomic adds, bulk row reductions or block-merged hot
+        // rows (which one is faster depends on how hot the hottest rows are)
         const bool f32 = p.precision != CTC_PREC_F64;
         for (int t : {128, 256, 512, 1024})
             for (int c : {base, base / 2, base / 4})
@@ -2113,6 +2113,7 @@ static std::vector<TuneCand> tune_space(const ctc_params &p)
                     if (f32 && p.sgd_atomic != 0) {
                         add(t, c, 0, 1);
                         add(t, c, 0, 2);
+                        add(t, c, 0, 3);
                     } else {
                         add(t, c, 0);
                     }

@@ -124,10 +124,11 @@ __device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const 
     const int gl = lane % GL, gw = lane / GL;
     double acc = 0;
     // group gw takes the GL consecutive records gw*GL .. gw*GL+GL-1 of the
-    // 32, so in a mode-0-sorted copy it mostly sees one mode-0 row: that
-    // row's slice stays in registers until the index changes
-    uint32_t cur0 = 0xffffffffu;
-    V va{};
+    // 32, so in a copy sorted by (mode 0, mode 1) it mostly sees one mode-0
+    // row, and runs of one mode-1 row inside it: each row's slice stays in
+    // registers until its index changes
+    uint32_t cur0 = 0xffffffffu, cur1 = 0xffffffffu;
+    V va{}, vb{};
     for (uint64_t base = first; base < end; base += stride) {
         const uint64_t mine = base + lane;
         uint4 r = make_uint4(0u, 0u, 0u, 0u);  // row 0 for the tail: in bounds, result unused
@@ -148,7 +149,10 @@ __device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const 
                 va = reinterpret_cast<const V *>(U0 + (size_t)i0 * R)[gl];
                 cur0 = i0;
             }
-            const V vb = reinterpret_cast<const V *>(U1 + (size_t)i1 * R)[gl];
+            if (i1 != cur1) {
+                vb = reinterpret_cast<const V *>(U1 + (size_t)i1 * R)[gl];
+                cur1 = i1;
+            }
             const V vc = reinterpret_cast<const V *>(U2 + (size_t)i2 * R)[gl];
             T p = 0;
 #pragma unroll
@@ -476,12 +480,19 @@ __global__ void __launch_bounds__(256) k_sgd_hot(const uint4 *__restrict__ rec, 
         const uint64_t tile = has_tile ? (t * tile_stride) % ntiles : 0;
         const uint64_t start = tile * tile_len;
         const uint64_t end = has_tile ? min(start + tile_len, (uint64_t)n) : start;
-        // every group of the block takes tile_len steps per round
+        // every group of the block takes tile_len steps per round; the next
+        // nonzero's record and hot codes are fetched during this step
+        uint4 rn = start < end ? rec[start] : make_uint4(0u, 0u, 0u, 0u);
+        uint32_t hn = start < end ? hot[start] : 0u;
         for (uint32_t step = 0; step < tile_len; ++step) {
             const uint64_t p = start + step;
             if (p < end) {
-                const uint4 r = rec[p];
-                const uint32_t hc = hot[p];
+                const uint4 r = rn;
+                const uint32_t hc = hn;
+                if (p + 1 < end) {
+                    rn = rec[p + 1];
+                    hn = hot[p + 1];
+                }
                 const float x = __uint_as_float(r.w);
                 float4 *arow = reinterpret_cast<float4 *>(U0 + (size_t)r.x * R) + gl * C;
                 float4 *brow = reinterpret_cast<float4 *>(U1 + (size_t)r.y * R) + gl * C;

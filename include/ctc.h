@@ -248,7 +248,12 @@ typedef struct {
     int sgd_atomic;        /* Hogwild: 2 = each nonzero's three row deltas added by
                               three bulk row reductions from shared memory (FP32;
                               the default), 1 = vector atomic adds, 0 = plain
-                              stores                                                */
+                              stores, 3 = block-merged hot rows (FP32): the
+                              block's groups step together, one nonzero each, and
+                              the deltas of each mode's 32 most frequent rows are
+                              summed in shared memory and added once per step
+                              (the step's nonzeros act as simultaneous Hogwild
+                              updates); the other rows as in 1                     */
     int eval_every;        /* evaluate RMSE every n epochs (0 = only at the end)    */
     int use_graph;         /* capture the epoch in a CUDA graph when possible       */
     uint64_t seed;         /* reserved for stochastic modes                          */
@@ -382,7 +387,8 @@ int ctc_batch_run(ctc_batch *b, ctc_model *const *models, const ctc_params *p, c
  * half powers of two), the algorithm, precision and rank of `p` and this
  * device's SM count, it times update epochs over a candidate set: tile
  * length (ALS, CCD, CCD++, SGD), lanes per nonzero (SGD threads_per_row),
- * the FP32 Hogwild reduction mode (SGD sgd_atomic 1 or 2), CCD++ column
+ * the FP32 Hogwild reduction mode (SGD sgd_atomic 1, 2 or 3), the SGD
+ * block size (threads_per_block, around each tile length's best), CCD++ column
  * staging on/off (smem_budget), and writes the fastest into
  * `out` (a copy of `p` with those fields replaced).  With cache_path, a
  * cached entry for the shape is returned without a search (unless

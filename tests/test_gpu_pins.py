@@ -13,7 +13,10 @@ ABI):
     sgpu/completion.c:296-362): stop epoch, best epoch and best factors
     equal the oracle's;
   - the FP32 and BF16 adjoint passes the first-order training uses, against
-    the FP64 gradient (ctc_grad), at order 3 and 4.
+    the FP64 gradient (ctc_grad), at order 3 and 4;
+  - mixed-precision CCD++ (packed residual slots): bit-identical to plain
+    FP32 when the residual keeps all 32 bits, within 0.5 % of it per outer
+    iteration on the Zipf sample, where it keeps 19.
 """
 import numpy as np
 import pytest
