@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="library defaults instead of autotuned parameters")
     ap.add_argument("--als", action="store_true",
                     help="the ALS leg alone on --workload (zipf-400m runs it by default)")
+    ap.add_argument("--mixed-step", action="store_true",
+                    help="run the timed step's CCD++ in mixed precision (packed residual slots) instead of FP32 "
+                         "(for profiling the mixed pass; the headline step is FP32)")
     ap.add_argument("--ref-cuda", action="store_true",
                     help="with --impl reference: time the reference's own CUDA kernels (built from its sources "
                          "for sm_100a) on this GPU instead of the CPU restatement")
@@ -236,7 +239,7 @@ def run_ours(args):
     del sorted3
 
     p_ccd = ctc.params("ccdpp", rank=R, inner=3, early_stop=0, iters=10, tile_len=args.ccdpp_tile,
-                       **{"lambda": 0.1})
+                       precision=ctc.PREC_MIXED if args.mixed_step else ctc.PREC_F32, **{"lambda": 0.1})
     p_sgd = ctc.params("sgd", rank=R, lr=1e-3, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY, lr_decay=0.95,
                        early_stop=0, iters=20, **{"lambda": 0.01})
     # autotuned tile length / lanes per nonzero / column staging for this
@@ -252,7 +255,8 @@ def run_ours(args):
         tuned = {"search_s": time.time() - t0, "cache_hit": bool(tr_ccd and tr_ccd[0]["cached"]),
                  "ccdpp": {"tile_len": p_ccd.tile_len, "smem_budget": p_ccd.smem_budget, "trials": tr_ccd},
                  "sgd": {"tile_len": p_sgd.tile_len, "threads_per_row": p_sgd.threads_per_row,
-                         "sgd_atomic": p_sgd.sgd_atomic, "trials": tr_sgd}}
+                         "sgd_atomic": p_sgd.sgd_atomic, "threads_per_block": p_sgd.threads_per_block,
+                         "trials": tr_sgd}}
     ds_ccd = ctc.Dataset(ctx, tr, None, te, p_ccd)
     ds_sgd = ctc.Dataset(ctx, [tr[0]], None, te, p_sgd)
     mdims = ds_ccd.dims()
@@ -328,7 +332,12 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Zipf CP tensor)",
         "config": {"workload": w.name, "dims": list(dims), "nnz_total": w.nnz, "nnz_train": n_train,
                    "nnz_test": n_test, "rank": R, "ccdpp": {"lambda": 0.1, "inner": 3},
-                   "sgd": {"lambda": 0.01, "lr": 1e-3, "decay": 0.95, "order": "hogwild-atomic"},
+                   "sgd": {"lambda": 0.01, "lr": 1e-3, "decay": 0.95,
+                           "order": {0: "hogwild-stores", 1: "hogwild-vector-atomics", 2: "hogwild-bulk-rows",
+                                     3: "hogwild-block-merged-hot-rows"}[p_sgd.sgd_atomic],
+                           "tile_len": p_sgd.tile_len, "threads_per_row": p_sgd.threads_per_row,
+                           "threads_per_block": p_sgd.threads_per_block},
+                   "ccdpp_precision": "mixed (packed slots)" if args.mixed_step else "f32",
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush)"},
         "epoch_s": {"ccdpp_outer": ccd_ms / 1000.0, "sgd": sgd_ms / 1000.0},
         "nnz_per_s": {"ccdpp": n_train / (ccd_ms / 1000.0), "sgd": n_train / (sgd_ms / 1000.0)},
@@ -622,7 +631,8 @@ def e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args, p_ccd=None, p_sgd=Non
 
     def knobs(p):
         return {} if p is None else dict(tile_len=p.tile_len, threads_per_row=p.threads_per_row,
-                                         smem_budget=p.smem_budget, sgd_atomic=p.sgd_atomic)
+                                         smem_budget=p.smem_budget, sgd_atomic=p.sgd_atomic,
+                                         threads_per_block=p.threads_per_block)
     h2d = 2 * (n_train + n_test) * 16 + 2 * sum(mdims) * R * 4
     d2h = 2 * 2 * sum(mdims) * R * 4
     times = []

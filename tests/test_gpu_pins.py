@@ -259,3 +259,49 @@ def test_ccdpp_packed_on_zipf_tracks_plain(ctx, zipf2m):
     out, m = runs[ctc.PREC_MIXED]
     tr = ctc.rmse(ctx, D.c(D.train), m)
     assert abs(out.epochs[-1]["rmse_tr"] - tr) / tr < 1e-3, (out.epochs[-1]["rmse_tr"], tr)
+
+
+# ------------------------------------------------------------------ CCD++ and ALS on the Zipf sample
+def test_ccdpp_fp32_on_zipf_matches_oracle(ctx, zipf2m):
+    """Plain FP32 CCD++ with the benchmarked schedule (lambda 0.1, 3 inner
+    sweeps) on the Zipf sample, whose hottest rows hold hundreds of
+    thousands of nonzeros (long-row groups, partial sums across warps):
+    per-iteration RMSE within 1e-5 and factors within 1e-4 of the FP64
+    oracle."""
+    D = zipf2m
+    U = [u.copy() for u in D.U0]
+    T = D.o(D.train)
+    r = po.residual(T, U)
+    hist = [(po.rmse(T, U, nthreads=8), po.rmse(D.o(D.test), U, nthreads=8))]
+    for _ in range(2):
+        po.ccdpp_outer(T, U, 0.1, 3, r, nthreads=8)
+        hist.append((po.rmse(T, U, nthreads=8), po.rmse(D.o(D.test), U, nthreads=8)))
+    p = ctc.params("ccdpp", rank=32, iters=2, inner=3, precision=ctc.PREC_F32, early_stop=0, eval_every=1,
+                   **{"lambda": 0.1})
+    m = D.model()
+    out = ctc.run(ctx, [D.c(D.train)], None, D.c(D.test), m, p)
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-5, e
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-5, e
+    assert max_factor_rel(m.factors(), U) < 1e-4
+
+
+@pytest.mark.parametrize("prec", [ctc.PREC_F32, ctc.PREC_MIXED])
+def test_als_on_zipf_matches_oracle(ctx, zipf2m, prec):
+    """ALS (lambda 0.1, rank 32) on the Zipf sample, one iteration: FP32
+    within 1e-5 (RMSE) and 1e-4 (factors) of the FP64 oracle; the mixed
+    form, whose long rows take their Gram from BF16 tensor-core MMAs, within
+    0.5 % (RMSE) and 3e-2 (factors)."""
+    D = zipf2m
+    U = [u.copy() for u in D.U0]
+    sorted_o = [D.o(synth.sort_for_mode(*D.train, m)) for m in range(3)]
+    for m in range(3):
+        po.als_mode(sorted_o[m], m, U, 0.1, None, False, nthreads=8)
+    tr, te = po.rmse(D.o(D.train), U, nthreads=8), po.rmse(D.o(D.test), U, nthreads=8)
+    p = ctc.params("als", rank=32, iters=1, precision=prec, early_stop=0, eval_every=1, **{"lambda": 0.1})
+    m = D.model()
+    out = ctc.run(ctx, [D.c(D.train)], None, D.c(D.test), m, p)
+    tol_r, tol_f = (1e-5, 1e-4) if prec == ctc.PREC_F32 else (5e-3, 3e-2)
+    assert abs(out.epochs[1]["rmse_tr"] - tr) / tr < tol_r
+    assert abs(out.epochs[1]["rmse_te"] - te) / te < tol_r
+    assert max_factor_rel(m.factors(), U) < tol_f
