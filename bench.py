@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="library defaults instead of autotuned parameters")
     ap.add_argument("--als", action="store_true",
                     help="the ALS leg alone on --workload (zipf-400m runs it by default)")
+    ap.add_argument("--sgd-atomic", type=int, default=-1,
+                    help="with --no-tune: the Hogwild reduction mode of the step's SGD (1 vector atomics, 2 bulk "
+                         "rows, 3 block-merged hot rows; default: the library's)")
     ap.add_argument("--mixed-step", action="store_true",
                     help="run the timed step's CCD++ in mixed precision (packed residual slots) instead of FP32 "
                          "(for profiling the mixed pass; the headline step is FP32)")
@@ -184,6 +187,58 @@ def max_over_ranks(x: float, device, world: int) -> float:
 
 
 # ---------------------------------------------------------------------------
+def cpu_als_small(seed):
+    """The small uniform workload as configured (2,000 x 1,500 x 200, 200k
+    nonzeros, 90/10 split, R 16, lambda 0.05, 10 iterations, factors
+    U(0,1)/sqrt(16)) on the host cores: the OpenMP FP64 restatement of the
+    reference's ALS update (the reference ships its updates only as CUDA).
+    Returns seconds per iteration, nnz/s, threads and the final test RMSE."""
+    from cutc_b200 import synth
+    from oracle import pyoracle as po
+    w = synth.WORKLOADS["small-als"]
+    g = synth.generate(w, seed=seed, device="cpu")
+    dims = list(w.dims)
+    tr = [po.Tensor(*synth.sort_for_mode(*g["train"], m), dims=dims) for m in range(3)]
+    te = po.Tensor(*g["test"], dims=dims)
+    rng = np.random.default_rng(seed)
+    U = [rng.uniform(0, 1, (d, w.rank)) / np.sqrt(w.rank) for d in dims]
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    for _ in range(10):
+        for m in range(3):
+            po.als_mode(tr[m], m, U, 0.05, None, False, nthreads=threads)
+    s = (time.perf_counter() - t0) / 10
+    return {"workload": w.name, "s_per_iteration": s, "nnz_per_s": tr[0].nnz / s, "cores": threads,
+            "iterations": 10, "test_rmse": po.rmse(te, U, nthreads=threads), "kind": "port",
+            "note": "OpenMP FP64 restatement of the reference ALS update (sgpu/als.cu:186-317, 467-491)"}
+
+
+def gpu_als_small(ctc, ctx, seed):
+    """The small uniform ALS workload (as cpu_als_small, same seeded tensor
+    and factors) on the GPU: FP32, 10 iterations from the host tensors
+    through ctc_run; device time of the update epochs per iteration and the
+    whole call's wall time (staging, epochs, evaluation, factors back)."""
+    from cutc_b200 import synth
+    w = synth.WORKLOADS["small-als"]
+    g = synth.generate(w, seed=seed, device="cpu")
+    rng = np.random.default_rng(seed)
+    U = [rng.uniform(0, 1, (d, w.rank)) / np.sqrt(w.rank) for d in w.dims]
+    tr = ctc.Tensor.from_coo(*synth.sort_for_mode(*g["train"], 0), dims=w.dims)
+    te = ctc.Tensor.from_coo(*g["test"], dims=w.dims)
+    p = ctc.params("als", rank=w.rank, iters=10, early_stop=0, eval_every=0, **{"lambda": 0.05})
+    res = None
+    for _ in range(2):  # the first call pays one-time module loads
+        m = ctc.Model(w.dims, w.rank)
+        m.set_factors(U)
+        t0 = time.perf_counter()
+        out = ctc.run(ctx, [tr], None, te, m, p)
+        wall = time.perf_counter() - t0
+        res = {"workload": w.name, "s_per_iteration": out.result["total_ms"] / 1000.0 / 10,
+               "nnz_per_s": tr.nnz / (out.result["total_ms"] / 1000.0 / 10), "call_s": wall,
+               "test_rmse": out.epochs[-1]["rmse_te"], "precision": "f32"}
+    return res
+
+
 def cpu_baseline(train_sorted0, dims, R, sample, seed, steps=1):
     """The reference's update rules on the host cores (OpenMP FP64 oracle)
     on a seeded random sample: CCD++ outer iteration (3 inner, lambda 0.1)
@@ -242,6 +297,8 @@ def run_ours(args):
                        precision=ctc.PREC_MIXED if args.mixed_step else ctc.PREC_F32, **{"lambda": 0.1})
     p_sgd = ctc.params("sgd", rank=R, lr=1e-3, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY, lr_decay=0.95,
                        early_stop=0, iters=20, **{"lambda": 0.01})
+    if args.sgd_atomic >= 0:
+        p_sgd.sgd_atomic = args.sgd_atomic
     # autotuned tile length / lanes per nonzero / column staging for this
     # shape (the library defaults are among the candidates: their epoch
     # times are reported as the plain form)
@@ -366,6 +423,7 @@ def run_ours(args):
         out["mixed_vs_plain"] = mixed_vs_plain(ctc, ctx, tr, te, mdims, R, args.seed, p_ccd, out["time_to_rmse"])
         out["e2e"] = e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args, p_ccd, p_sgd)
         out["ciss_build"] = ciss_build_times(ctc, ctx, tr[0])
+        out["als_small"] = gpu_als_small(ctc, ctx, args.seed)
         v, s, threads, nsamp = cpu_baseline(base0, dims, R, args.sample, args.seed)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                "sample": f"{nsamp} of {n_train} training nonzeros (seeded random), one "
@@ -684,6 +742,9 @@ def run_reference(args):
                                       f"CCD++ outer (3 inner) + Hogwild SGD epoch, FP64 OpenMP restatement of "
                                       f"the reference update rules (its updates ship only as CUDA)"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    # the small uniform ALS workload, which the reference's configuration
+    # defines to run on the CPU path
+    out["als_small_cpu"] = cpu_als_small(args.seed)
     print(json.dumps(out))
 
 

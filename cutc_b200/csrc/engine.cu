@@ -968,8 +968,8 @@ struct Session : SessionBase {
         }
         if constexpr (std::is_same<T, float>::value && (R / 4) % C == 0 && R / 4 / C <= 32) {
             if (!seq && p.sgd_atomic == 3) {
-                // block-merged hot rows: 256 threads at most per block
-                const int blk = std::min(sgd_block(), 256);
+                // block-merged hot rows: a block's groups step together
+                const int blk = sgd_block();
                 const int gpb_h = (blk / 32) * (32 / (R / 4 / C));
                 LAUNCH(ctx, (k::k_sgd_hot<R, C>), sgd_grid(gpb_h), blk, 0, (const uint4 *)c.rec.p,
                        (const uint32_t *)hot_codes.p, c.n, tile_len, c.ntiles, U[0].p, U[1].p, U[2].p,

@@ -262,12 +262,17 @@ def test_ccdpp_packed_on_zipf_tracks_plain(ctx, zipf2m):
 
 
 # ------------------------------------------------------------------ CCD++ and ALS on the Zipf sample
-def test_ccdpp_fp32_on_zipf_matches_oracle(ctx, zipf2m):
-    """Plain FP32 CCD++ with the benchmarked schedule (lambda 0.1, 3 inner
-    sweeps) on the Zipf sample, whose hottest rows hold hundreds of
-    thousands of nonzeros (long-row groups, partial sums across warps):
-    per-iteration RMSE within 1e-5 and factors within 1e-4 of the FP64
-    oracle."""
+def test_ccdpp_on_zipf_matches_oracle(ctx, zipf2m):
+    """CCD++ with the benchmarked schedule (lambda 0.1, 3 inner sweeps) on
+    the Zipf sample, whose hottest rows hold hundreds of thousands of
+    nonzeros (long-row groups, partial sums across warps).  FP64: factors
+    and per-iteration RMSE within 1e-9 of the FP64 oracle (the same
+    algorithm).  FP32: per-iteration RMSE within 1e-5; factors within 1e-2
+    of the largest entry, not 1e-4: on this sample the FP32 sums
+    r.h over a hot row cancel to a small numerator, which the weakly
+    regularised updates of rarely observed rows (lambda + sum h^2 near 0.1)
+    then amplify over the 192 column updates (measured: 3.9e-3, on the
+    2,000-row mode)."""
     D = zipf2m
     U = [u.copy() for u in D.U0]
     T = D.o(D.train)
@@ -276,14 +281,15 @@ def test_ccdpp_fp32_on_zipf_matches_oracle(ctx, zipf2m):
     for _ in range(2):
         po.ccdpp_outer(T, U, 0.1, 3, r, nthreads=8)
         hist.append((po.rmse(T, U, nthreads=8), po.rmse(D.o(D.test), U, nthreads=8)))
-    p = ctc.params("ccdpp", rank=32, iters=2, inner=3, precision=ctc.PREC_F32, early_stop=0, eval_every=1,
-                   **{"lambda": 0.1})
-    m = D.model()
-    out = ctc.run(ctx, [D.c(D.train)], None, D.c(D.test), m, p)
-    for e, (tr, te) in enumerate(hist):
-        assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-5, e
-        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-5, e
-    assert max_factor_rel(m.factors(), U) < 1e-4
+    for prec, tol_r, tol_f in ((ctc.PREC_F64, 1e-9, 1e-9), (ctc.PREC_F32, 1e-5, 1e-2)):
+        p = ctc.params("ccdpp", rank=32, iters=2, inner=3, precision=prec, early_stop=0, eval_every=1,
+                       **{"lambda": 0.1})
+        m = D.model()
+        out = ctc.run(ctx, [D.c(D.train)], None, D.c(D.test), m, p)
+        for e, (tr, te) in enumerate(hist):
+            assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < tol_r, (prec, e)
+            assert abs(out.epochs[e]["rmse_te"] - te) / te < tol_r, (prec, e)
+        assert max_factor_rel(m.factors(), U) < tol_f, prec
 
 
 @pytest.mark.parametrize("prec", [ctc.PREC_F32, ctc.PREC_MIXED])
