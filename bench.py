@@ -303,6 +303,7 @@ def run_ours(args):
     # shape (the library defaults are among the candidates: their epoch
     # times are reported as the plain form)
     tuned = None
+    cache = None
     if not args.no_tune and not args.ccdpp_tile:
         import tempfile
         cache = args.tune_cache or os.path.join(tempfile.mkdtemp(), "tune.txt")
@@ -416,11 +417,19 @@ def run_ours(args):
     if rank == 0 and not args.no_extras:
         # plain FP32 ALS on the same tensor (lambda 0.1), staged from the
         # mode-1 tensor alone: its copies are sorted on the device
-        ds_als = ctc.Dataset(ctx, [tr[0]], None, te, ctc.params("als", rank=R, early_stop=0, iters=10,
-                                                                **{"lambda": 0.1}))
+        # ALS, plain and mixed, each with its own tuned tile length
+        p_als = ctc.params("als", rank=R, early_stop=0, iters=10, **{"lambda": 0.1})
+        p_als_mx = ctc.params("als", rank=R, precision=ctc.PREC_MIXED, early_stop=0, iters=10, **{"lambda": 0.1})
+        if cache:
+            p_als, _ = ctc.autotune(ctx, [tr[0]], p_als, cache_path=cache)
+            p_als_mx, _ = ctc.autotune(ctx, [tr[0]], p_als_mx, cache_path=cache)
+            tuned["als"] = {"tile_len": p_als.tile_len}
+            tuned["als_mixed"] = {"tile_len": p_als_mx.tile_len}
+        ds_als = ctc.Dataset(ctx, [tr[0]], None, te, p_als)
         out["time_to_rmse"] = time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, args.seed, ds_als)
         ds_als.free()
-        out["mixed_vs_plain"] = mixed_vs_plain(ctc, ctx, tr, te, mdims, R, args.seed, p_ccd, out["time_to_rmse"])
+        out["mixed_vs_plain"] = mixed_vs_plain(ctc, ctx, tr, te, mdims, R, args.seed, p_ccd, out["time_to_rmse"],
+                                               p_als_mx)
         out["e2e"] = e2e(ctc, ctx, tr, te, mdims, R, n_train, n_test, args, p_ccd, p_sgd)
         out["ciss_build"] = ciss_build_times(ctc, ctx, tr[0])
         out["als_small"] = gpu_als_small(ctc, ctx, args.seed)
@@ -603,7 +612,7 @@ def time_to_rmse(ctc, ds_ccd, ds_sgd, mdims, R, seed, ds_als=None, legs=None, ta
     return res
 
 
-def mixed_vs_plain(ctc, ctx, tr, te, mdims, R, seed, p_ccd, plain):
+def mixed_vs_plain(ctc, ctx, tr, te, mdims, R, seed, p_ccd, plain, p_als_mx=None):
     """The mixed-precision forms on the same tensor and schedules, against
     the plain FP32 runs of time_to_rmse (`plain`): ALS with BF16 factor
     copies into tcgen05 Gram blocks for the pieces of long rows (FP64 row
@@ -613,8 +622,9 @@ def mixed_vs_plain(ctc, ctx, tr, te, mdims, R, seed, p_ccd, plain):
     reductions into the FP32 rows, which a narrower gather does not
     remove)."""
     legs = []
-    ds_als = ctc.Dataset(ctx, [tr[0]], None, te, ctc.params("als", rank=R, precision=ctc.PREC_MIXED, early_stop=0,
-                                                            iters=10, **{"lambda": 0.1}))
+    if p_als_mx is None:
+        p_als_mx = ctc.params("als", rank=R, precision=ctc.PREC_MIXED, early_stop=0, iters=10, **{"lambda": 0.1})
+    ds_als = ctc.Dataset(ctx, [tr[0]], None, te, p_als_mx)
     q = ctc.params("ccdpp", rank=R, inner=3, early_stop=0, iters=10, precision=ctc.PREC_MIXED,
                    tile_len=p_ccd.tile_len, smem_budget=p_ccd.smem_budget, **{"lambda": 0.1})
     ds_ccd = ctc.Dataset(ctx, [tr[0]], None, te, q)

@@ -2087,6 +2087,8 @@ static std::vector<TuneCand> tune_space(const ctc_params &p)
     };
     switch (p.alg) {
     case CTC_ALG_ALS:
+        // mixed precision: shorter tiles send more rows to the tensor-core Gram
+        if (p.precision == CTC_PREC_MIXED) add(128, 0, 0);
         for (int t : {256, 512, 1024, 2048}) add(t, 0, 0);
         break;
     case CTC_ALG_CCD:
