@@ -10,9 +10,9 @@
 // writes them to the piece's slot ({G row-major, b}, the layout the FP64
 // fixup solve k_als_fix reads).
 //
-// The h rows of 128 nonzeros are staged in shared memory as BF16, one
-// 128-byte row per nonzero with the 128-byte swizzle (16-byte chunk c of
-// row k stored at chunk c ^ (k & 7), 1 KiB aligned).  Read as an MN-major
+// The h rows of a chunk of nonzeros are staged in shared memory as BF16,
+// 128-byte rows with the 128-byte swizzle (16-byte chunk c of row k stored
+// at chunk c ^ (k & 7), 1 KiB aligned).  Read as an MN-major
 // operand that tile is both A = H^T (M = 64 x K) and B = H (K x N = 64), so
 // each tcgen05.mma (M=64, N=64, K=16, kind::f16, BF16 in, FP32 out)
 // accumulates 16 nonzeros of h h^T.  One thread issues the MMAs and commits
@@ -30,8 +30,7 @@
 namespace ctc {
 namespace tc {
 
-constexpr int kChunk = 128;   // nonzeros staged per round (one per thread)
-constexpr int kThreads = 128;
+constexpr int kThreads = 128;  // one 128-byte operand row per thread and chunk
 
 using px::smem_u32;
 using px::mbar_try_wait;
@@ -101,12 +100,13 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // indices of the mode's plan), rank R = 64 or 32; slot[t] = {G (R x R
 // row-major), b (R)}.  err[0] is set when a bounded wait expires.
 //
-// Operand rows are 128 bytes.  At R = 64 a row is one nonzero's h.  At
-// R = 32 a row holds two nonzeros, h(k) in its first 64 bytes and h(k + 64)
-// in its second: the 64 x 64 product of such rows has the Grams of the two
-// halves on its diagonal blocks (the off-diagonal blocks are not read), so
-// a 128-nonzero chunk is 64 rows and 4 MMAs, and G = block(0,0) +
-// block(1,1), added in that order.
+// Operand rows are 128 bytes, one per thread and chunk.  At R = 64 a row
+// is one nonzero's h (a chunk is 128 nonzeros).  At R = 32 a row holds two
+// nonzeros, h(c0 + t) in its first 64 bytes and h(c0 + 128 + t) in its
+// second: the 64 x 64 product of such rows has the Grams of the two halves
+// on its diagonal blocks (the off-diagonal blocks are not read), so a chunk
+// is 256 nonzeros in 128 rows and 8 MMAs, and G = block(0,0) + block(1,1),
+// added in that order.
 //
 // Two operand tiles alternate: while the MMAs of one chunk run, the CTA
 // gathers the next chunk into the other tile; a tile is rewritten only
@@ -118,9 +118,11 @@ __global__ void __launch_bounds__(kThreads, R == 64 ? 2 : 4)
                   const __nv_bfloat16 *__restrict__ Ub, float *__restrict__ slot, int *err)
 {
     static_assert(R == 64 || R == 32, "tensor-core Gram ranks");
-    constexpr int kRows = R == 64 ? kChunk : kChunk / 2;  // operand rows per chunk
-    constexpr int kTile = kRows * 128;                     // bytes per operand tile
-    constexpr int kVec = R / 8;                            // 16-byte words of a BF16 factor row
+    constexpr int NPT = 64 / R;           // nonzeros per thread and chunk (one 128-byte row each)
+    constexpr int kNz = kThreads * NPT;   // nonzeros per chunk
+    constexpr int kRows = kThreads;       // operand rows per chunk
+    constexpr int kTile = kRows * 128;    // bytes per operand tile
+    constexpr int kVec = R / 8;           // 16-byte words of a BF16 factor row
     extern __shared__ uint8_t dsm[];
     uint8_t *hs0 = dsm + ((1024u - (smem_u32(dsm) & 1023u)) & 1023u);
     __shared__ float rhs_part[kThreads / 32][R];
@@ -130,9 +132,6 @@ __global__ void __launch_bounds__(kThreads, R == 64 ? 2 : 4)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
     const uint32_t idesc = idesc_bf16_m64_n64();
-    // this thread's operand row and its first 16-byte chunk within the row
-    const int orow = R == 64 ? tid : (tid & 63);
-    const int ochunk = R == 64 ? 0 : (tid >> 6) * 4;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -172,55 +171,78 @@ __global__ void __launch_bounds__(kThreads, R == 64 ? 2 : 4)
         float rhs[R];
 #pragma unroll
         for (int f = 0; f < R; ++f) rhs[f] = 0.f;
-        for (uint32_t c0 = start; c0 < end && ok; c0 += kChunk) {
+        // records of the piece's first chunk; later chunks' records are
+        // fetched while the current chunk's rows are gathered
+        uint4 rn[NPT];
+#pragma unroll
+        for (int j = 0; j < NPT; ++j) {
+            const uint32_t p = start + tid + j * kThreads;
+            rn[j] = p < end ? rec[p] : make_uint4(0u, 0u, 0u, 0u);
+        }
+        for (uint32_t c0 = start; c0 < end && ok; c0 += kNz) {
             const int b = (int)(nchunk & 1u);
             drain(b);
             if (!ok) break;
             uint8_t *hs = hs0 + b * kTile;
-            uint8_t *row = hs + orow * 128;
-            const uint32_t p = c0 + tid;
-            if (p < end) {
-                const uint4 r = rec[p];
-                const float x = __uint_as_float(r.w);
-                const uint32_t q1 = m1 == 0 ? r.x : (m1 == 1 ? r.y : r.z);
-                const uint32_t q2 = m2 == 0 ? r.x : (m2 == 1 ? r.y : r.z);
-                const uint4 *ba = reinterpret_cast<const uint4 *>(Ua + (size_t)q1 * R);
-                const uint4 *bb = reinterpret_cast<const uint4 *>(Ub + (size_t)q2 * R);
-                uint4 va[kVec], vb[kVec];
+            uint8_t *row = hs + tid * 128;
+            uint4 r[NPT];
+            uint4 va[NPT][kVec], vb[NPT][kVec];
 #pragma unroll
-                for (int c = 0; c < kVec; ++c) {
-                    va[c] = ba[c];
-                    vb[c] = bb[c];
-                }
+            for (int j = 0; j < NPT; ++j) {
+                r[j] = rn[j];
+                if (c0 + tid + j * kThreads < end) {
+                    const uint32_t q1 = m1 == 0 ? r[j].x : (m1 == 1 ? r[j].y : r[j].z);
+                    const uint32_t q2 = m2 == 0 ? r[j].x : (m2 == 1 ? r[j].y : r[j].z);
+                    const uint4 *ba = reinterpret_cast<const uint4 *>(Ua + (size_t)q1 * R);
+                    const uint4 *bb = reinterpret_cast<const uint4 *>(Ub + (size_t)q2 * R);
 #pragma unroll
-                for (int c = 0; c < kVec; ++c) {
-                    const __nv_bfloat162 *pa = reinterpret_cast<const __nv_bfloat162 *>(&va[c]);
-                    const __nv_bfloat162 *pb = reinterpret_cast<const __nv_bfloat162 *>(&vb[c]);
-                    uint32_t outw[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float2 fa = __bfloat1622float2(pa[q]);
-                        const float2 fb = __bfloat1622float2(pb[q]);
-                        const float h0 = fa.x * fb.x, h1 = fa.y * fb.y;
-                        rhs[8 * c + 2 * q] += x * h0;
-                        rhs[8 * c + 2 * q + 1] += x * h1;
-                        outw[q] = pack_bf16(h0, h1);
+                    for (int c = 0; c < kVec; ++c) {
+                        va[j][c] = ba[c];
+                        vb[j][c] = bb[c];
                     }
-                    *reinterpret_cast<uint4 *>(row + (((ochunk + c) ^ (orow & 7)) << 4)) =
-                        make_uint4(outw[0], outw[1], outw[2], outw[3]);
                 }
-            } else {
+            }
 #pragma unroll
-                for (int c = 0; c < kVec; ++c)
-                    *reinterpret_cast<uint4 *>(row + (((ochunk + c) ^ (orow & 7)) << 4)) = make_uint4(0, 0, 0, 0);
+            for (int j = 0; j < NPT; ++j) {
+                const uint32_t pn = c0 + kNz + tid + j * kThreads;
+                rn[j] = pn < end ? rec[pn] : make_uint4(0u, 0u, 0u, 0u);
+            }
+#pragma unroll
+            for (int j = 0; j < NPT; ++j) {
+                // nonzero c0 + tid + j * kThreads fills segment j of operand row tid
+                if (c0 + tid + j * kThreads < end) {
+                    const float x = __uint_as_float(r[j].w);
+#pragma unroll
+                    for (int c = 0; c < kVec; ++c) {
+                        const __nv_bfloat162 *pa = reinterpret_cast<const __nv_bfloat162 *>(&va[j][c]);
+                        const __nv_bfloat162 *pb = reinterpret_cast<const __nv_bfloat162 *>(&vb[j][c]);
+                        uint32_t outw[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float2 fa = __bfloat1622float2(pa[q]);
+                            const float2 fb = __bfloat1622float2(pb[q]);
+                            const float h0 = fa.x * fb.x, h1 = fa.y * fb.y;
+                            rhs[8 * c + 2 * q] += x * h0;
+                            rhs[8 * c + 2 * q + 1] += x * h1;
+                            outw[q] = pack_bf16(h0, h1);
+                        }
+                        *reinterpret_cast<uint4 *>(row + (((j * kVec + c) ^ (tid & 7)) << 4)) =
+                            make_uint4(outw[0], outw[1], outw[2], outw[3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < kVec; ++c)
+                        *reinterpret_cast<uint4 *>(row + (((j * kVec + c) ^ (tid & 7)) << 4)) =
+                            make_uint4(0, 0, 0, 0);
+                }
             }
             // make the generic-proxy stores visible to the tensor core
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             if (tid == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t nk = min((uint32_t)kChunk, end - c0);
-                const uint32_t rows = R == 64 ? nk : min(nk, (uint32_t)kRows);
+                // rows past the chunk's nonzeros are zero in every segment
+                const uint32_t rows = min(end - c0, (uint32_t)kRows);
                 const uint32_t nmma = (rows + 15) / 16;
                 const uint32_t hs_addr = smem_u32(hs);
                 for (uint32_t kk = 0; kk < nmma; ++kk) {
@@ -295,11 +317,12 @@ __global__ void __launch_bounds__(kThreads, R == 64 ? 2 : 4)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(64u));
 }
 
-// dynamic shared memory of k_als_gram_tc<R>: two operand tiles + alignment
+// dynamic shared memory of k_als_gram_tc<R>: two operand tiles of kThreads
+// 128-byte rows + alignment
 template <int R>
 constexpr int gram_smem_bytes()
 {
-    return 2 * (R == 64 ? kChunk : kChunk / 2) * 128 + 1024;
+    return 2 * kThreads * 128 + 1024;
 }
 
 // FP32 factor rows -> BF16 copies (row-major, same shape)
