@@ -789,6 +789,11 @@ def als_leg(ctc, ctx, args, device):
     for name, prec in forms:
         p = ctc.params("als", rank=w.rank, precision=prec, iters=iters, early_stop=0, eval_every=0,
                        **{"lambda": lam})
+        trials = None
+        if not args.no_tune:
+            # tile length per form (mixed precision also tries 128, sending more
+            # rows to the tensor-core Gram); the search is not timed
+            p, trials = ctc.autotune(ctx, tr, p, cache_path=args.tune_cache or None)
         t1 = time.time()
         ds = ctc.Dataset(ctx, tr, None, te, p)
         stage_s = time.time() - t1
@@ -799,9 +804,10 @@ def als_leg(ctc, ctx, args, device):
         kt = {k: ctx.kernel_time(k) for k in ("k_als_tile", "k_als_sum_pieces", "k_als_fix", "k_als_gram_tc")}
         ctx.set_profiling(False)
         it_s = run.result["total_ms"] / 1000.0 / iters
-        out[name] = {"iteration_s": it_s, "nnz_per_s": ntr / it_s, "stage_s": stage_s,
+        out[name] = {"iteration_s": it_s, "nnz_per_s": ntr / it_s, "stage_s": stage_s, "tile_len": p.tile_len,
                      "test_rmse": run.epochs[-1]["rmse_te"], "train_rmse": run.epochs[-1]["rmse_tr"],
-                     "kernels": {k: {"launches": v[0], "ms_per_iter": v[1] / iters} for k, v in kt.items() if v[0]}}
+                     "kernels": {k: {"launches": v[0], "ms_per_iter": v[1] / iters} for k, v in kt.items() if v[0]},
+                     "tune_trials": trials}
         ds.free()
         m.free()
     return out

@@ -118,11 +118,13 @@ __global__ void __launch_bounds__(kThreads, R == 64 ? 2 : 4)
                   const __nv_bfloat16 *__restrict__ Ub, float *__restrict__ slot, int *err)
 {
     static_assert(R == 64 || R == 32, "tensor-core Gram ranks");
-    constexpr int NPT = 64 / R;           // nonzeros per thread and chunk (one 128-byte row each)
-    constexpr int kNz = kThreads * NPT;   // nonzeros per chunk
+    constexpr int kVec = R / 8;           // 16-byte words of a BF16 factor row
+    constexpr int kNz = kThreads * (64 / R);  // nonzeros per chunk: 128 rows of 128 bytes
     constexpr int kRows = kThreads;       // operand rows per chunk
     constexpr int kTile = kRows * 128;    // bytes per operand tile
-    constexpr int kVec = R / 8;           // 16-byte words of a BF16 factor row
+    constexpr int kLpn = kVec;            // lanes per nonzero in the gathers (one word each)
+    constexpr int kNpi = 32 / kLpn;       // nonzeros per warp and gather step
+    constexpr int kIt = kNz / 4 / kNpi;   // gather steps per warp and chunk (8)
     extern __shared__ uint8_t dsm[];
     uint8_t *hs0 = dsm + ((1024u - (smem_u32(dsm) & 1023u)) & 1023u);
     __shared__ float rhs_part[kThreads / 32][R];
@@ -132,6 +134,10 @@ __global__ void __launch_bounds__(kThreads, R == 64 ? 2 : 4)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;
     const uint32_t idesc = idesc_bf16_m64_n64();
+    // gathers: warp w takes the chunk's nonzeros w*kNz/4 .. (w+1)*kNz/4 - 1,
+    // kNpi per step, lane (word, n) = (lane % kLpn, lane / kLpn)
+    const int word = lane % kLpn;
+    const int nz0 = warp * (kNz / 4) + lane / kLpn;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -168,73 +174,64 @@ __global__ void __launch_bounds__(kThreads, R == 64 ? 2 : 4)
         const uint32_t tile = pieces[pi];
         const int4 td = tiles[tile];
         const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
-        float rhs[R];
+        // this lane's slice of the right-hand side: columns 8*word .. 8*word+7
+        float rhs[8];
 #pragma unroll
-        for (int f = 0; f < R; ++f) rhs[f] = 0.f;
+        for (int e = 0; e < 8; ++e) rhs[e] = 0.f;
         // records of the piece's first chunk; later chunks' records are
         // fetched while the current chunk's rows are gathered
-        uint4 rn[NPT];
+        uint4 rn[kIt];
 #pragma unroll
-        for (int j = 0; j < NPT; ++j) {
-            const uint32_t p = start + tid + j * kThreads;
-            rn[j] = p < end ? rec[p] : make_uint4(0u, 0u, 0u, 0u);
+        for (int it = 0; it < kIt; ++it) {
+            const uint32_t p = start + nz0 + it * kNpi;
+            rn[it] = p < end ? rec[p] : make_uint4(0u, 0u, 0u, 0u);
         }
         for (uint32_t c0 = start; c0 < end && ok; c0 += kNz) {
             const int b = (int)(nchunk & 1u);
             drain(b);
             if (!ok) break;
             uint8_t *hs = hs0 + b * kTile;
-            uint8_t *row = hs + tid * 128;
-            uint4 r[NPT];
-            uint4 va[NPT][kVec], vb[NPT][kVec];
+            // the group of kLpn lanes of nonzero k = nz0 + it * kNpi loads
+            // word `word` of its two factor rows: one L1 wavefront per row
+            uint4 va[kIt], vb[kIt];
+            float x[kIt];
 #pragma unroll
-            for (int j = 0; j < NPT; ++j) {
-                r[j] = rn[j];
-                if (c0 + tid + j * kThreads < end) {
-                    const uint32_t q1 = m1 == 0 ? r[j].x : (m1 == 1 ? r[j].y : r[j].z);
-                    const uint32_t q2 = m2 == 0 ? r[j].x : (m2 == 1 ? r[j].y : r[j].z);
-                    const uint4 *ba = reinterpret_cast<const uint4 *>(Ua + (size_t)q1 * R);
-                    const uint4 *bb = reinterpret_cast<const uint4 *>(Ub + (size_t)q2 * R);
-#pragma unroll
-                    for (int c = 0; c < kVec; ++c) {
-                        va[j][c] = ba[c];
-                        vb[j][c] = bb[c];
-                    }
+            for (int it = 0; it < kIt; ++it) {
+                x[it] = __uint_as_float(rn[it].w);
+                if (c0 + nz0 + it * kNpi < end) {
+                    const uint32_t q1 = m1 == 0 ? rn[it].x : (m1 == 1 ? rn[it].y : rn[it].z);
+                    const uint32_t q2 = m2 == 0 ? rn[it].x : (m2 == 1 ? rn[it].y : rn[it].z);
+                    va[it] = reinterpret_cast<const uint4 *>(Ua + (size_t)q1 * R)[word];
+                    vb[it] = reinterpret_cast<const uint4 *>(Ub + (size_t)q2 * R)[word];
                 }
             }
 #pragma unroll
-            for (int j = 0; j < NPT; ++j) {
-                const uint32_t pn = c0 + kNz + tid + j * kThreads;
-                rn[j] = pn < end ? rec[pn] : make_uint4(0u, 0u, 0u, 0u);
+            for (int it = 0; it < kIt; ++it) {
+                const uint32_t pn = c0 + kNz + nz0 + it * kNpi;
+                rn[it] = pn < end ? rec[pn] : make_uint4(0u, 0u, 0u, 0u);
             }
 #pragma unroll
-            for (int j = 0; j < NPT; ++j) {
-                // nonzero c0 + tid + j * kThreads fills segment j of operand row tid
-                if (c0 + tid + j * kThreads < end) {
-                    const float x = __uint_as_float(r[j].w);
+            for (int it = 0; it < kIt; ++it) {
+                // nonzero k of the chunk fills segment k / kThreads of operand row k % kThreads
+                const int k = nz0 + it * kNpi;
+                const int orow = k % kThreads, seg = k / kThreads;
+                uint4 out = make_uint4(0u, 0u, 0u, 0u);
+                if (c0 + k < end) {
+                    const __nv_bfloat162 *pa = reinterpret_cast<const __nv_bfloat162 *>(&va[it]);
+                    const __nv_bfloat162 *pb = reinterpret_cast<const __nv_bfloat162 *>(&vb[it]);
+                    uint32_t outw[4];
 #pragma unroll
-                    for (int c = 0; c < kVec; ++c) {
-                        const __nv_bfloat162 *pa = reinterpret_cast<const __nv_bfloat162 *>(&va[j][c]);
-                        const __nv_bfloat162 *pb = reinterpret_cast<const __nv_bfloat162 *>(&vb[j][c]);
-                        uint32_t outw[4];
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const float2 fa = __bfloat1622float2(pa[q]);
-                            const float2 fb = __bfloat1622float2(pb[q]);
-                            const float h0 = fa.x * fb.x, h1 = fa.y * fb.y;
-                            rhs[8 * c + 2 * q] += x * h0;
-                            rhs[8 * c + 2 * q + 1] += x * h1;
-                            outw[q] = pack_bf16(h0, h1);
-                        }
-                        *reinterpret_cast<uint4 *>(row + (((j * kVec + c) ^ (tid & 7)) << 4)) =
-                            make_uint4(outw[0], outw[1], outw[2], outw[3]);
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 fa = __bfloat1622float2(pa[q]);
+                        const float2 fb = __bfloat1622float2(pb[q]);
+                        const float h0 = fa.x * fb.x, h1 = fa.y * fb.y;
+                        rhs[2 * q] += x[it] * h0;
+                        rhs[2 * q + 1] += x[it] * h1;
+                        outw[q] = pack_bf16(h0, h1);
                     }
-                } else {
-#pragma unroll
-                    for (int c = 0; c < kVec; ++c)
-                        *reinterpret_cast<uint4 *>(row + (((j * kVec + c) ^ (tid & 7)) << 4)) =
-                            make_uint4(0, 0, 0, 0);
+                    out = make_uint4(outw[0], outw[1], outw[2], outw[3]);
                 }
+                *reinterpret_cast<uint4 *>(hs + orow * 128 + (((seg * kVec + word) ^ (orow & 7)) << 4)) = out;
             }
             // make the generic-proxy stores visible to the tensor core
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -259,13 +256,15 @@ __global__ void __launch_bounds__(kThreads, R == 64 ? 2 : 4)
         drain(1);
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // right-hand side: warp butterflies, then a fixed-order sum over warps
+        // right-hand side: sum the slices of the lanes that hold the same
+        // word (butterflies over the nonzero bits of the lane), then a
+        // fixed-order sum over warps
 #pragma unroll
-        for (int f = 0; f < R; ++f) {
-            float v = rhs[f];
+        for (int e = 0; e < 8; ++e) {
+            float v = rhs[e];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) rhs_part[warp][f] = v;
+            for (int o = 16; o >= kLpn; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane < kLpn) rhs_part[warp][8 * lane + e] = v;
         }
         // accumulator rows 16w..16w+15 live in TMEM lanes 32w..32w+15
         uint32_t g[64];

@@ -460,20 +460,22 @@ __global__ void __launch_bounds__(512) k_sgd_hot(const uint4 *__restrict__ rec, 
     constexpr int GPW = 32 / G;
     constexpr int NV = R / VN;  // float4 per row
     __shared__ __align__(16) float4 acc[3 * kSgdHot * NV];
-    __shared__ uint32_t touched[3];  // bit s of word m: slot s of mode m got a delta this step
+    // bit s of touched[p][m]: slot s of mode m got a delta in a step of parity p
+    __shared__ uint32_t touched[2][3];
     __shared__ uint32_t hrow[3 * kSgdHot];
     const int lane = threadIdx.x & 31;
     const int gl = lane % G;
     const int gw = lane / G;
     for (int i = threadIdx.x; i < 3 * kSgdHot * NV; i += blockDim.x) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = threadIdx.x; i < 3 * kSgdHot; i += blockDim.x) hrow[i] = hot_rows[i];
-    if (threadIdx.x < 3) touched[threadIdx.x] = 0u;
+    if (threadIdx.x < 6) touched[threadIdx.x / 3][threadIdx.x % 3] = 0u;
     __syncthreads();
     const uint64_t ngb = (uint64_t)(blockDim.x >> 5) * GPW;  // groups per block
     const uint64_t group = blockIdx.x * ngb + (uint64_t)(threadIdx.x >> 5) * GPW + gw;
     const uint64_t ngroups = (uint64_t)gridDim.x * ngb;
     const uint64_t rounds = (ntiles + ngroups - 1) / ngroups;
     const float s = *lr_dev;
+    uint32_t par = 0;  // parity of the block's step
     for (uint64_t k = 0; k < rounds; ++k) {
         const uint64_t t = group + k * ngroups;
         const bool has_tile = t < ntiles;
@@ -552,23 +554,25 @@ __global__ void __launch_bounds__(512) k_sgd_hot(const uint4 *__restrict__ rec, 
                 if (gl == 0)
 #pragma unroll
                     for (int m = 0; m < 3; ++m)
-                        if (slot[m] != kSgdCold) atomicOr(&touched[m], 1u << slot[m]);
+                        if (slot[m] != kSgdCold) atomicOr(&touched[par][m], 1u << slot[m]);
             }
             __syncthreads();
-            // one vector atomic per 16 bytes of every touched hot row
+            // one vector atomic per 16 bytes of every touched hot row; the
+            // other parity's marks (the previous step's, read before the
+            // barrier above) are cleared for the next step
+            if (threadIdx.x < 3) touched[par ^ 1u][threadIdx.x] = 0u;
             for (int i = threadIdx.x; i < 3 * kSgdHot * NV; i += blockDim.x) {
                 const int m = i / (kSgdHot * NV), sl = (i / NV) % kSgdHot, v = i % NV;
-                if ((touched[m] >> sl) & 1u) {
+                if ((touched[par][m] >> sl) & 1u) {
                     const float4 d = acc[i];
                     acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
                     float *um = m == 0 ? U0 : (m == 1 ? U1 : U2);
                     vatomic_add(reinterpret_cast<float4 *>(um + (size_t)hrow[m * kSgdHot + sl] * R) + v, d);
                 }
             }
+            // the accumulators are cleared before the next step adds to them
             __syncthreads();
-            // cleared before any thread can mark a slot in the next step
-            if (threadIdx.x < 3) touched[threadIdx.x] = 0u;
-            __syncthreads();
+            par ^= 1u;
         }
     }
 }
