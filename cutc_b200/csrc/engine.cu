@@ -443,13 +443,7 @@ static void stage_copies_dev(ctc_ctx *ctx, const ctc_params &p, uint32_t tl, con
             std::vector<uint32_t> rows, counts;
             if (dev_row_runs(ctx, src->rec.p, pp, (uint32_t)n, m, rows, counts))
                 fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", m + 1, m + 1);
-            // mixed ALS: every row the k x k dual does not solve (more than
-            // R/2 nonzeros) gets tiles of its own, whose Gram the tensor
-            // cores form; the light tiles keep only the short rows
-            const bool tc_rows = p.alg == CTC_ALG_ALS && p.precision == CTC_PREC_MIXED &&
-                                 (p.rank == 32 || p.rank == 64) && p.compat == 0;
-            plan = plan_tiles_runs(rows.data(), counts.data(), rows.size(), tl,
-                                   tc_rows ? (uint32_t)(p.rank / 2) : 0u);
+            plan = plan_tiles_runs(rows.data(), counts.data(), rows.size(), tl);
             upload_plan(ctx, plan, m, d);
         }
         if (ccdpp) {

@@ -482,29 +482,19 @@ __global__ void __launch_bounds__(512) k_sgd_hot(const uint4 *__restrict__ rec, 
         const uint64_t tile = has_tile ? (t * tile_stride) % ntiles : 0;
         const uint64_t start = tile * tile_len;
         const uint64_t end = has_tile ? min(start + tile_len, (uint64_t)n) : start;
-        // every group of the block takes tile_len steps per round.  The
-        // pipeline: while nonzero p is processed, the rows of p + 1 are read
-        // (after p's own vector atomics, so p's updates of cold rows are in
-        // them; this step's merged hot-row deltas are not, one step of
-        // staleness) and the record of p + 2 is fetched
+        // every group of the block takes tile_len steps per round; the next
+        // nonzero's record and hot codes are fetched during this step
         uint4 rn = start < end ? rec[start] : make_uint4(0u, 0u, 0u, 0u);
         uint32_t hn = start < end ? hot[start] : 0u;
-        float4 an[C], bn[C], cn[C];
-        if (start < end) {
-#pragma unroll
-            for (int q = 0; q < C; ++q) {
-                an[q] = __ldcg(reinterpret_cast<const float4 *>(U0 + (size_t)rn.x * R) + gl * C + q);
-                bn[q] = __ldcg(reinterpret_cast<const float4 *>(U1 + (size_t)rn.y * R) + gl * C + q);
-                cn[q] = __ldcg(reinterpret_cast<const float4 *>(U2 + (size_t)rn.z * R) + gl * C + q);
-            }
-        }
-        uint4 rnn = start + 1 < end ? rec[start + 1] : make_uint4(0u, 0u, 0u, 0u);
-        uint32_t hnn = start + 1 < end ? hot[start + 1] : 0u;
         for (uint32_t step = 0; step < tile_len; ++step) {
             const uint64_t p = start + step;
             if (p < end) {
                 const uint4 r = rn;
                 const uint32_t hc = hn;
+                if (p + 1 < end) {
+                    rn = rec[p + 1];
+                    hn = hot[p + 1];
+                }
                 const float x = __uint_as_float(r.w);
                 float4 *arow = reinterpret_cast<float4 *>(U0 + (size_t)r.x * R) + gl * C;
                 float4 *brow = reinterpret_cast<float4 *>(U1 + (size_t)r.y * R) + gl * C;
@@ -512,9 +502,9 @@ __global__ void __launch_bounds__(512) k_sgd_hot(const uint4 *__restrict__ rec, 
                 float4 a[C], b[C], c[C];
 #pragma unroll
                 for (int q = 0; q < C; ++q) {
-                    a[q] = an[q];
-                    b[q] = bn[q];
-                    c[q] = cn[q];
+                    a[q] = __ldcg(arow + q);
+                    b[q] = __ldcg(brow + q);
+                    c[q] = __ldcg(crow + q);
                 }
                 float part = 0;
 #pragma unroll
@@ -565,21 +555,6 @@ __global__ void __launch_bounds__(512) k_sgd_hot(const uint4 *__restrict__ rec, 
 #pragma unroll
                     for (int m = 0; m < 3; ++m)
                         if (slot[m] != kSgdCold) atomicOr(&touched[par][m], 1u << slot[m]);
-                // advance the pipeline: rows of p + 1, record of p + 2
-                rn = rnn;
-                hn = hnn;
-                if (p + 1 < end) {
-#pragma unroll
-                    for (int q = 0; q < C; ++q) {
-                        an[q] = __ldcg(reinterpret_cast<const float4 *>(U0 + (size_t)rn.x * R) + gl * C + q);
-                        bn[q] = __ldcg(reinterpret_cast<const float4 *>(U1 + (size_t)rn.y * R) + gl * C + q);
-                        cn[q] = __ldcg(reinterpret_cast<const float4 *>(U2 + (size_t)rn.z * R) + gl * C + q);
-                    }
-                }
-                if (p + 2 < end) {
-                    rnn = rec[p + 2];
-                    hnn = hot[p + 2];
-                }
             }
             __syncthreads();
             // one vector atomic per 16 bytes of every touched hot row; the
