@@ -118,7 +118,6 @@ __device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const 
     using V = typename Vec<T>::type;
     constexpr int VN = Vec<T>::n;
     constexpr int GL = R / VN;
-    constexpr int GPW = 32 / GL;
     static_assert(GL >= 1 && 32 % GL == 0, "lanes per nonzero");
     const int lane = threadIdx.x & 31;
     const int gl = lane % GL, gw = lane / GL;
@@ -126,7 +125,9 @@ __device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const 
     // group gw takes the GL consecutive records gw*GL .. gw*GL+GL-1 of the
     // 32, so in a copy sorted by (mode 0, mode 1) it mostly sees one mode-0
     // row, and runs of one mode-1 row inside it: each row's slice stays in
-    // registers until its index changes
+    // registers until its index changes.  (Gathering for four records before
+    // using any -- more loads in flight, 80 registers -- measured slower:
+    // 2.61 against 2.11 ms per evaluation of the 100M workload.)
     uint32_t cur0 = 0xffffffffu, cur1 = 0xffffffffu;
     V va{}, vb{};
     for (uint64_t base = first; base < end; base += stride) {
@@ -783,6 +784,25 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
         if constexpr (FIRST) return sc[q] ? sc[q][i] : cols.pk[q][i];
         else return sc[q] ? sc[q][i] : __ldg(cols.col[q] + i);
     };
+    // Later sweeps: the gathers of EC entries e0 .. e0+EC-1 are all issued
+    // before any of them is used (h = product of the other two modes'
+    // column f); entries past the lane's count, and pads, read index 0 (in
+    // bounds) and are skipped by the walk.  First sweeps gather each entry's
+    // packs where the walk uses them: holding three products per entry
+    // spilled registers there (measured on the 100M workload, tile 256:
+    // first sweeps 525-529 us with 1-4 entries ahead against 496 us; later
+    // sweeps 268 us with 4 ahead, 354 us with 8, 301 us with none).
+    constexpr int EC = FIRST ? 1 : (E < 4 ? E : 4);
+    auto gather = [&](int e0, const uint64_t(&kv)[E], int cnt, T(&h)[EC]) {
+#pragma unroll
+        for (int k = 0; k < EC; ++k) {
+            const int e = e0 + k;
+            uint32_t row, q1, q2;
+            unpack_key(kv[e], ks, row, q1, q2);
+            if (e >= cnt || kv[e] == kPadKey) q1 = q2 = 0u;
+            if constexpr (!FIRST) h[k] = gat(0, q1) * gat(1, q2);
+        }
+    };
 
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -808,22 +828,28 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
                 const uint64_t base = (uint64_t)(td.x + j) * (uint64_t)(32 * E);
                 ccdpp_load_slot<T, E, PK>(keys, res, base, lane, ks.rbits, kv, rv);
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    if (kv[e] != kPadKey) {
-                        uint32_t rr, q1, q2;
-                        unpack_key(kv[e], ks, rr, q1, q2);
-                        T r = rv[e];
-                        T h;
-                        if constexpr (FIRST) {
-                            const Pack3<T> ga = gat(0, q1), gb = gat(1, q2);
-                            r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
-                            rv[e] = r;
-                            h = ga.cur * gb.cur;
-                        } else {
-                            h = gat(0, q1) * gat(1, q2);
+                for (int e0 = 0; e0 < E; e0 += EC) {
+                    T h[EC];
+                    gather(e0, kv, E, h);
+#pragma unroll
+                    for (int k = 0; k < EC; ++k) {
+                        const int e = e0 + k;
+                        if (kv[e] != kPadKey) {
+                            T r = rv[e];
+                            T hh;
+                            if constexpr (FIRST) {
+                                uint32_t rr, q1, q2;
+                                unpack_key(kv[e], ks, rr, q1, q2);
+                                const Pack3<T> ga = gat(0, q1), gb = gat(1, q2);
+                                r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
+                                rv[e] = r;
+                                hh = ga.cur * gb.cur;
+                            } else {
+                                hh = h[k];
+                            }
+                            nu += r * hh;
+                            de += hh * hh;
                         }
-                        nu += r * h;
-                        de += h * h;
                     }
                 }
                 if constexpr (FIRST) {
@@ -876,35 +902,41 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
         int nruns = 0;
         Pack3<T> pm{};
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            if (e < cnt) {
-                uint32_t row, q1, q2;
-                unpack_key(kv[e], ks, row, q1, q2);
-                if (row != tk) {
-                    if (nruns == 1) {
-                        hk = tk;
-                        hn = tn;
-                        hd = tdd;
-                    } else if (nruns >= 2) {
-                        ccdpp_finalize<T>(tk, tn, tdd, lambda, out, pkm);
+        for (int e0 = 0; e0 < E; e0 += EC) {
+            T h[EC];
+            gather(e0, kv, cnt, h);
+#pragma unroll
+            for (int k = 0; k < EC; ++k) {
+                const int e = e0 + k;
+                if (e < cnt) {
+                    uint32_t row, q1, q2;
+                    unpack_key(kv[e], ks, row, q1, q2);
+                    if (row != tk) {
+                        if (nruns == 1) {
+                            hk = tk;
+                            hn = tn;
+                            hd = tdd;
+                        } else if (nruns >= 2) {
+                            ccdpp_finalize<T>(tk, tn, tdd, lambda, out, pkm);
+                        }
+                        tk = row;
+                        tn = tdd = 0;
+                        ++nruns;
+                        if constexpr (FIRST) pm = pkm[row];
                     }
-                    tk = row;
-                    tn = tdd = 0;
-                    ++nruns;
-                    if constexpr (FIRST) pm = pkm[row];
+                    T r = rv[e];
+                    T hh;
+                    if constexpr (FIRST) {
+                        const Pack3<T> ga = gat(0, q1), gb = gat(1, q2);
+                        r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
+                        rv[e] = r;
+                        hh = ga.cur * gb.cur;
+                    } else {
+                        hh = h[k];
+                    }
+                    tn += r * hh;
+                    tdd += hh * hh;
                 }
-                T r = rv[e];
-                T h;
-                if constexpr (FIRST) {
-                    const Pack3<T> ga = gat(0, q1), gb = gat(1, q2);
-                    r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
-                    rv[e] = r;
-                    h = ga.cur * gb.cur;
-                } else {
-                    h = gat(0, q1) * gat(1, q2);
-                }
-                tn += r * h;
-                tdd += h * h;
             }
         }
         if constexpr (FIRST) ccdpp_store_slot<T, E, PK>(keys, res, base, lane, cnt, kv, rv, ks.rbits);
