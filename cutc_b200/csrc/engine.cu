@@ -1301,6 +1301,17 @@ static void run_loop(ctc_dataset *ds, SessionBase *S, ctc_model *model, ctc_mode
     }
 }
 
+// 16-byte slices of an FP32 row per lane (1, 2 or 4) of a Hogwild launch for
+// this rank and ctc_params.threads_per_row, as the SGD launch picks them
+static int sgd_vectors_for(int rank, int threads_per_row)
+{
+    const int base = rank / 4;
+    const int c = threads_per_row > 0 ? base / threads_per_row : 1;
+    if (c >= 4 && base % 4 == 0) return 4;
+    if (c >= 2 && base % 2 == 0) return 2;
+    return 1;
+}
+
 static void check_params(const ctc_params *p)
 {
     if (!p) fail(CTC_E_ARG, "null params");
@@ -1320,10 +1331,14 @@ static void check_params(const ctc_params *p)
     if (p->alg == CTC_ALG_SGD && p->sgd_atomic == 3 && p->precision == CTC_PREC_F64)
         fail(CTC_E_UNSUP, "sgd_atomic 3 (block-merged hot rows) is FP32 only");
     const int tpb = p->threads_per_block;
-    if (tpb < 0 || (tpb & (tpb - 1)) != 0 || tpb > 512)
-        fail(CTC_E_ARG, "threads_per_block %d: 0 or a power of two up to 512", tpb);
+    if (tpb < 0 || (tpb & (tpb - 1)) != 0 || tpb > 1024)
+        fail(CTC_E_ARG, "threads_per_block %d: 0 or a power of two up to 1024", tpb);
     if (tpb > 0 && tpb < 32)
         fail(CTC_E_UNSUP, "threads_per_block %d: SGD blocks are whole warps here (32 to 512 threads)", tpb);
+    if (tpb == 1024 && (p->sgd_atomic != 3 || p->sgd_order == CTC_SGD_SEQUENTIAL ||
+                        sgd_vectors_for(p->rank, p->threads_per_row) > 2))
+        fail(CTC_E_UNSUP, "threads_per_block 1024: block-merged hot-row SGD (sgd_atomic 3) with "
+                          "threads_per_row >= rank / 8 only");
 }
 
 static void check_model(const ctc_dataset *d, const ctc_model *model, int rank)
@@ -2247,8 +2262,10 @@ extern "C" int ctc_autotune(ctc_ctx *ctx, const ctc_tensor *const train[3], cons
                 // Hogwild SGD: the block size (the reference GA's other gene)
                 // around this tile length's fastest candidate
                 if (q.alg == CTC_ALG_SGD && q.sgd_order == CTC_SGD_HOGWILD)
-                    for (int b : {128, 512}) {
+                    for (int b : {128, 512, 1024}) {
                         TuneCand c = tile_best;
+                        if (b == 1024 && (c.sgd_atomic != 3 || sgd_vectors_for(q.rank, c.threads_per_row) > 2))
+                            continue;
                         c.threads_per_block = b;
                         const double per = trial(c);
                         if (per < tile_ms) {

@@ -447,8 +447,10 @@ __global__ void __launch_bounds__(512) k_sgd(const uint4 *__restrict__ rec,
 constexpr int kSgdHot = 32;          // hot rows per mode
 constexpr uint32_t kSgdCold = 1023u; // slot code of a row that is not hot
 
+// 1024-thread blocks for one or two 16-byte slices per lane (at most 64
+// registers), 512 for four
 template <int R, int C>
-__global__ void __launch_bounds__(512) k_sgd_hot(const uint4 *__restrict__ rec, const uint32_t *__restrict__ hot,
+__global__ void __launch_bounds__(C <= 2 ? 1024 : 512) k_sgd_hot(const uint4 *__restrict__ rec, const uint32_t *__restrict__ hot,
                                                  uint32_t n, uint32_t tile_len, uint32_t ntiles, float *U0,
                                                  float *U1, float *U2, const float *__restrict__ lr_dev, float lambda,
                                                  uint64_t tile_stride, const float *__restrict__ damp0,

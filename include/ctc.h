@@ -232,7 +232,10 @@ typedef struct {
                               block-size gene (ga/sgd.cu:66-78, fitness.c:67-75:
                               2^(2..9)): 32, 64, 128, 256 or 512; 0 = 256 (an
                               autotuner axis).  4-16 are rejected (CTC_E_UNSUP:
-                              a block is whole warps here).  The other
+                              a block is whole warps here).  1024 is accepted
+                              for sgd_atomic 3 when a lane holds at most two
+                              16-byte slices of a row (threads_per_row >=
+                              rank / 8), else CTC_E_UNSUP.  The other
                               algorithms' kernels have fixed block shapes and do
                               not read it                                        */
     int precision;         /* enum ctc_precision                                    */

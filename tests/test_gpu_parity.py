@@ -282,15 +282,16 @@ def test_sgd_hogwild_final_rmse(ctx, atomic, R):
     assert abs(out.epochs[-1]["rmse_te"] - hist[-1][1]) / hist[-1][1] < 0.005
 
 
-@pytest.mark.parametrize("block", [32, 128, 512])
-def test_sgd_hogwild_block_size(ctx, block):
+@pytest.mark.parametrize("block,atomic,tpr", [(32, 2, 0), (128, 2, 0), (512, 2, 0), (1024, 3, 8), (1024, 3, 4)])
+def test_sgd_hogwild_block_size(ctx, block, atomic, tpr):
     """ctc_params.threads_per_block (the reference GA's block-size gene)
     sets the Hogwild launch; every block size stays within 0.5 % of the
-    sequential order."""
+    sequential order (1024-thread blocks: the block-merged hot-row form,
+    one or two 16-byte slices per lane)."""
     P = Problem(200000, (2000, 1500, 200), 32, seed=13)
     U, hist = oracle_sgd(P, 10, 0.01, 0.01, decay=0.95)
     G, out = engine_run(ctx, P, ctc.SGD, 10, precision=ctc.PREC_F32, sgd_order=ctc.SGD_HOGWILD,
-                        sgd_atomic=2, threads_per_block=block, lr=0.01, lr_scale=1.0,
+                        sgd_atomic=atomic, threads_per_block=block, threads_per_row=tpr, lr=0.01, lr_scale=1.0,
                         lr_schedule=ctc.LR_EXP_DECAY, lr_decay=0.95, **{"lambda": 0.01})
     assert abs(out.epochs[-1]["rmse_te"] - hist[-1][1]) / hist[-1][1] < 0.005
 

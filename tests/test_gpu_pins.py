@@ -82,15 +82,25 @@ def zipf2m_oracle(zipf2m):
     return po.rmse(D.o(D.test), U, nthreads=8), po.rmse(T, U, nthreads=8)
 
 
-@pytest.mark.parametrize("atomic", [1, 2, 3])
-def test_sgd_hogwild_damped_on_zipf_matches_sequential_oracle(ctx, zipf2m, zipf2m_oracle, atomic):
+@pytest.mark.parametrize("atomic,block,tile,tpr,groups",
+                         [(1, 0, 0, 0, 0), (2, 0, 0, 0, 0), (3, 0, 0, 0, 0), (3, 1024, 0, 8, 0), (3, 1024, 128, 8, 384)])
+def test_sgd_hogwild_damped_on_zipf_matches_sequential_oracle(ctx, zipf2m, zipf2m_oracle, atomic, block, tile,
+                                                             tpr, groups):
     """The benchmarked Hogwild form: per-row damping at its default bound
     (rows whose expected in-flight updates exceed 128 take proportionally
     smaller steps; on this sample the hottest rows of modes 2 and 3 are
-    damped), lr 1e-3 x 0.95 per epoch, lambda 0.01, 20 epochs."""
+    damped), lr 1e-3 x 0.95 per epoch, lambda 0.01, 20 epochs; each
+    reduction mode at the library's launch shape, the hot-row form in
+    1024-thread blocks, and the shape the autotuner picks on the 100M tensor
+    (1024-thread blocks, 128-nonzero tiles, 8 lanes a nonzero) at that
+    tensor's concurrency: there one block per SM keeps 148 x 128 = 18,944 of
+    703,000 tiles (2.7 %) in flight, while on this 2M sample the same launch
+    would run all 15,600 tiles at once (1.2 % off the oracle, at any block
+    size), so the groups in flight are capped at 384 (2.5 %)."""
     D = zipf2m
     p = ctc.params("sgd", rank=32, iters=20, lr=1e-3, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY,
                    lr_decay=0.95, sgd_order=ctc.SGD_HOGWILD, sgd_atomic=atomic, early_stop=0, eval_every=0,
+                   threads_per_block=block, tile_len=tile, threads_per_row=tpr, sgd_groups=groups,
                    **{"lambda": 0.01})
     m = D.model()
     out = ctc.run(ctx, [D.c(D.train)], None, D.c(D.test), m, p)

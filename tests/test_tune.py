@@ -48,13 +48,20 @@ def test_lookup_hit_miss_and_last_entry_wins(tmp_path):
 
 def test_block_size_is_validated_on_the_host():
     """threads_per_block: 0 or a power of two up to 512; the reference GA's
-    4-16 thread blocks are below a warp and rejected as unsupported.  The
-    checks run before any device is touched."""
+    4-16 thread blocks are below a warp and rejected as unsupported; 1024
+    only for the block-merged hot-row form with at most two 16-byte slices
+    per lane.  The checks run before any device is touched."""
     import ctypes as C
     L = ctc.lib()
     for ok in (0, 32, 64, 128, 256, 512):
         assert L.ctc_params_check(C.byref(ctc.params(ctc.SGD, rank=16, threads_per_block=ok))) == 0
-    for bad, code in ((100, -1), (1024, -1), (-32, -1), (16, -5), (4, -5)):
+    for bad, code in ((100, -1), (2048, -1), (-32, -1), (16, -5), (4, -5), (1024, -5)):
         p = ctc.params(ctc.SGD, rank=16, threads_per_block=bad)
         assert L.ctc_params_check(C.byref(p)) == code, bad
         assert b"threads_per_block" in L.ctc_last_error()
+    # rank 32: 8 lanes a nonzero hold one slice each, 4 lanes two, 2 lanes four
+    for tpr, code in ((8, 0), (4, 0), (0, 0), (2, -5)):
+        p = ctc.params(ctc.SGD, rank=32, threads_per_block=1024, sgd_atomic=3, threads_per_row=tpr)
+        assert L.ctc_params_check(C.byref(p)) == code, tpr
+    p = ctc.params(ctc.SGD, rank=32, threads_per_block=1024, sgd_atomic=1)
+    assert L.ctc_params_check(C.byref(p)) == -5
