@@ -668,6 +668,7 @@ struct Session : SessionBase {
     // and the rows of the slots, mode-major
     DevBuf<uint32_t> hot_codes, hot_rows;
     bool hot_ready = false;
+    bool eager_done = false;  // the session's first epoch ran without a graph
     void prepare_hot()
     {
         hot_ready = true;
@@ -1110,17 +1111,31 @@ struct Session : SessionBase {
     void epochs(int n) override
     {
         if (!model_set) fail(CTC_E_ARG, "no model staged on the dataset");
-        if (p.alg == CTC_ALG_SGD && !damp_ready) prepare_damping(sgd_groups_per_block());
+        if (p.alg == CTC_ALG_SGD && !damp_ready) {
+            TracePhase tp("SGD damping");
+            prepare_damping(sgd_groups_per_block());
+        }
         if constexpr (std::is_same<T, float>::value)
-            if (p.alg == CTC_ALG_SGD && p.sgd_atomic == 3 && p.sgd_order != CTC_SGD_SEQUENTIAL && !hot_ready)
+            if (p.alg == CTC_ALG_SGD && p.sgd_atomic == 3 && p.sgd_order != CTC_SGD_SEQUENTIAL && !hot_ready) {
+                TracePhase tp("SGD hot rows");
                 prepare_hot();
+            }
         const bool use_graph = p.use_graph && !ctx->kt.on && p.sgd_order != CTC_SGD_SEQUENTIAL;
         for (int i = 0; i < n; ++i) {
             if (!use_graph) {
                 one_epoch();
                 continue;
             }
+            // the first epoch of a session runs its launches directly: a
+            // single-epoch run (the reference-shaped ctc_run) does not pay
+            // for capturing and instantiating a graph it would launch once
+            if (!graph && !eager_done) {
+                eager_done = true;
+                one_epoch();
+                continue;
+            }
             if (!graph) {
+                TracePhase tp("epoch graph capture");
                 cudaGraph_t g = nullptr;
                 ctx->capturing = true;
                 CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
