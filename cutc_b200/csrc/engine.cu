@@ -537,6 +537,11 @@ struct Session : SessionBase {
     DevBuf<T> U[3], Ubest[3], Urow[3], slot, slot2, lr_dev;
     DevBuf<k::Pack3<T>> pk[3];  // CCD++ per-column {cur, prev, old}
     DevBuf<unsigned int> hcnt[3];  // CCD++ pieces arrived per heavy row (reset by the finaliser)
+    // CCD++ task claim counters: pass k claims from claim[k % 2] and zeroes
+    // the other for pass k + 1 (an epoch has an even number of passes, so a
+    // captured epoch replays with the same parities)
+    DevBuf<unsigned int> claim;
+    unsigned claim_pass = 0;
     // mixed-precision ALS at rank 64: BF16 copies of the factors feed the
     // tensor-core Gram of long-row pieces; err flags an expired bounded wait
     bool tc = false;
@@ -569,6 +574,10 @@ struct Session : SessionBase {
                 hcnt[m].alloc(D->copy[m].nheavy);
                 CK(cudaMemsetAsync(hcnt[m].p, 0, hcnt[m].n * sizeof(unsigned int), ctx->stream));
             }
+        }
+        if (colmajor) {
+            claim.alloc(2);
+            CK(cudaMemsetAsync(claim.p, 0, 2 * sizeof(unsigned int), ctx->stream));
         }
         // scratch sized once so an epoch can be captured as a graph
         size_t need = 1;
@@ -1042,14 +1051,15 @@ struct Session : SessionBase {
     void ccdpp_launch(DevTensor<T> &c, bool first, unsigned g, size_t smem, const k::CcdppCols<T> &cols, T *out,
                       int m)
     {
+        const int cs = (int)(claim_pass++ & 1u);
         if (first)
             LAUNCH(ctx, (k::k_ccdpp_pass<T, true, E, PK>), g, 512, smem, (const int4 *)c.tasks.p, c.ntasks, c.keys.p,
                    c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p, (const uint4 *)c.heavy.p,
-                   hcnt[m].p, dev_err.p);
+                   hcnt[m].p, dev_err.p, claim.p, cs);
         else
             LAUNCH(ctx, (k::k_ccdpp_pass<T, false, E, PK>), g, 512, smem, (const int4 *)c.tasks.p, c.ntasks,
                    c.keys.p, c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p,
-                   (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p);
+                   (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p, claim.p, cs);
     }
 
     // One CCD++ outer iteration: per column f, the {cur, prev, old} packs,

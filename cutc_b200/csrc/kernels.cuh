@@ -737,8 +737,12 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
                                                        uint64_t *__restrict__ keys, T *__restrict__ res,
                                                        KeyShape ks, Pack3<T> *pkm, CcdppCols<T> cols, T *out,
                                                        T lambda, T *__restrict__ slot_nu, T *__restrict__ slot_de,
-                                                       const uint4 *__restrict__ heavy, unsigned int *hcnt, int *err)
+                                                       const uint4 *__restrict__ heavy, unsigned int *hcnt, int *err,
+                                                       unsigned int *claim_ctr, int claim_slot)
 {
+    // the other claim counter was this pass's predecessor's: zero it for the
+    // pass after this one (passes on one stream never overlap)
+    if (blockIdx.x == 0 && threadIdx.x == 0) claim_ctr[claim_slot ^ 1] = 0u;
     using ColT = typename std::conditional<FIRST, Pack3<T>, T>::type;
     constexpr uint32_t kNone = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char ccdpp_smem[];
@@ -806,15 +810,31 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
         }
     };
 
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     // tasks: {tile, len, -1, 0} for a light tile, {first tile, pieces,
     // heavy row, group} for up to kCcdppGroup consecutive pieces of one long
-    // row; the next task's descriptor is fetched while this one runs
-    int4 td_next = warp < ntasks ? tasks[warp] : make_int4(0, 0, -1, 0);
-    for (uint64_t task = warp; task < ntasks; task += nwarps) {
-        const int4 td = td_next;
-        if (task + nwarps < ntasks) td_next = tasks[task + nwarps];
+    // row.  A warp claims its tasks one at a time from the pass's counter,
+    // so warps that drew short tasks take more (a long-row group runs up to
+    // kCcdppGroup times a light tile); the task after the current one is
+    // claimed, and its descriptor fetched, while the current one runs.
+    const int4 kNoTask = make_int4(0, 0, -1, 0);
+    auto claim = [&]() -> uint32_t {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(claim_ctr + claim_slot, 1u);
+        return __shfl_sync(0xffffffffu, t, 0);
+    };
+    uint32_t cur_i = claim();
+    int4 td_cur = cur_i < ntasks ? tasks[cur_i] : kNoTask;
+    uint32_t nxt_i = cur_i < ntasks ? claim() : ntasks;
+    int4 td_nxt = nxt_i < ntasks ? tasks[nxt_i] : kNoTask;
+    while (cur_i < ntasks) {
+        const int4 td = td_cur;
+        // advance first (the task bodies below end with `continue`)
+        cur_i = nxt_i;
+        td_cur = td_nxt;
+        if (cur_i < ntasks) {
+            nxt_i = claim();
+            if (nxt_i < ntasks) td_nxt = tasks[nxt_i];
+        }
         uint64_t kv[E];
         T rv[E];
         if (td.z >= 0) {
