@@ -537,11 +537,9 @@ struct Session : SessionBase {
     DevBuf<T> U[3], Ubest[3], Urow[3], slot, slot2, lr_dev;
     DevBuf<k::Pack3<T>> pk[3];  // CCD++ per-column {cur, prev, old}
     DevBuf<unsigned int> hcnt[3];  // CCD++ pieces arrived per heavy row (reset by the finaliser)
-    // CCD++ task claim counters: pass k claims from claim[k % 2] and zeroes
-    // the other for pass k + 1 (an epoch has an even number of passes, so a
-    // captured epoch replays with the same parities)
+    // {next, done} task claim counters of the kernels that claim their warp
+    // tasks (k::TaskClaim); every launch leaves them at zero
     DevBuf<unsigned int> claim;
-    unsigned claim_pass = 0;
     // mixed-precision ALS at rank 64: BF16 copies of the factors feed the
     // tensor-core Gram of long-row pieces; err flags an expired bounded wait
     bool tc = false;
@@ -575,10 +573,8 @@ struct Session : SessionBase {
                 CK(cudaMemsetAsync(hcnt[m].p, 0, hcnt[m].n * sizeof(unsigned int), ctx->stream));
             }
         }
-        if (colmajor) {
-            claim.alloc(2);
-            CK(cudaMemsetAsync(claim.p, 0, 2 * sizeof(unsigned int), ctx->stream));
-        }
+        claim.alloc(2);
+        CK(cudaMemsetAsync(claim.p, 0, 2 * sizeof(unsigned int), ctx->stream));
         // scratch sized once so an epoch can be captured as a graph
         size_t need = 1;
         for (int m = 0; m < 3; ++m) {
@@ -843,7 +839,7 @@ struct Session : SessionBase {
                    4 * k::AlsBatch<T, R>::warp_doubles * sizeof(double), (const int4 *)c.tiles.p,
                    c.ntiles, (const uint4 *)c.rec.p, (const double *)c.v64.p,
                    (const T *)(c.has_w ? c.w.p : nullptr), m, U[m].p, (const T *)U[m1].p, (const T *)U[m2].p,
-                   (T)p.lambda, slot.p, nonspd_dev.p, tc ? 1 : 0);
+                   (T)p.lambda, slot.p, nonspd_dev.p, tc ? 1 : 0, k::TaskClaim{claim.p});
             if (tc && c.npieces) als_gram_tc(c, m);
             if (c.nheavy) {
                 // pieces summed element-parallel first; the solve reads one slot per row
@@ -1051,15 +1047,14 @@ struct Session : SessionBase {
     void ccdpp_launch(DevTensor<T> &c, bool first, unsigned g, size_t smem, const k::CcdppCols<T> &cols, T *out,
                       int m)
     {
-        const int cs = (int)(claim_pass++ & 1u);
         if (first)
             LAUNCH(ctx, (k::k_ccdpp_pass<T, true, E, PK>), g, 512, smem, (const int4 *)c.tasks.p, c.ntasks, c.keys.p,
                    c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p, (const uint4 *)c.heavy.p,
-                   hcnt[m].p, dev_err.p, claim.p, cs);
+                   hcnt[m].p, dev_err.p, k::TaskClaim{claim.p});
         else
             LAUNCH(ctx, (k::k_ccdpp_pass<T, false, E, PK>), g, 512, smem, (const int4 *)c.tasks.p, c.ntasks,
                    c.keys.p, c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p,
-                   (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p, claim.p, cs);
+                   (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p, k::TaskClaim{claim.p});
     }
 
     // One CCD++ outer iteration: per column f, the {cur, prev, old} packs,

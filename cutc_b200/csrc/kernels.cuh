@@ -83,6 +83,34 @@ __device__ __forceinline__ void vatomic_add(double2 *p, const double2 &d)
     atomicAdd(&p->y, d.y);
 }
 
+// Warp tasks claimed one at a time from a counter pair {next, done} that
+// every launch leaves at zero: a warp claims indices until it draws one past
+// the end, then counts itself done, and the last warp of the grid to finish
+// zeroes both for the next launch on the stream.  Every warp of the grid
+// calls finish() exactly once.  Warps that drew short tasks thus take more,
+// where a fixed stride would leave the grid waiting on the unluckiest warp.
+struct TaskClaim {
+    unsigned int *ctr;
+    __device__ __forceinline__ uint32_t next(int lane) const
+    {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(ctr, 1u);
+        return __shfl_sync(0xffffffffu, t, 0);
+    }
+    __device__ __forceinline__ void finish(int lane) const
+    {
+        if (lane == 0) {
+            const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+            __threadfence();  // this warp's claims come before its count
+            if (atomicAdd(ctr + 1, 1u) == nwarps - 1u) {
+                __threadfence();
+                ctr[0] = 0u;
+                ctr[1] = 0u;
+            }
+        }
+    }
+};
+
 // Block-wide double sum; result valid in thread 0.
 __device__ __forceinline__ double block_sum(double v)
 {
@@ -738,11 +766,8 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
                                                        KeyShape ks, Pack3<T> *pkm, CcdppCols<T> cols, T *out,
                                                        T lambda, T *__restrict__ slot_nu, T *__restrict__ slot_de,
                                                        const uint4 *__restrict__ heavy, unsigned int *hcnt, int *err,
-                                                       unsigned int *claim_ctr, int claim_slot)
+                                                       TaskClaim claim)
 {
-    // the other claim counter was this pass's predecessor's: zero it for the
-    // pass after this one (passes on one stream never overlap)
-    if (blockIdx.x == 0 && threadIdx.x == 0) claim_ctr[claim_slot ^ 1] = 0u;
     using ColT = typename std::conditional<FIRST, Pack3<T>, T>::type;
     constexpr uint32_t kNone = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char ccdpp_smem[];
@@ -783,6 +808,7 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
                 px::mbar_wait_bounded(px::smem_u32(&mbar), 0);
             }
             __syncthreads();
+            claim.finish(lane);  // every warp still counts itself done
             return;
         }
     }
@@ -812,19 +838,14 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
 
     // tasks: {tile, len, -1, 0} for a light tile, {first tile, pieces,
     // heavy row, group} for up to kCcdppGroup consecutive pieces of one long
-    // row.  A warp claims its tasks one at a time from the pass's counter,
-    // so warps that drew short tasks take more (a long-row group runs up to
-    // kCcdppGroup times a light tile); the task after the current one is
-    // claimed, and its descriptor fetched, while the current one runs.
+    // row.  A warp claims its tasks one at a time (TaskClaim), so warps that
+    // drew short tasks take more (a long-row group runs up to kCcdppGroup
+    // times a light tile); the task after the current one is claimed, and
+    // its descriptor fetched, while the current one runs.
     const int4 kNoTask = make_int4(0, 0, -1, 0);
-    auto claim = [&]() -> uint32_t {
-        uint32_t t = 0;
-        if (lane == 0) t = atomicAdd(claim_ctr + claim_slot, 1u);
-        return __shfl_sync(0xffffffffu, t, 0);
-    };
-    uint32_t cur_i = claim();
+    uint32_t cur_i = claim.next(lane);
     int4 td_cur = cur_i < ntasks ? tasks[cur_i] : kNoTask;
-    uint32_t nxt_i = cur_i < ntasks ? claim() : ntasks;
+    uint32_t nxt_i = cur_i < ntasks ? claim.next(lane) : ntasks;
     int4 td_nxt = nxt_i < ntasks ? tasks[nxt_i] : kNoTask;
     while (cur_i < ntasks) {
         const int4 td = td_cur;
@@ -832,7 +853,7 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
         cur_i = nxt_i;
         td_cur = td_nxt;
         if (cur_i < ntasks) {
-            nxt_i = claim();
+            nxt_i = claim.next(lane);
             if (nxt_i < ntasks) td_nxt = tasks[nxt_i];
         }
         uint64_t kv[E];
@@ -995,6 +1016,7 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
         }
         if (nruns >= 1 && next_in != out_key) ccdpp_finalize<T>(out_key, sn, sd, lambda, out, pkm);
     }
+    claim.finish(lane);
 }
 
 // pack[n][row] = {U_n(row, f), U_n(row, f-1) or 0, U_n(row, f), 0} for the
@@ -1715,7 +1737,7 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
                                                   const T *__restrict__ Ua,
                                                   const T *__restrict__ Ub, T lambda,
                                                   T *__restrict__ slot,
-                                                  unsigned long long *nonspd, int skip_heavy)
+                                                  unsigned long long *nonspd, int skip_heavy, TaskClaim claim)
 {
     using Sh = AlsShape<R>;
     using Bt = AlsBatch<T, R>;
@@ -1724,14 +1746,14 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     double *W = smem + (size_t)wib * Bt::warp_doubles;
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const int gl = lane % L;
     int bad = 0, parked = 0;
     const bool short_rows = w == nullptr && lambda > T(0);
     T G[R][C];
     T b[C];
-    for (uint64_t tile = warp; tile < ntiles; tile += nwarps) {
+    // tiles claimed one at a time (TaskClaim): tiles of many short rows, or
+    // pieces that the tensor-core Gram takes, cost very different times
+    for (uint32_t tile = claim.next(lane); tile < ntiles; tile = claim.next(lane)) {
         const int4 td = tiles[tile];
         const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
         if (td.z >= 0) {
@@ -1782,6 +1804,7 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
     if (parked) bad += als_solve_parked<T, R>(W, parked, lambda, Um);
     bad = __reduce_add_sync(0xffffffffu, bad);
     if (lane == 0 && bad) atomicAdd(nonspd, (unsigned long long)bad);
+    claim.finish(lane);
 }
 
 // Sum of each long row's piece partials, element-parallel: thread per
