@@ -607,11 +607,10 @@ struct Session : SessionBase {
             set_sgd_smem<4>();
         }
         if (p.alg == CTC_ALG_ALS) {
-            using Sh = k::AlsShape<R>;
-            const int smem = (int)(4 * Sh::smem_doubles * sizeof(double));
+            // both kernels park one warp's systems per warp of a 4-warp block
             const int smem_tile = (int)(4 * k::AlsBatch<T, R>::warp_doubles * sizeof(double));
             CK(cudaFuncSetAttribute(k::k_als_tile<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_tile));
-            CK(cudaFuncSetAttribute(k::k_als_fix<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            CK(cudaFuncSetAttribute(k::k_als_fix<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_tile));
         }
         CK(cudaStreamSynchronize(ctx->stream));
     }
@@ -828,8 +827,7 @@ struct Session : SessionBase {
     // ---- epochs
     void als_epoch()
     {
-        using Sh = k::AlsShape<R>;
-        const size_t smem = 4 * Sh::smem_doubles * sizeof(double);
+        const size_t smem = 4 * k::AlsBatch<T, R>::warp_doubles * sizeof(double);
         for (int q = 0; q < 3; ++q) {
             const int m = (p.mode_start + q) % 3;
             const int m1 = (m + 1) % 3, m2 = (m + 2) % 3;

@@ -1284,96 +1284,10 @@ struct AlsShape {
     static constexpr int C = R <= 8 ? 2 : (R <= 16 ? 4 : 2);
     static constexpr int L = R / C;
     static constexpr int NG = 32 / L;
-    static constexpr int smem_doubles = R * R + 2 * R;  // per warp
 };
 
-// Solve (G + lambda I) u = b for the row held by group 0 of the warp.
-// G[a][c] is Gram column (gl + L*c), b[c] the right-hand side entries.
-// Returns 1 when a pivot was not positive (diagonal shifted).
-template <typename T, int R>
-__device__ __forceinline__ int als_solve_warp(const T (&G)[R][AlsShape<R>::C], const T (&b)[AlsShape<R>::C],
-                              T lambda, double *S, T *urow)
-{
-    using Sh = AlsShape<R>;
-    constexpr int L = Sh::L, C = Sh::C;
-    const int lane = threadIdx.x & 31;
-    const int gl = lane % L;
-    const bool g0 = lane < L;
-    double *y = S + R * R;
-    double *u = y + R;
-    if (g0) {
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            const int col = gl + L * c;
-#pragma unroll
-            for (int a = 0; a < R; ++a) S[a * R + col] = (double)G[a][c] + (a == col ? (double)lambda : 0.0);
-            y[col] = (double)b[c];
-        }
-    }
-    __syncwarp();
-    int bad = 0;
-    // right-looking Cholesky, lower triangle of S (row-major, S[i*R+k], k<=i)
-    for (int j = 0; j < R; ++j) {
-        double d = S[j * R + j];
-        if (!(d > 0.0)) {
-            bad = 1;
-            d = 1e-300 + fabs(d) + 1e-12 * (double)lambda + 1e-30;
-        }
-        const double ljj = sqrt(d);
-        __syncwarp();
-        if (lane == 0) S[j * R + j] = ljj;
-        for (int i = j + 1 + lane; i < R; i += 32) S[i * R + j] /= ljj;
-        __syncwarp();
-        for (int i = j + 1 + lane; i < R; i += 32) {
-            const double lij = S[i * R + j];
-            for (int k2 = j + 1; k2 <= i; ++k2) S[i * R + k2] -= lij * S[k2 * R + j];
-        }
-        __syncwarp();
-    }
-    // two solves: the solution, then one refinement step
-    for (int it = 0; it < 2; ++it) {
-        // forward: L z = y (in place in y)
-        for (int i = 0; i < R; ++i) {
-            const double zi = y[i] / S[i * R + i];
-            __syncwarp();
-            if (lane == 0) y[i] = zi;
-            for (int k2 = i + 1 + lane; k2 < R; k2 += 32) y[k2] -= S[k2 * R + i] * zi;
-            __syncwarp();
-        }
-        // backward: L^T v = z
-        for (int i = R - 1; i >= 0; --i) {
-            const double vi = y[i] / S[i * R + i];
-            __syncwarp();
-            if (lane == 0) y[i] = vi;
-            for (int k2 = lane; k2 < i; k2 += 32) y[k2] -= S[i * R + k2] * vi;
-            __syncwarp();
-        }
-        if (it == 0) {
-            for (int k2 = lane; k2 < R; k2 += 32) u[k2] = y[k2];
-            __syncwarp();
-            // residual b - (G + lambda I) u, from the register Gram (symmetric)
-            if (g0) {
-#pragma unroll
-                for (int c = 0; c < C; ++c) {
-                    const int col = gl + L * c;
-                    double acc = (double)b[c] - (double)lambda * u[col];
-#pragma unroll
-                    for (int a = 0; a < R; ++a) acc -= (double)G[a][c] * u[a];
-                    y[col] = acc;
-                }
-            }
-            __syncwarp();
-        } else {
-            for (int k2 = lane; k2 < R; k2 += 32) u[k2] += y[k2];
-            __syncwarp();
-        }
-    }
-    for (int k2 = lane; k2 < R; k2 += 32) urow[k2] = (T)u[k2];
-    __syncwarp();
-    return bad;
-}
-
-// Batched row solves of the light tiles: a warp parks the regularised
+// Batched row solves (the light tiles' rows, and the long rows after their
+// pieces are summed): a warp parks the regularised
 // systems of NS rows in shared memory and factors them together, one group
 // of GS lanes per system (FP64 right-looking Cholesky on the packed lower
 // triangle, forward/back substitution, one refinement step against the
@@ -1829,22 +1743,27 @@ __global__ void __launch_bounds__(256) k_als_sum_pieces(const uint4 *__restrict_
     }
 }
 
-// summed != 0: the pieces were already summed into each row's first slot
+// summed != 0: the pieces were already summed into each row's first slot.
+// The rows' systems are solved like the light tiles' (parked, packed lower
+// triangle, columns owned across the lanes): a row-major system with one
+// row per lane put every lane of a column step on the same shared-memory
+// bank at rank 32.
 template <typename T, int R>
 __global__ void __launch_bounds__(128) k_als_fix(const uint4 *__restrict__ heavy, uint32_t nheavy,
                                                  const T *__restrict__ slot, T *Um, T lambda,
                                                  unsigned long long *nonspd, int summed)
 {
     using Sh = AlsShape<R>;
+    using Bt = AlsBatch<T, R>;
     constexpr int L = Sh::L, C = Sh::C;
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    double *S = smem + (size_t)wib * Sh::smem_doubles;
+    double *W = smem + (size_t)wib * Bt::warp_doubles;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const int gl = lane % L;
-    int bad = 0;
+    int bad = 0, parked = 0;
     T G[R][C];
     T b[C];
     for (uint64_t h = warp; h < nheavy; h += nwarps) {
@@ -1866,8 +1785,14 @@ __global__ void __launch_bounds__(128) k_als_fix(const uint4 *__restrict__ heavy
                 b[c] += src[R * R + col];
             }
         }
-        bad += als_solve_warp<T, R>(G, b, lambda, S, Um + (size_t)hr.x * R);
+        als_park<T, R>(W, parked, hr.x, G, b, lambda);
+        if (++parked == Bt::NS) {
+            bad += als_solve_parked<T, R>(W, parked, lambda, Um);
+            parked = 0;
+        }
     }
+    if (parked) bad += als_solve_parked<T, R>(W, parked, lambda, Um);
+    bad = __reduce_add_sync(0xffffffffu, bad);
     if (lane == 0 && bad) atomicAdd(nonspd, (unsigned long long)bad);
 }
 
