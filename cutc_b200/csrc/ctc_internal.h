@@ -58,7 +58,10 @@ struct TilePlan {
     uint32_t nheavy() const { return (uint32_t)(heavy_rows.size() / 4); }
 };
 TilePlan plan_tiles_chunked(const uint64_t *ind, uint64_t n, uint32_t tile_len, bool *unsorted);
-TilePlan plan_tiles_runs(const uint32_t *rows, const uint32_t *counts, uint64_t nruns, uint32_t tile_len);
+// heavy_min: rows longer than this get tiles of their own (pieces of at
+// most tile_len); 0 means tile_len, the planners' common rule
+TilePlan plan_tiles_runs(const uint32_t *rows, const uint32_t *counts, uint64_t nruns, uint32_t tile_len,
+                         uint32_t heavy_min = 0);
 
 // FP64 gradient of the masked CP loss for order-3/4 tensors (fo.cu)
 void ctc_grad_fo(ctc_ctx *ctx, const ctc_tensor *t, const ctc_model *model, double lambda, double *const *grads,

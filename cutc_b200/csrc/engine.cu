@@ -387,6 +387,13 @@ static int default_tile(int alg)
 // come back to the host for the tile plan (plan_tiles_runs: the plan of the
 // host planner), and the CCD++ slots or the record copy are gathered on
 // the device.
+// Mixed ALS: the row length above which a row takes tiles of its own and a
+// tensor-core Gram, below the tile length that packs the light rows (on the
+// 100M rank-32 tensor, tile 1024: 21.1 ms per iteration with the tile
+// length as the threshold, 20.2 / 19.7 / 19.7 ms with 512 / 256 / 128, test
+// RMSE after 10 iterations 0.2934-0.2939 against 0.2940 in FP32; every row
+// above R/2 nonzeros moved the factors 0.25 from the oracle on a 2M sample)
+constexpr uint32_t kMixedHeavyMin = 256;
 template <typename T>
 static void stage_copies_dev(ctc_ctx *ctx, const ctc_params &p, uint32_t tl, const ctc_tensor *const train[3],
                              const uint64_t *dims, bool trunc, DatasetImpl<T> &impl)
@@ -443,7 +450,11 @@ static void stage_copies_dev(ctc_ctx *ctx, const ctc_params &p, uint32_t tl, con
             std::vector<uint32_t> rows, counts;
             if (dev_row_runs(ctx, src->rec.p, pp, (uint32_t)n, m, rows, counts))
                 fail(CTC_E_ARG, "training tensor %d is not sorted for mode %d", m + 1, m + 1);
-            plan = plan_tiles_runs(rows.data(), counts.data(), rows.size(), tl);
+            // mixed ALS: rows longer than kMixedHeavyMin get tiles of their
+            // own, whose Grams the tensor cores form
+            const bool tc_rows = p.alg == CTC_ALG_ALS && p.precision == CTC_PREC_MIXED &&
+                                 (p.rank == 32 || p.rank == 64) && p.compat == 0;
+            plan = plan_tiles_runs(rows.data(), counts.data(), rows.size(), tl, tc_rows ? kMixedHeavyMin : 0u);
             upload_plan(ctx, plan, m, d);
         }
         if (ccdpp) {

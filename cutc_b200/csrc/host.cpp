@@ -781,9 +781,11 @@ TilePlan plan_tiles_chunked(const uint64_t *ind, uint64_t n, uint32_t T, bool *u
 // rows[r] repeated counts[r] times, in order): the chunk cut c is the first
 // run start at or after n*c/64 (a cut never precedes the one before it),
 // light tiles end at a cut, and tiles / heavy rows are numbered in order,
-// so the two builders give the same plan.  O(runs + tiles).
-TilePlan plan_tiles_runs(const uint32_t *rows, const uint32_t *counts, uint64_t nruns, uint32_t T)
+// so the two builders give the same plan.  O(runs + tiles).  Rows longer
+// than H (0: T) get tiles of their own, pieces of at most T nonzeros.
+TilePlan plan_tiles_runs(const uint32_t *rows, const uint32_t *counts, uint64_t nruns, uint32_t T, uint32_t H)
 {
+    if (H == 0 || H > T) H = T;
     std::vector<uint64_t> start(nruns + 1, 0);
     for (uint64_t r = 0; r < nruns; ++r) start[r + 1] = start[r] + counts[r];
     const uint64_t n = start[nruns];
@@ -802,7 +804,7 @@ TilePlan plan_tiles_runs(const uint32_t *rows, const uint32_t *counts, uint64_t 
         const uint64_t rend = cut[c + 1];
         while (r < rend) {
             const uint64_t len = counts[r];
-            if (len > T) {
+            if (len > H) {
                 const uint32_t h = p.nheavy(), first = p.ntiles();
                 const uint32_t np = (uint32_t)((len + T - 1) / T);
                 const uint64_t s0 = start[r], e = s0 + len;
@@ -819,7 +821,7 @@ TilePlan plan_tiles_runs(const uint32_t *rows, const uint32_t *counts, uint64_t 
             uint64_t size = 0;
             while (r < rend) {
                 const uint64_t l = counts[r];
-                if (l > T || size + l > T) break;
+                if (l > H || size + l > T) break;
                 size += l;
                 ++r;
             }
