@@ -1463,22 +1463,57 @@ __device__ __forceinline__ void als_accumulate(const uint4 *__restrict__ rec,
 #pragma unroll
         for (int a = 0; a < R; ++a) G[a][c] = 0;
     }
+    // a two-stage pipeline: while step k is multiplied in, the rows of step
+    // k + 1 (whose record came a step earlier) and the record of step k + 2
+    // are on their way
+    const uint4 kZero = make_uint4(0u, 0u, 0u, 0u);
+    uint4 r0 = s + g < e ? rec[s + g] : kZero;
+    uint4 r1 = s + g + NG < e ? rec[s + g + NG] : kZero;
+    T ua[C], ub[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) ua[c] = ub[c] = 0;
+    if (s + g < e) {
+        const T *ra = Ua + (size_t)key_of(r0, m1) * R;
+        const T *rb = Ub + (size_t)key_of(r0, m2) * R;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            ua[c] = ra[gl + L * c];
+            ub[c] = rb[gl + L * c];
+        }
+    }
     for (uint32_t base = s; base < e; base += NG) {
         const uint32_t p = base + g;
         const bool valid = p < e;
+        T na[C], nb[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) na[c] = nb[c] = 0;
+        if (p + NG < e) {
+            const T *ra = Ua + (size_t)key_of(r1, m1) * R;
+            const T *rb = Ub + (size_t)key_of(r1, m2) * R;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                na[c] = ra[gl + L * c];
+                nb[c] = rb[gl + L * c];
+            }
+        }
+        const uint4 r2 = p + 2 * NG < e ? rec[p + 2 * NG] : kZero;
         T hc[C], hw[C];
         T wx = 0, wn = 0;
         if (valid) {
-            const uint4 r = rec[p];
             wn = w ? w[p] : T(1);
-            wx = wn * value_of<T>(r, v64, p);
-            const T *ra = Ua + (size_t)key_of(r, m1) * R;
-            const T *rb = Ub + (size_t)key_of(r, m2) * R;
+            wx = wn * value_of<T>(r0, v64, p);
 #pragma unroll
-            for (int c = 0; c < C; ++c) hc[c] = ra[gl + L * c] * rb[gl + L * c];
+            for (int c = 0; c < C; ++c) hc[c] = ua[c] * ub[c];
         } else {
 #pragma unroll
             for (int c = 0; c < C; ++c) hc[c] = 0;
+        }
+        r0 = r1;
+        r1 = r2;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            ua[c] = na[c];
+            ub[c] = nb[c];
         }
 #pragma unroll
         for (int c = 0; c < C; ++c) {
