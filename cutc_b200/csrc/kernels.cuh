@@ -153,9 +153,9 @@ __device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const 
     // group gw takes the GL consecutive records gw*GL .. gw*GL+GL-1 of the
     // 32, so in a copy sorted by (mode 0, mode 1) it mostly sees one mode-0
     // row, and runs of one mode-1 row inside it: each row's slice stays in
-    // registers until its index changes.  (Gathering for four records before
-    // using any -- more loads in flight, 80 registers -- measured slower:
-    // 2.61 against 2.11 ms per evaluation of the 100M workload.)
+    // registers until its index changes.  One record ahead took an
+    // evaluation of the 100M workload from 2.11 to 2.02 ms; gathering for
+    // four records before using any (80 registers) was slower, 2.61 ms.
     uint32_t cur0 = 0xffffffffu, cur1 = 0xffffffffu;
     V va{}, vb{};
     for (uint64_t base = first; base < end; base += stride) {
@@ -167,25 +167,29 @@ __device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const 
             x = value_of<T>(r, v64, mine);
         }
         const uint64_t cnt = end - base;
-#pragma unroll 4
-        for (int j = 0; j < GL; ++j) {
-            const int src = gw * GL + j;
+        // one record ahead: the slices of record j + 1 are loaded while
+        // record j is multiplied
+        auto fetch = [&](int src, V &a, V &b, V &c) {
             const uint32_t i0 = __shfl_sync(0xffffffffu, r.x, src);
             const uint32_t i1 = __shfl_sync(0xffffffffu, r.y, src);
             const uint32_t i2 = __shfl_sync(0xffffffffu, r.z, src);
+            if (i0 != cur0) a = reinterpret_cast<const V *>(U0 + (size_t)i0 * R)[gl];
+            if (i1 != cur1) b = reinterpret_cast<const V *>(U1 + (size_t)i1 * R)[gl];
+            c = reinterpret_cast<const V *>(U2 + (size_t)i2 * R)[gl];
+            cur0 = i0;
+            cur1 = i1;
+        };
+        V na = va, nb = vb, nc;
+        fetch(gw * GL, na, nb, nc);
+#pragma unroll
+        for (int j = 0; j < GL; ++j) {
+            const int src = gw * GL + j;
             const T xv = __shfl_sync(0xffffffffu, x, src);
-            if (i0 != cur0) {
-                va = reinterpret_cast<const V *>(U0 + (size_t)i0 * R)[gl];
-                cur0 = i0;
-            }
-            if (i1 != cur1) {
-                vb = reinterpret_cast<const V *>(U1 + (size_t)i1 * R)[gl];
-                cur1 = i1;
-            }
-            const V vc = reinterpret_cast<const V *>(U2 + (size_t)i2 * R)[gl];
+            const V a = na, b = nb, c = nc;
+            if (j + 1 < GL) fetch(src + 1, na, nb, nc);
             T p = 0;
 #pragma unroll
-            for (int v = 0; v < VN; ++v) p += vget(va, v) * vget(vb, v) * vget(vc, v);
+            for (int v = 0; v < VN; ++v) p += vget(a, v) * vget(b, v) * vget(c, v);
 #pragma unroll
             for (int o = GL / 2; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
             if (gl == 0 && (uint64_t)src < cnt) {
@@ -193,6 +197,8 @@ __device__ __forceinline__ double sse_span(const uint4 *__restrict__ rec, const 
                 acc += (double)e * (double)e;
             }
         }
+        va = na;  // the slices of the rows cur0 / cur1 name
+        vb = nb;
     }
     return acc;
 }
