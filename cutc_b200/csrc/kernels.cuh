@@ -91,6 +91,11 @@ __device__ __forceinline__ void vatomic_add(double2 *p, const double2 &d)
 // where a fixed stride would leave the grid waiting on the unluckiest warp.
 struct TaskClaim {
     unsigned int *ctr;
+    // quarters of the tasks handed out on a fixed stride before any is
+    // claimed (0: all claimed), for grids whose warps are all resident: the
+    // stride takes part of them without an atomic, and the claimed rest
+    // evens out the finish
+    uint32_t stride_quarters;
     __device__ __forceinline__ uint32_t next(int lane) const
     {
         uint32_t t = 0;
@@ -108,6 +113,26 @@ struct TaskClaim {
                 ctr[1] = 0u;
             }
         }
+    }
+};
+
+// A warp's task indices under a TaskClaim: its fixed-stride share first
+// (warp, warp + nwarps, ... for stride_quarters / 4 of the tasks), then
+// indices claimed after that share.  Warp-uniform.
+struct WarpTaskSeq {
+    TaskClaim c;
+    uint32_t warp, nwarps, per, k, base;
+    __device__ __forceinline__ WarpTaskSeq(const TaskClaim &tc, uint32_t ntasks) : c(tc), k(0)
+    {
+        warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        nwarps = (gridDim.x * blockDim.x) >> 5;
+        per = (uint32_t)(((uint64_t)ntasks * tc.stride_quarters / 4u) / nwarps);
+        base = per * nwarps;
+    }
+    __device__ __forceinline__ uint32_t next(int lane)
+    {
+        if (k < per) return warp + (k++) * nwarps;
+        return base + c.next(lane);
     }
 };
 
@@ -844,14 +869,16 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
 
     // tasks: {tile, len, -1, 0} for a light tile, {first tile, pieces,
     // heavy row, group} for up to kCcdppGroup consecutive pieces of one long
-    // row.  A warp claims its tasks one at a time (TaskClaim), so warps that
-    // drew short tasks take more (a long-row group runs up to kCcdppGroup
-    // times a light tile); the task after the current one is claimed, and
-    // its descriptor fetched, while the current one runs.
+    // row.  A warp takes a fixed-stride share of the tasks, then claims the
+    // rest one at a time (TaskClaim, WarpTaskSeq), so warps that drew short
+    // tasks take more (a long-row group runs up to kCcdppGroup times a light
+    // tile); the task after the current one is known, and its descriptor
+    // fetched, while the current one runs.
     const int4 kNoTask = make_int4(0, 0, -1, 0);
-    uint32_t cur_i = claim.next(lane);
+    WarpTaskSeq seq(claim, ntasks);
+    uint32_t cur_i = seq.next(lane);
     int4 td_cur = cur_i < ntasks ? tasks[cur_i] : kNoTask;
-    uint32_t nxt_i = cur_i < ntasks ? claim.next(lane) : ntasks;
+    uint32_t nxt_i = cur_i < ntasks ? seq.next(lane) : ntasks;
     int4 td_nxt = nxt_i < ntasks ? tasks[nxt_i] : kNoTask;
     while (cur_i < ntasks) {
         const int4 td = td_cur;
@@ -859,7 +886,7 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
         cur_i = nxt_i;
         td_cur = td_nxt;
         if (cur_i < ntasks) {
-            nxt_i = claim.next(lane);
+            nxt_i = seq.next(lane);
             if (nxt_i < ntasks) td_nxt = tasks[nxt_i];
         }
         uint64_t kv[E];
@@ -1708,6 +1735,9 @@ __global__ void __launch_bounds__(128) k_als_tile(const int4 *__restrict__ tiles
     T b[C];
     // tiles claimed one at a time (TaskClaim): tiles of many short rows, or
     // pieces that the tensor-core Gram takes, cost very different times
+    // (every tile claimed: the grid is larger than the resident blocks, and
+    // the fixed-stride sequence's state raised the rank-32 FP32 kernel from
+    // 128 to 254 registers, halving its warps per SM)
     for (uint32_t tile = claim.next(lane); tile < ntiles; tile = claim.next(lane)) {
         const int4 td = tiles[tile];
         const uint32_t start = (uint32_t)td.x, end = start + (uint32_t)td.y;
