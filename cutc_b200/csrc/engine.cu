@@ -109,6 +109,7 @@ struct DevTensor {
     uint32_t nslots = 0;  // CCD++: ntiles * slot length (lane-interleaved tiles)
     DevBuf<int4> tasks;   // CCD++ warp tasks (light tiles, groups of pieces)
     uint32_t ntasks = 0;
+    uint64_t nrows = 0;   // rows of the copy's mode that hold nonzeros (0: not counted)
 };
 
 static int bits_for(uint64_t d)
@@ -462,6 +463,7 @@ static void stage_copies_dev(ctc_ctx *ctx, const ctc_params &p, uint32_t tl, con
                                  (p.rank == 32 || p.rank == 64) && p.compat == 0;
             plan = plan_tiles_runs(rows.data(), counts.data(), rows.size(), tl, tc_rows ? kMixedHeavyMin : 0u);
             upload_plan(ctx, plan, m, d);
+            d.nrows = rows.size();  // one run per row: the copy is sorted by its mode
         }
         if (ccdpp) {
             TracePhase tp("CCD++ slots");
@@ -553,6 +555,7 @@ struct Session : SessionBase {
     uint32_t tile_len;
     DevBuf<T> U[3], Ubest[3], Urow[3], slot, slot2, lr_dev;
     DevBuf<k::Pack3<T>> pk[3];  // CCD++ per-column {cur, prev, old}
+    DevBuf<k::Pack2<T>> pk2[3];  // ... and {old, prev} (+2: staged copies read whole 16-byte words)
     DevBuf<unsigned int> hcnt[3];  // CCD++ pieces arrived per heavy row (reset by the finaliser)
     // {next, done} task claim counters of the kernels that claim their warp
     // tasks (k::TaskClaim); every launch leaves them at zero
@@ -586,6 +589,8 @@ struct Session : SessionBase {
             if (colmajor) {
                 Urow[m].alloc(sz);
                 pk[m].alloc(dims[m]);
+                pk2[m].alloc(dims[m] + 2);
+                CK(cudaMemsetAsync(pk2[m].p, 0, pk2[m].n * sizeof(k::Pack2<T>), ctx->stream));
                 hcnt[m].alloc(D->copy[m].nheavy);
                 CK(cudaMemsetAsync(hcnt[m].p, 0, hcnt[m].n * sizeof(unsigned int), ctx->stream));
             }
@@ -650,6 +655,10 @@ struct Session : SessionBase {
                                 smem));
         CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, false, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem));
+        CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, true, E, false, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, true, E, true, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     }
 
     // shared memory per block of a CCD++ pass for staged factor columns: two
@@ -1026,21 +1035,37 @@ struct Session : SessionBase {
         }
     }
 
+    // fresh: the column's first pass (no mode swept yet in this column)
     template <int E>
-    void ccdpp_pass(int m, int f, bool first)
+    void ccdpp_pass(int m, int f, bool first, bool fresh)
     {
         DevTensor<T> &c = D->copy[m];
         T *out = U[m].p + (size_t)f * dims[m];
         k::CcdppCols<T> cols{};
-        size_t need[2];
+        size_t need[2], need2[2];
         for (int q = 0; q < 2; ++q) {
             const int n = (m + 1 + q) % 3;
             cols.col[q] = U[n].p + (size_t)f * dims[n];
             cols.pk[q] = pk[n].p;
+            cols.pk2[q] = pk2[n].p;
             cols.dim[q] = dims[n];
             // bytes one copy takes (the column copy may start up to 15
             // bytes early to reach a 16-byte boundary)
             need[q] = first ? (size_t)dims[n] * sizeof(k::Pack3<T>) : (((size_t)dims[n] * sizeof(T) + 15 + 15) & ~15ull);
+            need2[q] = ((size_t)dims[n] * sizeof(k::Pack2<T>) + 15) & ~15ull;
+        }
+        // the column's first pass: both gathered modes' half packs staged in
+        // a 1024-thread block per SM, when they fit its shared memory
+        if (fresh && p.smem_budget >= 0 &&
+            need2[0] + need2[1] <= std::min<size_t>((size_t)ccdpp_smem_max(),
+                                                    p.smem_budget > 0 ? 2 * (size_t)p.smem_budget : SIZE_MAX)) {
+            cols.stage[0] = cols.stage[1] = 1;
+            const unsigned g = grid_for((uint64_t)c.ntasks, 32, kSMs);
+            if (c.ks.rbits)
+                ccdpp_launch_fresh<E, true>(c, g, need2[0] + need2[1], cols, out, m);
+            else
+                ccdpp_launch_fresh<E, false>(c, g, need2[0] + need2[1], cols, out, m);
+            return;
         }
         // stage both when they fit, else the one that fits
         const size_t budget = ccdpp_budget();
@@ -1072,6 +1097,14 @@ struct Session : SessionBase {
                    (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p, k::TaskClaim{claim.p, kCcdppStrideQuarters});
     }
 
+    template <int E, bool PK>
+    void ccdpp_launch_fresh(DevTensor<T> &c, unsigned g, size_t smem, const k::CcdppCols<T> &cols, T *out, int m)
+    {
+        LAUNCH(ctx, (k::k_ccdpp_pass<T, true, E, PK, true>), g, 1024, smem, (const int4 *)c.tasks.p, c.ntasks,
+               c.keys.p, c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p, (const uint4 *)c.heavy.p,
+               hcnt[m].p, dev_err.p, k::TaskClaim{claim.p, kCcdppStrideQuarters});
+    }
+
     // One CCD++ outer iteration: per column f, the {cur, prev, old} packs,
     // then `inner` sweeps over the modes of the column update (the first
     // sweep of each copy also refreshes its residual); finally one pass per
@@ -1085,6 +1118,7 @@ struct Session : SessionBase {
             k::PackArgs pa{};
             for (int n = 0; n < 3; ++n) {
                 pa.pk[n] = pk[n].p;
+                pa.pk2[n] = pk2[n].p;
                 pa.col[n] = U[n].p + (size_t)f * dims[n];
                 pa.pcol[n] = f > 0 ? (const void *)(U[n].p + (size_t)(f - 1) * dims[n]) : nullptr;
                 pa.dims[n] = dims[n];
@@ -1094,10 +1128,14 @@ struct Session : SessionBase {
             for (int it = 0; it < inner; ++it) {
                 for (int q = 0; q < 3; ++q) {
                     const int m = (p.mode_start + q) % 3;
-                    CK(cudaMemsetAsync(U[m].p + (size_t)f * dims[m], 0, dims[m] * sizeof(T), ctx->stream));
-                    if (lanes == 4) ccdpp_pass<4>(m, f, it == 0);
-                    else if (lanes == 8) ccdpp_pass<8>(m, f, it == 0);
-                    else ccdpp_pass<16>(m, f, it == 0);
+                    // a row without nonzeros gets u = 0 / (lambda + 0): the
+                    // pass writes only the rows it sees
+                    if (D->copy[m].nrows != dims[m])
+                        CK(cudaMemsetAsync(U[m].p + (size_t)f * dims[m], 0, dims[m] * sizeof(T), ctx->stream));
+                    const bool fresh = it == 0 && q == 0;
+                    if (lanes == 4) ccdpp_pass<4>(m, f, it == 0, fresh);
+                    else if (lanes == 8) ccdpp_pass<8>(m, f, it == 0, fresh);
+                    else ccdpp_pass<16>(m, f, it == 0, fresh);
                 }
             }
         }

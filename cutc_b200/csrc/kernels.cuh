@@ -711,6 +711,16 @@ template <typename T>
 struct alignas(4 * sizeof(T)) Pack3 {
     T cur, prev, old, pad;
 };
+// A mode not yet swept in column f (cur == old): {old, final f-1}, half a
+// Pack3, so that the first pass of a column can stage both gathered modes
+template <typename T>
+struct alignas(2 * sizeof(T)) Pack2 {
+    T old, prev;
+};
+template <typename T>
+__device__ __forceinline__ T pack_cur(const Pack3<T> &p) { return p.cur; }
+template <typename T>
+__device__ __forceinline__ T pack_cur(const Pack2<T> &p) { return p.old; }
 
 template <typename T>
 __device__ __forceinline__ void ccdpp_finalize(uint32_t row, T nu, T de, T lambda, T *out, Pack3<T> *pkm)
@@ -770,15 +780,20 @@ template <typename T>
 struct CcdppCols {
     const T *col[2];          // column f of modes m+1, m+2 (global)
     const Pack3<T> *pk[2];    // packs of modes m+1, m+2 (global)
+    const Pack2<T> *pk2[2];   // their half packs (the column's first pass)
     uint32_t dim[2];
     int stage[2];             // 1: staged in shared memory
 };
 
-template <typename T, bool FIRST>
+template <typename T, bool FIRST, bool FRESH>
 __device__ __forceinline__ uint32_t ccdpp_stage_span(const CcdppCols<T> &c, int q, const unsigned char *&src,
                                                      uint32_t &skew)
 {
-    if constexpr (FIRST) {
+    if constexpr (FIRST && FRESH) {
+        src = reinterpret_cast<const unsigned char *>(c.pk2[q]);
+        skew = 0;
+        return (c.dim[q] * (uint32_t)sizeof(Pack2<T>) + 15u) & ~15u;
+    } else if constexpr (FIRST) {
         src = reinterpret_cast<const unsigned char *>(c.pk[q]);
         skew = 0;
         return c.dim[q] * (uint32_t)sizeof(Pack3<T>);
@@ -790,16 +805,20 @@ __device__ __forceinline__ uint32_t ccdpp_stage_span(const CcdppCols<T> &c, int 
     }
 }
 
-// PK: packed slots (residual in the key word, no residual array).
-template <typename T, bool FIRST, int E, bool PK = false>
-__global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ tasks, uint32_t ntasks,
-                                                       uint64_t *__restrict__ keys, T *__restrict__ res,
-                                                       KeyShape ks, Pack3<T> *pkm, CcdppCols<T> cols, T *out,
-                                                       T lambda, T *__restrict__ slot_nu, T *__restrict__ slot_de,
-                                                       const uint4 *__restrict__ heavy, unsigned int *hcnt, int *err,
-                                                       TaskClaim claim)
+// PK: packed slots (residual in the key word, no residual array).  FRESH
+// (with FIRST): the column's first pass, where neither gathered mode has
+// been swept yet, gathers half packs; it runs as one 1024-thread block per
+// SM, whose shared memory holds both gathered modes' half packs.
+template <typename T, bool FIRST, int E, bool PK = false, bool FRESH = false>
+__global__ void __launch_bounds__(FRESH ? 1024 : 512, FRESH ? 1 : 2)
+    k_ccdpp_pass(const int4 *__restrict__ tasks, uint32_t ntasks, uint64_t *__restrict__ keys, T *__restrict__ res,
+                 KeyShape ks, Pack3<T> *pkm, CcdppCols<T> cols, T *out, T lambda, T *__restrict__ slot_nu,
+                 T *__restrict__ slot_de, const uint4 *__restrict__ heavy, unsigned int *hcnt, int *err,
+                 TaskClaim claim)
 {
-    using ColT = typename std::conditional<FIRST, Pack3<T>, T>::type;
+    static_assert(FIRST || !FRESH, "half packs only in a column's first pass");
+    using ColT = typename std::conditional<FIRST, typename std::conditional<FRESH, Pack2<T>, Pack3<T>>::type,
+                                           T>::type;
     constexpr uint32_t kNone = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char ccdpp_smem[];
     __shared__ __align__(8) uint64_t mbar;
@@ -815,7 +834,7 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
         for (int q = 0; q < 2; ++q)
             if (cols.stage[q]) {
                 uint32_t skew;
-                bytes[q] = ccdpp_stage_span<T, FIRST>(cols, q, src[q], skew);
+                bytes[q] = ccdpp_stage_span<T, FIRST, FRESH>(cols, q, src[q], skew);
                 dst[q] = off;
                 sc[q] = reinterpret_cast<const ColT *>(ccdpp_smem + off + skew);
                 off += bytes[q];
@@ -844,7 +863,8 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
         }
     }
     auto gat = [&](int q, uint32_t i) -> ColT {
-        if constexpr (FIRST) return sc[q] ? sc[q][i] : cols.pk[q][i];
+        if constexpr (FIRST && FRESH) return sc[q] ? sc[q][i] : cols.pk2[q][i];
+        else if constexpr (FIRST) return sc[q] ? sc[q][i] : cols.pk[q][i];
         else return sc[q] ? sc[q][i] : __ldg(cols.col[q] + i);
     };
     // Later sweeps: the gathers of EC entries e0 .. e0+EC-1 are all issued
@@ -916,10 +936,10 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
                             if constexpr (FIRST) {
                                 uint32_t rr, q1, q2;
                                 unpack_key(kv[e], ks, rr, q1, q2);
-                                const Pack3<T> ga = gat(0, q1), gb = gat(1, q2);
+                                const ColT ga = gat(0, q1), gb = gat(1, q2);
                                 r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
                                 rv[e] = r;
-                                hh = ga.cur * gb.cur;
+                                hh = pack_cur<T>(ga) * pack_cur<T>(gb);
                             } else {
                                 hh = h[k];
                             }
@@ -1003,10 +1023,10 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
                     T r = rv[e];
                     T hh;
                     if constexpr (FIRST) {
-                        const Pack3<T> ga = gat(0, q1), gb = gat(1, q2);
+                        const ColT ga = gat(0, q1), gb = gat(1, q2);
                         r = r - pm.prev * ga.prev * gb.prev + pm.old * ga.old * gb.old;
                         rv[e] = r;
-                        hh = ga.cur * gb.cur;
+                        hh = pack_cur<T>(ga) * pack_cur<T>(gb);
                     } else {
                         hh = h[k];
                     }
@@ -1053,9 +1073,11 @@ __global__ void __launch_bounds__(512, 2) k_ccdpp_pass(const int4 *__restrict__ 
 }
 
 // pack[n][row] = {U_n(row, f), U_n(row, f-1) or 0, U_n(row, f), 0} for the
-// three modes (column-major factors), before the sweeps of column f.
+// three modes (column-major factors), before the sweeps of column f, and
+// the half pack {U_n(row, f), U_n(row, f-1) or 0} when pk2[n] is given.
 struct PackArgs {
     void *pk[3];
+    void *pk2[3];
     const void *col[3];   // column f
     const void *pcol[3];  // column f-1 or null
     uint32_t dims[3];
@@ -1085,6 +1107,12 @@ __global__ void k_ccdpp_pack(PackArgs a)
         v.old = c;
         v.pad = 0;
         static_cast<Pack3<T> *>(a.pk[n])[r] = v;
+        if (a.pk2[n]) {
+            Pack2<T> h;
+            h.old = c;
+            h.prev = p;
+            static_cast<Pack2<T> *>(a.pk2[n])[r] = h;
+        }
     }
 }
 
@@ -1155,18 +1183,40 @@ __global__ void __launch_bounds__(256) k_ccdpp_finish(uint64_t *__restrict__ key
                                                       const T *__restrict__ c1, const T *__restrict__ c2,
                                                       double *__restrict__ partial)
 {
+    // four slots per thread per round, every load and gather issued before
+    // any residual is formed
+    constexpr int U = 4;
     double acc = 0;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        const uint64_t key = keys[p];
-        if (key == kPadKey) continue;
-        uint32_t idx[3];
-        key_modes(key, ks, m, idx);
-        const T r0 = PK ? (T)packed_res(key, ks.rbits) : res[p];
-        const T r = r0 - c0[idx[0]] * c1[idx[1]] * c2[idx[2]];
-        ccdpp_store_res<T, PK>(keys, res, p, key, r, ks.rbits);
-        // the SSE of the residual as stored
-        const T rs = PK ? (T)packed_res(with_res(key, (float)r, ks.rbits), ks.rbits) : r;
-        acc += (double)rs * (double)rs;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint64_t p0 = blockIdx.x * blockDim.x + threadIdx.x; p0 < n; p0 += (uint64_t)U * stride) {
+        uint64_t key[U];
+        T r0[U], g[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t p = p0 + (uint64_t)u * stride;
+            key[u] = p < n ? keys[p] : kPadKey;
+            r0[u] = (!PK && p < n) ? res[p] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            g[u] = 0;
+            if (key[u] != kPadKey) {
+                uint32_t idx[3];
+                key_modes(key[u], ks, m, idx);
+                g[u] = c0[idx[0]] * c1[idx[1]] * c2[idx[2]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (key[u] == kPadKey) continue;
+            const uint64_t p = p0 + (uint64_t)u * stride;
+            const T rb = PK ? (T)packed_res(key[u], ks.rbits) : r0[u];
+            const T r = rb - g[u];
+            ccdpp_store_res<T, PK>(keys, res, p, key[u], r, ks.rbits);
+            // the SSE of the residual as stored
+            const T rs = PK ? (T)packed_res(with_res(key[u], (float)r, ks.rbits), ks.rbits) : r;
+            acc += (double)rs * (double)rs;
+        }
     }
     if (partial) {
         acc = block_sum(acc);
