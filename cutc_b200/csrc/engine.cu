@@ -394,6 +394,9 @@ static int default_tile(int alg)
 // 91.0 ms with half on the stride, 93.1 ms with three quarters, 100.6 ms
 // with all but the remainder.
 constexpr uint32_t kCcdppStrideQuarters = 2;
+// CCD++ later sweeps staging one column of at least this many bytes while
+// gathering the other through L1 run as one 1024-thread block per SM
+constexpr size_t kCcdppBigStaged = 32 * 1024;
 // Mixed ALS: the row length above which a row takes tiles of its own and a
 // tensor-core Gram, below the tile length that packs the light rows (on the
 // 100M rank-32 tensor, tile 1024: 21.1 ms per iteration with the tile
@@ -658,6 +661,10 @@ struct Session : SessionBase {
         CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, true, E, false, true>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, true, E, true, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, false, E, false, false, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CK(cudaFuncSetAttribute(k::k_ccdpp_pass<T, false, E, true, false, true>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     }
 
@@ -1076,11 +1083,30 @@ struct Session : SessionBase {
             cols.stage[q] = 1;
         }
         const size_t smem = (cols.stage[0] ? need[0] : 0) + (cols.stage[1] ? need[1] : 0);
+        // a later sweep that stages one sizeable column and gathers the other
+        // through L1: one 1024-thread block per SM holds the staged column
+        // once, which leaves L1 more room for the other
+        if (!first && (cols.stage[0] ^ cols.stage[1]) && smem >= kCcdppBigStaged) {
+            const unsigned g = grid_for((uint64_t)c.ntasks, 32, kSMs);
+            if (c.ks.rbits)
+                ccdpp_launch_big<E, true>(c, g, smem, cols, out, m);
+            else
+                ccdpp_launch_big<E, false>(c, g, smem, cols, out, m);
+            return;
+        }
         const unsigned g = grid_for((uint64_t)c.ntasks, 16, kSMs * 2);
         if (c.ks.rbits)
             ccdpp_launch<E, true>(c, first, g, smem, cols, out, m);
         else
             ccdpp_launch<E, false>(c, first, g, smem, cols, out, m);
+    }
+
+    template <int E, bool PK>
+    void ccdpp_launch_big(DevTensor<T> &c, unsigned g, size_t smem, const k::CcdppCols<T> &cols, T *out, int m)
+    {
+        LAUNCH(ctx, (k::k_ccdpp_pass<T, false, E, PK, false, true>), g, 1024, smem, (const int4 *)c.tasks.p,
+               c.ntasks, c.keys.p, c.res.p, c.ks, pk[m].p, cols, out, (T)p.lambda, slot.p, slot2.p,
+               (const uint4 *)c.heavy.p, hcnt[m].p, dev_err.p, k::TaskClaim{claim.p, kCcdppStrideQuarters});
     }
 
     template <int E, bool PK>

@@ -809,8 +809,11 @@ __device__ __forceinline__ uint32_t ccdpp_stage_span(const CcdppCols<T> &c, int 
 // (with FIRST): the column's first pass, where neither gathered mode has
 // been swept yet, gathers half packs; it runs as one 1024-thread block per
 // SM, whose shared memory holds both gathered modes' half packs.
-template <typename T, bool FIRST, int E, bool PK = false, bool FRESH = false>
-__global__ void __launch_bounds__(FRESH ? 1024 : 512, FRESH ? 1 : 2)
+// BIG: one 1024-thread block per SM (FRESH passes, and later sweeps whose
+// staged column would otherwise be held twice per SM, at the cost of the L1
+// their other gathers go through)
+template <typename T, bool FIRST, int E, bool PK = false, bool FRESH = false, bool BIG = FRESH>
+__global__ void __launch_bounds__(BIG ? 1024 : 512, BIG ? 1 : 2)
     k_ccdpp_pass(const int4 *__restrict__ tasks, uint32_t ntasks, uint64_t *__restrict__ keys, T *__restrict__ res,
                  KeyShape ks, Pack3<T> *pkm, CcdppCols<T> cols, T *out, T lambda, T *__restrict__ slot_nu,
                  T *__restrict__ slot_de, const uint4 *__restrict__ heavy, unsigned int *hcnt, int *err,
