@@ -234,6 +234,34 @@ def test_ccdpp_column_staging_paths_agree(ctx, tile_len):
     assert max_factor_rel(G, U) < 1e-4
 
 
+def test_ccdpp_one_block_per_sm_sweeps_agree(ctx):
+    """Later sweeps that stage one column of 32 KB or more and gather the
+    other through L1 run as one 1024-thread block per SM: here the mode-1
+    passes, which stage the 12,000-row column (48 KB) and gather the
+    40,000-row one (FP32: 48 KB; FP64: 96 KB).  (The columns' first passes
+    do not stage half packs: the two gathered modes' packs exceed a block's
+    shared memory.)  In FP32 and FP64 the factors equal those of the run
+    that stages nothing, bit for bit; the FP64 run matches the FP64 oracle
+    to 1e-9 in RMSE and 1e-7 in the factors (this small, overfitted problem,
+    whose 40,000-row mode has about 3 nonzeros a row against lambda 0.1,
+    ends at a train RMSE near 0.06 and amplifies rounding: FP32 shows at
+    1e-3 relative, FP64 factors at 5.5e-9)."""
+    P = Problem(150000, (300, 12000, 40000), 16, seed=45)
+    U, hist, _ = oracle_ccdpp(P, 2, 0.1, 2)
+    for prec in (ctc.PREC_F32, ctc.PREC_F64):
+        runs = {}
+        for budget in (0, -1):
+            runs[budget] = engine_run(ctx, P, ctc.CCDPP, 2, precision=prec, inner=2, tile_len=256,
+                                      smem_budget=budget, **{"lambda": 0.1})
+        for m in range(3):
+            assert np.array_equal(runs[0][0][m], runs[-1][0][m]), (prec, m)
+    G, out = runs[0]
+    for e, (tr, te) in enumerate(hist):
+        assert abs(out.epochs[e]["rmse_tr"] - tr) / tr < 1e-9, e
+        assert abs(out.epochs[e]["rmse_te"] - te) / te < 1e-9, e
+    assert max_factor_rel(G, U) < 1e-7
+
+
 # ------------------------------------------------------------------ SGD
 def oracle_sgd(P, iters, lr, lam, scale=1.0, decay=1.0, trunc=False):
     U = P.factors()
