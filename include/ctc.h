@@ -273,7 +273,11 @@ typedef struct {
                               (sgpu/sgd.cu:32)                                      */
     int smem_budget;       /* CCD++: shared memory per block (bytes) for the factor
                               columns a pass gathers; columns that fit are staged
-                              there once per block.  0 = 110 KiB, < 0 = none       */
+                              there once per block.  0 = 110 KiB, < 0 = none.  A
+                              column's first pass stages both gathered modes'
+                              half packs in one 1024-thread block per SM when
+                              they fit twice the budget (0: the block's whole
+                              shared memory)                                        */
 } ctc_params;
 
 /* Reference-default parameters for an algorithm (sgpu/base.h:19-64). */
