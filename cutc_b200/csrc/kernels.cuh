@@ -670,7 +670,11 @@ static __global__ void k_sgd_hot_codes(const uint4 *__restrict__ rec, uint32_t n
 // which is the rank-one add-back of f fused with the subtraction of f-1.
 // The other two modes' column f (or packs, in FIRST) are gathered from
 // shared memory when they fit the block's budget (copied in once per
-// persistent block by a bulk async copy), else through L1.
+// persistent block by a bulk async copy), else through L1.  Blocks are
+// 512 threads, two per SM, except for a column's first pass when both
+// gathered modes' half packs fit one block's shared memory, and for later
+// sweeps that stage one sizeable column while gathering the other through
+// L1: those run as one 1024-thread block per SM.
 // ---------------------------------------------------------------------
 struct KeyShape {
     uint32_t s_row, s_q1;   // key >> s_row = row ; (key >> s_q1) & m_q1 = q1
