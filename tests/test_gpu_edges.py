@@ -1,0 +1,140 @@
+"""The update rules at the edges of the input space, in FP64 on the GPU
+against the FP64 oracle: factors within 1e-9 of the largest factor entry,
+per-iteration RMSE within 1e-9 (relative, absolute below 1; the values
+lie between 1 and 5).
+
+- a mode with a single row, in each of the three positions;
+- a single nonzero;
+- 32k, 32k + 1 and 32k + 31 nonzeros: full, just started and nearly full
+  32-entry groups, the warp and tile edges of the reference layout
+  (sgpu/base.h:62, DEFAULT_T_TILE_LENGTH 32);
+- modes whose rows are mostly empty: ALS and CCD++ set a row without
+  nonzeros to 0 (sgpu/als.cu:699, 730, 757 clear each factor before its
+  row solves; the rank-one update gives 0 / (lambda + 0)), CCD and SGD
+  leave it as it was;
+- the mode-1 tensor alone, so that the other two copies are sorted, split
+  into row runs and planned on the device at these sizes too.
+
+An empty training or test tensor is rejected on the host, before any
+launch, with CTC_E_ARG (the reference would divide by its zero nonzero
+count in the RMSE, sgpu/completion.c:129)."""
+import numpy as np
+import pytest
+
+import cutc_b200 as ctc
+from oracle import pyoracle as po
+from tests.helpers import Problem, max_factor_rel
+
+R = 8
+ITERS = 2
+# CCD (the reference rule, all R columns of a row from one residual) needs
+# the larger lambda to stay bounded on these few nonzeros
+LAM = {"als": 0.5, "ccd": 5.0, "ccdpp": 0.1, "sgd": 0.01}
+INNER = 2
+LR, DECAY = 0.01, 0.95
+
+CASES = {
+    "one-row-mode-1": (25, (1, 9, 8)),
+    "one-row-mode-2": (25, (9, 1, 8)),
+    "one-row-mode-3": (25, (9, 8, 1)),
+    "one-nonzero": (1, (3, 4, 5)),
+    "nnz-64": (64, (12, 10, 8)),
+    "nnz-65": (65, (12, 10, 8)),
+    "nnz-95": (95, (12, 10, 8)),
+    "mostly-empty-rows": (40, (500, 400, 300)),
+}
+
+
+def make_problem(case):
+    nnz, dims = CASES[case]
+    P = Problem(nnz, dims, R, seed=200 + sorted(CASES).index(case), test_frac=0.0)
+    P.test = (P.train[0][:, :5], P.train[1][:5])
+    return P
+
+
+def oracle_run(P, alg):
+    U = P.factors()
+    hist = [(po.rmse(P.o_train(), U), po.rmse(P.o_test(), U))]
+    T0 = P.o_sorted(0)
+    resid = po.residual(T0, U) if alg == "ccdpp" else None
+    lr = LR
+    for _ in range(ITERS):
+        if alg == "als":
+            for m in range(3):
+                po.als_mode(P.o_sorted(m), m, U, LAM[alg])
+        elif alg == "ccd":
+            for m in range(3):
+                po.ccd_compat_mode(P.o_sorted(m), m, U, LAM[alg], None, False)
+        elif alg == "ccdpp":
+            po.ccdpp_outer(T0, U, LAM[alg], INNER, resid)
+        else:
+            po.sgd_epoch(T0, U, lr, LAM[alg])
+            lr *= DECAY
+        hist.append((po.rmse(P.o_train(), U), po.rmse(P.o_test(), U)))
+    return U, hist
+
+
+def engine_params(alg):
+    kw = dict(rank=R, iters=ITERS, precision=ctc.PREC_F64, early_stop=0, eval_every=1)
+    kw["lambda"] = LAM[alg]
+    if alg == "ccdpp":
+        kw["inner"] = INNER
+    if alg == "sgd":
+        kw.update(sgd_order=ctc.SGD_SEQUENTIAL, lr=LR, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY,
+                  lr_decay=DECAY)
+    return ctc.params(alg, **kw)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("copies", ["three", "one"])
+@pytest.mark.parametrize("alg", ["als", "ccd", "ccdpp", "sgd"])
+@pytest.mark.parametrize("case", list(CASES))
+def test_edge_shapes_match_oracle(ctx, case, alg, copies):
+    if alg == "sgd" and copies == "one":
+        pytest.skip("SGD reads the mode-1 copy only")
+    P = make_problem(case)
+    U, hist = oracle_run(P, alg)
+    train = P.c_sorted() if copies == "three" else P.c_sorted()[:1]
+    model = P.c_model()
+    out = ctc.run(ctx, train, None, P.c_test(), model, engine_params(alg))
+    G = model.factors()
+    assert max_factor_rel(G, U) < 1e-9
+    for e, (tr, te) in enumerate(hist):
+        if alg != "sgd":
+            assert abs(out.epochs[e]["rmse_tr"] - tr) < 1e-9 * max(tr, 1.0), e
+        assert abs(out.epochs[e]["rmse_te"] - te) < 1e-9 * max(te, 1.0), e
+
+
+def test_mostly_empty_rows_keep_the_reference_values():
+    """The oracle side of the empty-row rule the GPU test above checks
+    (no GPU needed): after ALS and CCD++ the rows without nonzeros are 0,
+    after CCD and SGD they keep their initial values."""
+    P = make_problem("mostly-empty-rows")
+    for alg in ("als", "ccd", "ccdpp", "sgd"):
+        U, _ = oracle_run(P, alg)
+        for m in range(3):
+            hit = np.zeros(P.dims[m], dtype=bool)
+            hit[P.train[0][m].astype(np.int64) - 1] = True
+            empty = ~hit
+            assert empty.sum() > 0
+            if alg in ("als", "ccdpp"):
+                assert np.all(U[m][empty] == 0.0), (alg, m)
+            else:
+                assert np.array_equal(U[m][empty], P.U0[m][empty]), (alg, m)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("alg", ["als", "ccd", "ccdpp", "sgd"])
+def test_empty_tensors_are_rejected(ctx, alg):
+    P = make_problem("nnz-64")
+    empty = ctc.Tensor.from_coo(np.zeros((3, 0), dtype=np.uint64), np.zeros(0), dims=P.dims)
+    p = engine_params(alg)
+    with pytest.raises(ctc.CtcError) as e:
+        ctc.run(ctx, [empty], None, P.c_test(), P.c_model(), p)
+    assert e.value.code == -1 and "empty" in str(e.value)
+    with pytest.raises(ctc.CtcError) as e:
+        ctc.run(ctx, P.c_sorted(), None, empty, P.c_model(), p)
+    assert e.value.code == -1 and "empty" in str(e.value)
+    with pytest.raises(ctc.CtcError) as e:
+        ctc.rmse(ctx, empty, P.c_model())
+    assert e.value.code == -1 and "empty" in str(e.value)
