@@ -74,8 +74,8 @@ def oracle_run(P, alg):
     return U, hist
 
 
-def engine_params(alg):
-    kw = dict(rank=R, iters=ITERS, precision=ctc.PREC_F64, early_stop=0, eval_every=1)
+def engine_params(alg, precision=ctc.PREC_F64):
+    kw = dict(rank=R, iters=ITERS, precision=precision, early_stop=0, eval_every=1)
     kw["lambda"] = LAM[alg]
     if alg == "ccdpp":
         kw["inner"] = INNER
@@ -103,6 +103,64 @@ def test_edge_shapes_match_oracle(ctx, case, alg, copies):
         if alg != "sgd":
             assert abs(out.epochs[e]["rmse_tr"] - tr) < 1e-9 * max(tr, 1.0), e
         assert abs(out.epochs[e]["rmse_te"] - te) < 1e-9 * max(te, 1.0), e
+
+
+# FP32 against the FP64 oracle on the same edges.  RMSE within 5e-5
+# absolute: 1e-5 of the largest value (5); on these few nonzeros a late
+# RMSE is a small difference of values near 5, so a relative bound would
+# measure the cancellation, not the kernels.  Factors within 1e-4 of the
+# largest entry, CCD++ within 1e-3: its rank-one updates on 95 nonzeros
+# amplify rounding (a float32 numpy restatement of the same two outer
+# iterations lands 1.3e-4 from FP64; ALS restated the same way, 7.5e-6).
+F32_FACTORS = {"als": 1e-4, "ccd": 1e-4, "ccdpp": 1e-3, "sgd": 1e-4}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("alg", ["als", "ccd", "ccdpp", "sgd"])
+@pytest.mark.parametrize("case", list(CASES))
+def test_edge_shapes_fp32(ctx, case, alg):
+    """FP32 at the same edges.  For CCD++ the mixed-precision form (the
+    residual packed into the key word) runs too: these dimensions leave
+    all 32 residual bits beside the key, so it must equal the FP32 run bit
+    for bit."""
+    P = make_problem(case)
+    U, hist = oracle_run(P, alg)
+    model = P.c_model()
+    out = ctc.run(ctx, P.c_sorted(), None, P.c_test(), model, engine_params(alg, ctc.PREC_F32))
+    G = model.factors()
+    assert max_factor_rel(G, U) < F32_FACTORS[alg]
+    for e, (tr, te) in enumerate(hist):
+        if alg != "sgd":
+            assert abs(out.epochs[e]["rmse_tr"] - tr) < 5e-5, e
+        assert abs(out.epochs[e]["rmse_te"] - te) < 5e-5, e
+    if alg == "ccdpp":
+        mm = P.c_model()
+        om = ctc.run(ctx, P.c_sorted(), None, P.c_test(), mm, engine_params(alg, ctc.PREC_MIXED))
+        for a, b in zip(mm.factors(), G):
+            assert np.array_equal(a, b)
+        assert [x["rmse_te"] for x in om.epochs] == [x["rmse_te"] for x in out.epochs]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("atomic", [1, 2, 3])
+@pytest.mark.parametrize("case", list(CASES))
+def test_edge_shapes_hogwild_learn(ctx, case, atomic):
+    """Hogwild SGD in FP32 (vector atomics, bulk row reductions, block-merged
+    hot rows: fewer rows than hot-row slots here) on the same edges, five
+    epochs at lr 0.05: the factors stay finite and the test RMSE falls, as
+    the sequential oracle's does on every case (a bulk reduction still in
+    flight when the next nonzero of the same row reads it is Hogwild's own
+    staleness, so these tiny, all-hot tensors are not held to the
+    sequential trajectory; the 0.5 % pins run on realistic tensors)."""
+    P = make_problem(case)
+    kw = dict(rank=R, iters=5, precision=ctc.PREC_F32, early_stop=0, eval_every=1, tile_len=128,
+              sgd_atomic=atomic, lr=0.05, lr_scale=1.0, lr_schedule=ctc.LR_EXP_DECAY, lr_decay=DECAY)
+    kw["lambda"] = LAM["sgd"]
+    model = P.c_model()
+    out = ctc.run(ctx, P.c_sorted()[:1], None, P.c_test(), model, ctc.params("sgd", **kw))
+    assert all(np.isfinite(g).all() for g in model.factors())
+    te = [e["rmse_te"] for e in out.epochs]
+    assert te[-1] < te[0], te
 
 
 def test_mostly_empty_rows_keep_the_reference_values():
