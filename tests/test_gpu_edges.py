@@ -163,6 +163,31 @@ def test_edge_shapes_hogwild_learn(ctx, case, atomic):
     assert te[-1] < te[0], te
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("alg", ["als", "ccd", "sgd"])
+def test_edge_shapes_in_one_batch(ctx, alg):
+    """All the edge tensors above as the instances of one batch
+    (ctc_batch_*: stacked block-diagonally, one launch per mode update for
+    all of them; CCD++ does not batch): each instance matches its own FP64
+    oracle run, factors and per-iteration RMSE within 1e-9."""
+    probs = [make_problem(c) for c in CASES]
+    p = engine_params(alg)
+    B = ctc.Batch(ctx, [ctc.Tensor.from_coo(*P.train, dims=P.dims) for P in probs],
+                  [P.c_test() for P in probs], p)
+    models = [P.c_model() for P in probs]
+    try:
+        out = B.run(models, p)
+    finally:
+        B.free()
+    for b, P in enumerate(probs):
+        U, hist = oracle_run(P, alg)
+        assert max_factor_rel(models[b].factors(), U) < 1e-9, list(CASES)[b]
+        for e, (tr, te) in enumerate(hist):
+            if alg != "sgd":
+                assert abs(out.epochs[e][2][b] - tr) < 1e-9 * max(tr, 1.0), (list(CASES)[b], e)
+            assert abs(out.epochs[e][3][b] - te) < 1e-9 * max(te, 1.0), (list(CASES)[b], e)
+
+
 def test_mostly_empty_rows_keep_the_reference_values():
     """The oracle side of the empty-row rule the GPU test above checks
     (no GPU needed): after ALS and CCD++ the rows without nonzeros are 0,
