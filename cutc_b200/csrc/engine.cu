@@ -258,8 +258,9 @@ static void stage_tensor(ctc_ctx *ctx, const ctc_tensor *t, bool trunc, DevTenso
             memcpy(&bits, &vf, 4);
             const uint64_t a0 = i0[i] - 1, a1 = i1[i] - 1, a2 = i2[i] - 1;
             oob |= (a0 >= c0) | (a1 >= c1) | (a2 >= c2);
-            h[i - b] = make_uint4((uint32_t)a0, (uint32_t)a1, (uint32_t)a2, bits);
+            stream_store16(h + (i - b), (uint32_t)a0, (uint32_t)a1, (uint32_t)a2, bits);
         }
+        stream_fence();
         if (oob) bad = 1;
     });
     if (check) {

@@ -20,6 +20,10 @@
 #include <type_traits>
 #include <vector>
 
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
+
 namespace ctc {
 
 static void check_cuda(cudaError_t e, const char *what)
@@ -175,6 +179,28 @@ namespace ctc {
 // host memory, element b at h[0]); the copy of one chunk runs while the
 // next one is filled on the host threads.
 constexpr size_t kPinBytes = (size_t)32 << 20;
+
+// 16 bytes into pinned staging memory (16-byte aligned) with a streaming
+// store where the host has one: the staging buffers are written once and
+// then read by the copy engine, so a normal store's fetch of the line it
+// is about to overwrite is wasted host memory traffic.  A thread that
+// streamed calls stream_fence() before its data may be copied.
+static inline void stream_store16(void *dst, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+#if defined(__SSE2__)
+    _mm_stream_si128(reinterpret_cast<__m128i *>(dst), _mm_set_epi32((int)d, (int)c, (int)b, (int)a));
+#else
+    const uint32_t v[4] = {a, b, c, d};
+    memcpy(dst, v, sizeof(v));
+#endif
+}
+
+static inline void stream_fence()
+{
+#if defined(__SSE2__)
+    _mm_sfence();
+#endif
+}
 
 static void ensure_pinned(ctc_ctx *ctx)
 {
