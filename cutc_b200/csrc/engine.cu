@@ -301,9 +301,16 @@ static void upload_plan(ctc_ctx *ctx, const TilePlan &p, int mode, DevTensor<T> 
     d.nheavy = p.nheavy();
     d.tiles.upload(reinterpret_cast<const int4 *>(p.tiles.data()), p.ntiles(), ctx->stream);
     d.heavy.upload(reinterpret_cast<const uint4 *>(p.heavy_rows.data()), p.nheavy(), ctx->stream);
+    // the tiles that are pieces of long rows, in order: each long row's
+    // pieces are the consecutive tiles first .. first + count - 1, and the
+    // long rows are numbered in tile order
     std::vector<uint32_t> pieces;
-    for (uint32_t t = 0; t < p.ntiles(); ++t)
-        if (p.tiles[4 * t + 2] >= 0) pieces.push_back(t);
+    size_t np = 0;
+    for (uint32_t h = 0; h < p.nheavy(); ++h) np += p.heavy_rows[4 * h + 2];
+    pieces.resize(np);
+    np = 0;
+    for (uint32_t h = 0; h < p.nheavy(); ++h)
+        for (uint32_t q = 0; q < p.heavy_rows[4 * h + 2]; ++q) pieces[np++] = p.heavy_rows[4 * h + 1] + q;
     d.npieces = (uint32_t)pieces.size();
     d.pieces.upload(pieces.data(), pieces.size(), ctx->stream);
     CK(cudaStreamSynchronize(ctx->stream));

@@ -783,6 +783,46 @@ TilePlan plan_tiles_chunked(const uint64_t *ind, uint64_t n, uint32_t T, bool *u
 // light tiles end at a cut, and tiles / heavy rows are numbered in order,
 // so the two builders give the same plan.  O(runs + tiles).  Rows longer
 // than H (0: T) get tiles of their own, pieces of at most T nonzeros.
+// The chunks are planned in parallel on the host workers (heavy-row
+// numbers and first tiles counted within the chunk), then laid end to end.
+static TilePlan plan_run_span(const uint32_t *rows, const uint32_t *counts, const uint64_t *start, uint64_t r,
+                              uint64_t rend, uint32_t T, uint32_t H)
+{
+    TilePlan p;
+    p.tiles.reserve((size_t)((start[rend] - start[r]) / std::max<uint32_t>(T / 2, 1) + 16) * 4);
+    auto tile = [&p](uint64_t s, uint64_t len, int32_t h, int32_t q) {
+        p.tiles.push_back((int32_t)s);
+        p.tiles.push_back((int32_t)len);
+        p.tiles.push_back(h);
+        p.tiles.push_back(q);
+    };
+    while (r < rend) {
+        const uint64_t len = counts[r];
+        if (len > H) {
+            const uint32_t h = p.nheavy(), first = p.ntiles();
+            const uint32_t np = (uint32_t)((len + T - 1) / T);
+            const uint64_t s0 = start[r], e = s0 + len;
+            for (uint32_t q = 0; q < np; ++q) {
+                const uint64_t s = s0 + (uint64_t)q * T;
+                tile(s, std::min<uint64_t>(T, e - s), (int32_t)h, (int32_t)q);
+            }
+            p.heavy_rows.insert(p.heavy_rows.end(), {rows[r], first, np, 0u});
+            ++r;
+            continue;
+        }
+        const uint64_t s = start[r];
+        uint64_t size = 0;
+        while (r < rend) {
+            const uint64_t l = counts[r];
+            if (l > H || size + l > T) break;
+            size += l;
+            ++r;
+        }
+        tile(s, size, -1, 0);
+    }
+    return p;
+}
+
 TilePlan plan_tiles_runs(const uint32_t *rows, const uint32_t *counts, uint64_t nruns, uint32_t T, uint32_t H)
 {
     if (H == 0 || H > T) H = T;
@@ -797,37 +837,35 @@ TilePlan plan_tiles_runs(const uint32_t *rows, const uint32_t *counts, uint64_t 
         const uint64_t x = std::max<uint64_t>(n * (uint64_t)c / chunks, start[cut[c - 1]]);
         cut[c] = (uint64_t)(std::lower_bound(start.begin(), start.end(), x) - start.begin());
     }
-    TilePlan p;
-    p.tiles.reserve((size_t)(n / std::max<uint32_t>(T / 2, 1) + 16) * 4);
+    if (chunks == 1) return plan_run_span(rows, counts, start.data(), 0, nruns, T, H);
+    std::vector<TilePlan> part(chunks);
+    host_run(chunks, [&](int c) { part[c] = plan_run_span(rows, counts, start.data(), cut[c], cut[c + 1], T, H); });
+    std::vector<uint32_t> tbase(chunks + 1, 0), hbase(chunks + 1, 0);
     for (int c = 0; c < chunks; ++c) {
-        uint64_t r = cut[c];
-        const uint64_t rend = cut[c + 1];
-        while (r < rend) {
-            const uint64_t len = counts[r];
-            if (len > H) {
-                const uint32_t h = p.nheavy(), first = p.ntiles();
-                const uint32_t np = (uint32_t)((len + T - 1) / T);
-                const uint64_t s0 = start[r], e = s0 + len;
-                for (uint32_t q = 0; q < np; ++q) {
-                    const uint64_t s = s0 + (uint64_t)q * T;
-                    p.tiles.insert(p.tiles.end(),
-                                   {(int32_t)s, (int32_t)std::min<uint64_t>(T, e - s), (int32_t)h, (int32_t)q});
-                }
-                p.heavy_rows.insert(p.heavy_rows.end(), {rows[r], first, np, 0u});
-                ++r;
-                continue;
-            }
-            const uint64_t s = start[r];
-            uint64_t size = 0;
-            while (r < rend) {
-                const uint64_t l = counts[r];
-                if (l > H || size + l > T) break;
-                size += l;
-                ++r;
-            }
-            p.tiles.insert(p.tiles.end(), {(int32_t)s, (int32_t)size, -1, 0});
-        }
+        tbase[c + 1] = tbase[c] + part[c].ntiles();
+        hbase[c + 1] = hbase[c] + part[c].nheavy();
     }
+    TilePlan p;
+    p.tiles.resize((size_t)tbase[chunks] * 4);
+    p.heavy_rows.resize((size_t)hbase[chunks] * 4);
+    host_run(chunks, [&](int c) {
+        const TilePlan &q = part[c];
+        int32_t *t = p.tiles.data() + (size_t)tbase[c] * 4;
+        for (size_t i = 0; i < q.tiles.size(); i += 4) {
+            const int32_t h = q.tiles[i + 2];
+            t[i] = q.tiles[i];
+            t[i + 1] = q.tiles[i + 1];
+            t[i + 2] = h >= 0 ? h + (int32_t)hbase[c] : h;
+            t[i + 3] = q.tiles[i + 3];
+        }
+        uint32_t *hr = p.heavy_rows.data() + (size_t)hbase[c] * 4;
+        for (size_t i = 0; i < q.heavy_rows.size(); i += 4) {
+            hr[i] = q.heavy_rows[i];
+            hr[i + 1] = q.heavy_rows[i + 1] + tbase[c];
+            hr[i + 2] = q.heavy_rows[i + 2];
+            hr[i + 3] = q.heavy_rows[i + 3];
+        }
+    });
     return p;
 }
 

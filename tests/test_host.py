@@ -374,6 +374,11 @@ def test_plan_from_runs_is_the_plan_from_indices(n, nrows, T):
         pieces = ta[first:first + np_]
         assert np.all(pieces[:, 2] == h) and np.array_equal(pieces[:, 3], np.arange(np_))
         assert np.all(ind[pieces[:, 0]] == row + 1)
+    # the tiles with a long-row index are exactly the long rows' ranges, in
+    # order (the staging lists the pieces from the long-row table)
+    ranges = [np.arange(f, f + k) for (_, f, k, _) in ha]
+    listed = np.concatenate(ranges) if ranges else np.zeros(0, dtype=np.int64)
+    assert np.array_equal(np.flatnonzero(ta[:, 2] >= 0), listed)
 
 
 def test_plan_rejects_unsorted_indices():
