@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <charconv>
 #include <condition_variable>
+#include <exception>
 #include <functional>
 #include <memory>
 #include <mutex>
@@ -50,6 +51,9 @@ int host_threads()
 // works too): parallel loops over staging chunks no longer create and join
 // a thread set per call.  One job runs at a time; callers from several
 // threads queue on run_mu, and a loop started inside a task runs inline.
+// A task that throws (an allocation failure, a library error) does not end
+// the process: the job's other tasks still run, and the first exception is
+// rethrown to the caller once all of them are done.
 namespace {
 thread_local bool tl_in_task = false;
 
@@ -57,6 +61,7 @@ struct HostPool {
     std::mutex run_mu, mu;
     std::condition_variable cv_start, cv_done;
     const std::function<void(int)> *job = nullptr;
+    std::exception_ptr err;
     int ntasks = 0, next = 0, pending = 0;
     uint64_t gen = 0;
     bool stop = false;
@@ -83,9 +88,15 @@ struct HostPool {
             const std::function<void(int)> *f = job;
             l.unlock();
             tl_in_task = true;
-            (*f)(t);
+            std::exception_ptr e;
+            try {
+                (*f)(t);
+            } catch (...) {
+                e = std::current_exception();
+            }
             tl_in_task = false;
             l.lock();
+            if (e && !err) err = e;
             if (--pending == 0) cv_done.notify_all();
         }
     }
@@ -113,6 +124,9 @@ struct HostPool {
         drain(l);
         cv_done.wait(l, [&] { return pending == 0; });
         job = nullptr;
+        std::exception_ptr e = err;
+        err = nullptr;
+        if (e) std::rethrow_exception(e);
     }
 };
 }  // namespace
